@@ -1,0 +1,108 @@
+"""ctypes binding of libkpzb200.so (the C ABI in include/kpzb.h).
+
+The shared library is built in tree by ``cudakpz_b200.build``.  There is no
+fallback: if the library is missing or fails to load, importing this module
+raises ``ImportError`` with the reason.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from pathlib import Path
+
+LIB_PATH = Path(__file__).resolve().parent / "libkpzb200.so"
+
+KPZB_OK = 0
+STATUS_NAMES = {0: "KPZB_OK", 1: "KPZB_EINVAL", 2: "KPZB_ENOMEM", 3: "KPZB_ECUDA",
+                4: "KPZB_ETIMEOUT", 5: "KPZB_ESTATE", 6: "KPZB_EUNSUPPORTED"}
+
+ENC_LOCAL, ENC_CBBIT = 0, 1
+DYN_SCA, DYN_SCABIT, DYN_DT = 0, 1, 2
+
+
+class KpzbError(RuntimeError):
+    """A kpzb_* call returned a non-zero status."""
+
+    def __init__(self, status: int, func: str, msg: str):
+        super().__init__(f"{func} -> {STATUS_NAMES.get(status, status)}: {msg}")
+        self.status = status
+
+
+_u32p = C.POINTER(C.c_uint32)
+_u64p = C.POINTER(C.c_uint64)
+_i64p = C.POINTER(C.c_int64)
+_dblp = C.POINTER(C.c_double)
+_intp = C.POINTER(C.c_int)
+_vp = C.c_void_p
+
+# name -> (restype, argtypes); every symbol declared in include/kpzb.h
+SIGNATURES = {
+    "kpzb_last_error": (C.c_char_p, []),
+    "kpzb_version": (C.c_char_p, []),
+    "kpzb_create": (C.c_int, [C.POINTER(_vp), C.c_int, C.c_int, C.c_int, C.c_int]),
+    "kpzb_destroy": (C.c_int, [_vp]),
+    "kpzb_init_homogeneous": (C.c_int, [_vp]),
+    "kpzb_set_pq": (C.c_int, [_vp, C.c_double, C.c_double]),
+    "kpzb_seed": (C.c_int, [_vp, C.c_uint64, C.c_uint32]),
+    "kpzb_mcs": (C.c_int, [_vp, C.c_int]),
+    "kpzb_mcs_async": (C.c_int, [_vp, C.c_int]),
+    "kpzb_join": (C.c_int, [_vp]),
+    "kpzb_set_fusion": (C.c_int, [_vp, C.c_int]),
+    "kpzb_get_fusion": (C.c_int, [_vp, _intp]),
+    "kpzb_push": (C.c_int, [_vp, _vp]),
+    "kpzb_pop": (C.c_int, [_vp, _vp]),
+    "kpzb_push_device": (C.c_int, [_vp, _vp]),
+    "kpzb_pop_device": (C.c_int, [_vp, _vp]),
+    "kpzb_size_words": (C.c_size_t, [_vp]),
+    "kpzb_encoding": (C.c_int, [_vp]),
+    "kpzb_roughness": (C.c_int, [_vp, _dblp]),
+    "kpzb_height_sums": (C.c_int, [_vp, _i64p, _i64p]),
+    "kpzb_corr_tag": (C.c_int, [_vp, _dblp]),
+    "kpzb_correlate": (C.c_int, [_vp, _dblp]),
+    "kpzb_get_mcs": (C.c_int, [_vp, _u64p]),
+    "kpzb_set_mcs": (C.c_int, [_vp, C.c_uint64]),
+    "kpzb_counters": (C.c_int, [_vp, _i64p, C.c_int]),
+    "kpzb_enable_counters": (C.c_int, [_vp, C.c_int]),
+    "kpzb_check_invariants": (C.c_int, [_vp, _i64p]),
+    "kpzb_device_ptr": (C.c_int, [_vp, C.POINTER(_vp), C.POINTER(C.c_size_t)]),
+    "kpzb_stream": (_vp, [_vp]),
+    "kpzb_set_stream": (C.c_int, [_vp, _vp]),
+    "kpzb_batch_create": (C.c_int, [C.POINTER(_vp), C.c_int, _intp, _dblp, _dblp, _u64p,
+                                    C.POINTER(C.c_uint32), C.c_int]),
+    "kpzb_batch_destroy": (C.c_int, [_vp]),
+    "kpzb_batch_init_homogeneous": (C.c_int, [_vp]),
+    "kpzb_batch_mcs": (C.c_int, [_vp, C.c_int]),
+    "kpzb_batch_push": (C.c_int, [_vp, C.c_int, _vp]),
+    "kpzb_batch_pop": (C.c_int, [_vp, C.c_int, _vp]),
+    "kpzb_batch_roughness": (C.c_int, [_vp, _dblp]),
+    "kpzb_gram_create": (C.c_int, [C.POINTER(_vp), C.c_int, C.c_int, C.c_int, C.c_int]),
+    "kpzb_gram_destroy": (C.c_int, [_vp]),
+    "kpzb_gram_add_device": (C.c_int, [_vp, _vp]),
+    "kpzb_gram_add_host": (C.c_int, [_vp, _vp]),
+    "kpzb_gram_compute": (C.c_int, [_vp, C.c_int, _i64p, _i64p]),
+    "kpzb_gram_count": (C.c_int, [_vp]),
+}
+
+
+def _load():
+    if not LIB_PATH.exists():
+        raise ImportError(
+            f"{LIB_PATH} is missing; build it with `python -m cudakpz_b200.build` "
+            "(the CUDA path has no fallback)")
+    try:
+        lib = C.CDLL(str(LIB_PATH), mode=os.RTLD_NOW | os.RTLD_GLOBAL)
+    except OSError as e:  # pragma: no cover - depends on the machine
+        raise ImportError(f"cannot load {LIB_PATH}: {e}") from e
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    return lib
+
+
+lib = _load()
+
+
+def check(status: int, func: str) -> None:
+    if status != KPZB_OK:
+        raise KpzbError(status, func, lib.kpzb_last_error().decode(errors="replace"))

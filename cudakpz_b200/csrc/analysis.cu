@@ -1,0 +1,443 @@
+// analysis.cu -- height reconstruction, roughness moments, correlator and lattice
+// invariants on ENC_CBBIT lattices (sm_100a).
+//
+// Heights follow the reference's path walk (kpz/correlator.cpp:47-96, :337-399):
+//   row y starts at Hs(y) = h(0,y-1) + (2*s_y(0,y)-1) with h(0,-1) = 0, walks x = 1..L-1
+//   adding 2*s_x(x,y)-1, and the wrap adds 2*s_x(0,y)-1 giving h(0,y) = Hs(y) + rowsum(y).
+// Moments: S1 and S2 exact in int64, S3..S7 in FP64; ch uses the exact int64 cross sum;
+// cs counts equal minus different slope bits (kpz/correlator.cpp:463-477).
+// Invariants extend SchedulerService::consitencyCheck (kpz/schedulerService.cpp:733-854)
+// to ENC_CBBIT: x-slope row sums, y-slope column sums, plaquette loops.
+//
+// Three passes: (1) per-row x=0 slopes and x-slope sums, (2) one-CTA scan over rows to
+// get row-start heights, (3) per-site walk with a CTA-wide scan of 64-site chunk sums.
+// Per-CTA partials are reduced in a fixed order so the FP64 sums are deterministic.
+#include "kpzb_common.cuh"
+#include "kpzb_internal.h"
+
+namespace kpzb {
+
+constexpr int AN_THREADS = 256;
+constexpr int AN_MAX_GRID = 1184;
+
+struct Partial {
+    long long s1, s2, hmin, hmax, cross, agree, snap_s1, pad;
+    double s[5];
+    double pad2[3];
+};
+
+// ---- pass 1: per-row x=0 slopes and x-slope row sums (one warp per row) ----
+__global__ void rowinfo_kernel(const uint32_t* __restrict__ sys, int lx, int ly, int32_t* rowinfo)
+{
+    const uint64_t Wr = 1ull << (lx - 6);
+    const uint64_t Q = 1ull << (lx + ly - 6);
+    const uint64_t rows = 1ull << ly;
+    const int lane = threadIdx.x & 31;
+    const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+    const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    for (uint64_t y = warp; y < rows; y += nwarps) {
+        int cnt = 0;
+        for (uint64_t j = lane; j < Wr; j += 32)
+            cnt += __popc(sys[y * Wr + j]) + __popc(sys[2 * Q + y * Wr + j]);
+        for (int o = 16; o > 0; o >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
+        if (lane == 0) {
+            // site (0,y) lies on sublattice y&1, word 0, bit 0
+            const uint64_t b0 = (y & 1) ? 2 * Q : 0;
+            const int sy0 = (int)(sys[b0 + Q + y * Wr] & 1u);
+            rowinfo[2 * y] = 2 * sy0 - 1;
+            rowinfo[2 * y + 1] = 2 * cnt - (int)(1ull << lx);
+        }
+    }
+}
+
+// ---- pass 2: row-start heights Hs(y) (single CTA, chunked Hillis-Steele scan) ----
+__global__ void rowstart_kernel(const int32_t* __restrict__ rowinfo, int ly, int64_t* rowstart)
+{
+    __shared__ long long buf[1024];
+    __shared__ long long carry;
+    const uint64_t rows = 1ull << ly;
+    if (threadIdx.x == 0) carry = 0;
+    __syncthreads();
+    for (uint64_t base = 0; base < rows; base += 1024) {
+        const uint64_t y = base + threadIdx.x;
+        // Hs(y) = sum_{y'<=y} ycol(y') + sum_{y'<y} rowsum(y')
+        // contribution of row y to the inclusive scan: ycol(y) + rowsum(y-1) handled as
+        // v(y) = ycol(y) + rowsum(y); Hs(y) = incl(v)(y) - rowsum(y)
+        long long v = (y < rows) ? (long long)rowinfo[2 * y] + rowinfo[2 * y + 1] : 0;
+        buf[threadIdx.x] = v;
+        __syncthreads();
+        for (int o = 1; o < 1024; o <<= 1) {
+            long long add = (threadIdx.x >= (unsigned)o) ? buf[threadIdx.x - o] : 0;
+            __syncthreads();
+            buf[threadIdx.x] += add;
+            __syncthreads();
+        }
+        if (y < rows) rowstart[y] = carry + buf[threadIdx.x] - rowinfo[2 * y + 1];
+        __syncthreads();
+        if (threadIdx.x == 1023) carry += buf[1023];
+        __syncthreads();
+    }
+}
+
+// ---- pass 3: per-site walk ----
+// MODE 0: moments; MODE 1: moments + correlate against snap; MODE 2: write heights.
+template <int MODE>
+__global__ void __launch_bounds__(AN_THREADS)
+walk_kernel(const uint32_t* __restrict__ sys, const uint32_t* __restrict__ snap, int lx, int ly,
+            const int32_t* __restrict__ rowinfo, const int64_t* __restrict__ rowstart,
+            const int32_t* __restrict__ rowinfo_s, const int64_t* __restrict__ rowstart_s,
+            int32_t* __restrict__ heights, Partial* __restrict__ partials)
+{
+    __shared__ long long wsum[AN_THREADS / 32];
+    __shared__ long long wsum_s[AN_THREADS / 32];
+    __shared__ long long segc[AN_THREADS];
+    __shared__ long long segc_s[AN_THREADS];
+
+    const uint64_t Wr = 1ull << (lx - 6);
+    const uint64_t Q = 1ull << (lx + ly - 6);
+    const uint64_t rows = 1ull << ly;
+    const int TPR = (int)(Wr < AN_THREADS ? Wr : AN_THREADS);
+    const int RPC = AN_THREADS / TPR;
+    const int tx = threadIdx.x % TPR, ty = threadIdx.x / TPR;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const int nseg = (int)(Wr / TPR);
+    const uint64_t groups = rows / RPC;
+    const uint64_t L = 1ull << lx;
+
+    long long s1 = 0, s2 = 0, cross = 0, agree = 0, ss1 = 0;
+    long long hmin = 0x7fffffffffffffffll, hmax = -0x7fffffffffffffffll;
+    double s3 = 0, s4 = 0, s5 = 0, s6 = 0, s7 = 0;
+
+    for (uint64_t g = blockIdx.x; g < groups; g += gridDim.x) {
+        const uint64_t y = g * RPC + ty;
+        const uint64_t be = (y & 1) ? 2 * Q : 0, bo = (y & 1) ? 0 : 2 * Q;
+        const long long Hs = rowstart[y];
+        const long long rsum = rowinfo[2 * y + 1];
+        long long Hs_s = 0, rsum_s = 0;
+        if (MODE == 1) {
+            Hs_s = rowstart_s[y];
+            rsum_s = rowinfo_s[2 * y + 1];
+        }
+        // e0 = 2*s_x(0,y)-1 (bit 0 of the even-x word 0)
+        const long long e0 = 2 * (long long)(sys[be + y * Wr] & 1u) - 1;
+        long long e0_s = 0;
+        if (MODE == 1) e0_s = 2 * (long long)(snap[be + y * Wr] & 1u) - 1;
+        long long run = 0, run_s = 0;  // prefix carried from previous segments
+        for (int seg = 0; seg < nseg; ++seg) {
+            const uint64_t c = (uint64_t)seg * TPR + tx;
+            const uint32_t E = sys[be + y * Wr + c], O = sys[bo + y * Wr + c];
+            uint32_t Es = 0, Os = 0;
+            if (MODE == 1) {
+                Es = snap[be + y * Wr + c];
+                Os = snap[bo + y * Wr + c];
+                const uint32_t EY = sys[be + Q + y * Wr + c], OY = sys[bo + Q + y * Wr + c];
+                const uint32_t EYs = snap[be + Q + y * Wr + c], OYs = snap[bo + Q + y * Wr + c];
+                agree += 2 * (__popc(~(E ^ Es)) + __popc(~(O ^ Os)) + __popc(~(EY ^ EYs)) +
+                              __popc(~(OY ^ OYs))) - 128;
+            }
+            long long v = 2 * (__popc(E) + __popc(O)) - 64;
+            long long vs = (MODE == 1) ? 2 * (__popc(Es) + __popc(Os)) - 64 : 0;
+            // inclusive scan of v over the TPR threads of this row
+            long long incl = v, incl_s = vs;
+            const int wl = TPR < 32 ? TPR : 32;
+            for (int o = 1; o < wl; o <<= 1) {
+                long long a = __shfl_up_sync(0xffffffffu, incl, o, wl);
+                long long as = __shfl_up_sync(0xffffffffu, incl_s, o, wl);
+                if ((lane % wl) >= o) {
+                    incl += a;
+                    incl_s += as;
+                }
+            }
+            if (TPR > 32) {
+                if (lane == 31) {
+                    wsum[wid] = incl;
+                    wsum_s[wid] = incl_s;
+                }
+                __syncthreads();
+                const int w0 = (ty * TPR) >> 5;  // first warp of this row
+                for (int w = w0; w < wid; ++w) {
+                    incl += wsum[w];
+                    incl_s += wsum_s[w];
+                }
+            }
+            // P(x) before this chunk (inclusive prefix from x = 0)
+            long long P = run + incl - v;
+            long long Ps = run_s + incl_s - vs;
+            // last thread of the row publishes the segment total
+            if (tx == TPR - 1) {
+                segc[ty] = run + incl;
+                segc_s[ty] = run_s + incl_s;
+            }
+            __syncthreads();
+            run = segc[ty];
+            run_s = segc_s[ty];
+            __syncthreads();
+            for (int i = 0; i < 64; ++i) {
+                const uint32_t bit = (((i & 1) ? O : E) >> (i >> 1)) & 1u;
+                P += 2 * (long long)bit - 1;
+                const uint64_t x = c * 64 + i;
+                const long long h = (x == 0) ? Hs + rsum : Hs - e0 + P;
+                if (MODE == 2) {
+                    heights[y * L + x] = (int32_t)h;
+                } else {
+                    s1 += h;
+                    s2 += h * h;
+                    const double d = (double)h, d2 = d * d, d3 = d2 * d;
+                    s3 += d3;
+                    s4 += d2 * d2;
+                    s5 += d3 * d2;
+                    s6 += d3 * d3;
+                    s7 += d3 * d3 * d;
+                    hmin = min(hmin, h);
+                    hmax = max(hmax, h);
+                    if (MODE == 1) {
+                        const uint32_t bs = (((i & 1) ? Os : Es) >> (i >> 1)) & 1u;
+                        Ps += 2 * (long long)bs - 1;
+                        const long long hs = (x == 0) ? Hs_s + rsum_s : Hs_s - e0_s + Ps;
+                        cross += h * hs;
+                        ss1 += hs;
+                    }
+                }
+            }
+        }
+    }
+    if constexpr (MODE == 2) return;
+    // block reduction in fixed order
+    __shared__ Partial red[AN_THREADS / 32];
+    for (int o = 16; o > 0; o >>= 1) {
+        s1 += __shfl_xor_sync(0xffffffffu, s1, o);
+        s2 += __shfl_xor_sync(0xffffffffu, s2, o);
+        cross += __shfl_xor_sync(0xffffffffu, cross, o);
+        agree += __shfl_xor_sync(0xffffffffu, agree, o);
+        ss1 += __shfl_xor_sync(0xffffffffu, ss1, o);
+        hmin = min(hmin, __shfl_xor_sync(0xffffffffu, hmin, o));
+        hmax = max(hmax, __shfl_xor_sync(0xffffffffu, hmax, o));
+        s3 += __shfl_xor_sync(0xffffffffu, s3, o);
+        s4 += __shfl_xor_sync(0xffffffffu, s4, o);
+        s5 += __shfl_xor_sync(0xffffffffu, s5, o);
+        s6 += __shfl_xor_sync(0xffffffffu, s6, o);
+        s7 += __shfl_xor_sync(0xffffffffu, s7, o);
+    }
+    if (lane == 0) {
+        Partial p;
+        p.s1 = s1; p.s2 = s2; p.hmin = hmin; p.hmax = hmax; p.cross = cross; p.agree = agree;
+        p.snap_s1 = ss1; p.pad = 0;
+        p.s[0] = s3; p.s[1] = s4; p.s[2] = s5; p.s[3] = s6; p.s[4] = s7;
+        red[wid] = p;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        Partial p = red[0];
+        for (int w = 1; w < AN_THREADS / 32; ++w) {
+            const Partial& q = red[w];
+            p.s1 += q.s1; p.s2 += q.s2; p.cross += q.cross; p.agree += q.agree;
+            p.snap_s1 += q.snap_s1;
+            p.hmin = min(p.hmin, q.hmin); p.hmax = max(p.hmax, q.hmax);
+            for (int k = 0; k < 5; ++k) p.s[k] += q.s[k];
+        }
+        partials[blockIdx.x] = p;
+    }
+}
+
+__global__ void final_reduce_kernel(const Partial* __restrict__ partials, int n, Partial* out)
+{
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    Partial p = partials[0];
+    for (int i = 1; i < n; ++i) {
+        const Partial& q = partials[i];
+        p.s1 += q.s1; p.s2 += q.s2; p.cross += q.cross; p.agree += q.agree;
+        p.snap_s1 += q.snap_s1;
+        p.hmin = min(p.hmin, q.hmin); p.hmax = max(p.hmax, q.hmax);
+        for (int k = 0; k < 5; ++k) p.s[k] += q.s[k];
+    }
+    *out = p;
+}
+
+cudaError_t analysis_alloc(AnalysisScratch* s, int ly)
+{
+    const size_t rows = 1ull << ly;
+    s->rows_cap = rows;
+    cudaError_t e;
+    // two row tables (system and snapshot) and partials + final record
+    if ((e = cudaMalloc(&s->rowinfo, 4 * rows * sizeof(int32_t))) != cudaSuccess) return e;
+    if ((e = cudaMalloc(&s->rowstart, 2 * rows * sizeof(int64_t))) != cudaSuccess) return e;
+    if ((e = cudaMalloc(&s->acc, (AN_MAX_GRID + 1) * sizeof(Partial) + 64)) != cudaSuccess) return e;
+    return cudaSuccess;
+}
+
+void analysis_free(AnalysisScratch* s)
+{
+    cudaFree(s->rowinfo);
+    cudaFree(s->rowstart);
+    cudaFree(s->acc);
+    s->rowinfo = nullptr;
+    s->rowstart = nullptr;
+    s->acc = nullptr;
+}
+
+static int walk_grid(int lx, int ly)
+{
+    const uint64_t Wr = 1ull << (lx - 6);
+    const int TPR = (int)(Wr < AN_THREADS ? Wr : AN_THREADS);
+    const uint64_t groups = (1ull << ly) / (AN_THREADS / TPR);
+    return (int)(groups < AN_MAX_GRID ? groups : AN_MAX_GRID);
+}
+
+static cudaError_t row_tables(const uint32_t* d, int lx, int ly, int32_t* ri, int64_t* rs,
+                              cudaStream_t st)
+{
+    const uint64_t rows = 1ull << ly;
+    const int grid = (int)((rows * 32 + 255) / 256 < 4096 ? (rows * 32 + 255) / 256 : 4096);
+    rowinfo_kernel<<<grid, 256, 0, st>>>(d, lx, ly, ri);
+    rowstart_kernel<<<1, 1024, 0, st>>>(ri, ly, rs);
+    return cudaGetLastError();
+}
+
+cudaError_t analysis_moments(const uint32_t* d_sys, const uint32_t* d_snap, int lx, int ly,
+                             AnalysisScratch* s, MomentsOut* out, cudaStream_t st)
+{
+    const uint64_t rows = 1ull << ly;
+    int32_t* ri = s->rowinfo;
+    int32_t* ri_s = s->rowinfo + 2 * rows;
+    int64_t* rs = s->rowstart;
+    int64_t* rs_s = s->rowstart + rows;
+    Partial* parts = reinterpret_cast<Partial*>(s->acc);
+    Partial* fin = parts + AN_MAX_GRID;
+    cudaError_t e = row_tables(d_sys, lx, ly, ri, rs, st);
+    if (e != cudaSuccess) return e;
+    const int grid = walk_grid(lx, ly);
+    if (d_snap) {
+        if ((e = row_tables(d_snap, lx, ly, ri_s, rs_s, st)) != cudaSuccess) return e;
+        walk_kernel<1><<<grid, AN_THREADS, 0, st>>>(d_sys, d_snap, lx, ly, ri, rs, ri_s, rs_s,
+                                                    nullptr, parts);
+    } else {
+        walk_kernel<0><<<grid, AN_THREADS, 0, st>>>(d_sys, nullptr, lx, ly, ri, rs, nullptr,
+                                                    nullptr, nullptr, parts);
+    }
+    final_reduce_kernel<<<1, 32, 0, st>>>(parts, grid, fin);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    Partial h;
+    if ((e = cudaMemcpyAsync(&h, fin, sizeof(Partial), cudaMemcpyDeviceToHost, st)) != cudaSuccess)
+        return e;
+    if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return e;
+    out->s1 = h.s1;
+    out->s2 = h.s2;
+    for (int k = 0; k < 5; ++k) out->s3to7[k] = h.s[k];
+    out->hmin = h.hmin;
+    out->hmax = h.hmax;
+    out->cross = h.cross;
+    out->agree = h.agree;
+    out->snap_s1 = h.snap_s1;
+    return cudaSuccess;
+}
+
+cudaError_t analysis_heights(const uint32_t* d_sys, int lx, int ly, AnalysisScratch* s,
+                             int32_t* d_heights, cudaStream_t st)
+{
+    cudaError_t e = row_tables(d_sys, lx, ly, s->rowinfo, s->rowstart, st);
+    if (e != cudaSuccess) return e;
+    walk_kernel<2><<<walk_grid(lx, ly), AN_THREADS, 0, st>>>(d_sys, nullptr, lx, ly, s->rowinfo,
+                                                             s->rowstart, nullptr, nullptr,
+                                                             d_heights, nullptr);
+    return cudaGetLastError();
+}
+
+// ---- invariants ----
+// columns: thread per (x parity a, word column j, band of 256 rows); per-bit counters.
+__global__ void colsum_kernel(const uint32_t* __restrict__ sys, int lx, int ly, int* colsum)
+{
+    const uint64_t Wr = 1ull << (lx - 6);
+    const uint64_t Q = 1ull << (lx + ly - 6);
+    const uint64_t rows = 1ull << ly;
+    const uint64_t band = rows < 256 ? rows : 256;
+    const uint64_t nb = rows / band;
+    const uint64_t total = 2 * Wr * nb;
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < total;
+         i += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t j = i % Wr;
+        const int a = (int)((i / Wr) & 1);
+        const uint64_t b = i / (2 * Wr);
+        int cnt[32];
+#pragma unroll
+        for (int k = 0; k < 32; ++k) cnt[k] = 0;
+        for (uint64_t y = b * band; y < (b + 1) * band; ++y) {
+            const int sub = a ^ (int)(y & 1);
+            const uint32_t w = sys[(sub ? 2 * Q : 0) + Q + y * Wr + j];
+#pragma unroll
+            for (int k = 0; k < 32; ++k) cnt[k] += (w >> k) & 1u;
+        }
+#pragma unroll
+        for (int k = 0; k < 32; ++k) {
+            const uint64_t x = 64 * j + 2 * k + a;
+            atomicAdd(&colsum[x], 2 * cnt[k] - (int)band);
+        }
+    }
+}
+
+__global__ void invariants_kernel(const uint32_t* __restrict__ sys, int lx, int ly,
+                                  const int32_t* __restrict__ rowinfo, const int* __restrict__ colsum,
+                                  unsigned long long* rep)
+{
+    const uint64_t Wr = 1ull << (lx - 6);
+    const uint64_t Q = 1ull << (lx + ly - 6);
+    const uint64_t rows = 1ull << ly;
+    const uint64_t L = 1ull << lx;
+    unsigned long long badr = 0, badc = 0, badp = 0;
+    const uint64_t tid = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    const uint64_t nth = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t y = tid; y < rows; y += nth) badr += rowinfo[2 * y + 1] != 0;
+    for (uint64_t x = tid; x < L; x += nth) badc += colsum[x] != 0;
+    // plaquettes: per (sublattice, row, word)
+    for (uint64_t i = tid; i < 2 * Q; i += nth) {
+        const int sub = (int)(i / Q);
+        const uint64_t r = i % Q;
+        const uint64_t y = r / Wr, j = r % Wr;
+        const uint64_t bt = sub ? 2 * Q : 0, bo = sub ? 0 : 2 * Q;
+        const int A = sub ^ (int)(y & 1);  // x parity of this sublattice in row y
+        const uint32_t a = sys[bt + y * Wr + j];          // s_x(x,y)
+        const uint32_t b = sys[bt + Q + y * Wr + j];      // s_y(x,y)
+        uint32_t c;                                        // s_y(x-1,y)
+        const uint32_t oy = sys[bo + Q + y * Wr + j];
+        if (A) c = oy;
+        else c = (oy << 1) | (sys[bo + Q + y * Wr + ((j + Wr - 1) & (Wr - 1))] >> 31);
+        const uint32_t d = sys[bo + ((y + rows - 1) & (rows - 1)) * Wr + j];  // s_x(x,y-1)
+        const uint32_t bad = ((a ^ c) ^ (b ^ d)) | ((a & c) ^ (b & d));
+        badp += __popc(bad);
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        badr += __shfl_xor_sync(0xffffffffu, badr, o);
+        badc += __shfl_xor_sync(0xffffffffu, badc, o);
+        badp += __shfl_xor_sync(0xffffffffu, badp, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicAdd(&rep[0], badr);
+        atomicAdd(&rep[1], badc);
+        atomicAdd(&rep[2], badp);
+    }
+}
+
+cudaError_t analysis_invariants(const uint32_t* d_sys, int lx, int ly, AnalysisScratch* s,
+                                int64_t rep[3], cudaStream_t st)
+{
+    const uint64_t rows = 1ull << ly, L = 1ull << lx;
+    int* colsum = nullptr;
+    cudaError_t e;
+    if ((e = cudaMallocAsync(&colsum, L * sizeof(int) + 64, st)) != cudaSuccess) return e;
+    unsigned long long* drep = reinterpret_cast<unsigned long long*>(colsum + L);
+    cudaMemsetAsync(colsum, 0, L * sizeof(int) + 64, st);
+    const int grid0 = (int)((rows * 32 + 255) / 256 < 4096 ? (rows * 32 + 255) / 256 : 4096);
+    rowinfo_kernel<<<grid0, 256, 0, st>>>(d_sys, lx, ly, s->rowinfo);
+    colsum_kernel<<<512, 256, 0, st>>>(d_sys, lx, ly, colsum);
+    invariants_kernel<<<1184, 256, 0, st>>>(d_sys, lx, ly, s->rowinfo, colsum, drep);
+    unsigned long long h[3] = {0, 0, 0};
+    cudaMemcpyAsync(h, drep, sizeof(h), cudaMemcpyDeviceToHost, st);
+    e = cudaStreamSynchronize(st);
+    cudaFreeAsync(colsum, st);
+    if (e == cudaSuccess) e = cudaGetLastError();
+    rep[0] = (int64_t)h[0];
+    rep[1] = (int64_t)h[1];
+    rep[2] = (int64_t)h[2];
+    return e;
+}
+
+}  // namespace kpzb

@@ -1,0 +1,491 @@
+// api.cu -- the C ABI (include/kpzb.h): handle lifecycle, MCS loop, push/pop, analysis.
+//
+// Mirrors Kpz::SchedulerService (kpz/schedulerService.h:73-255) and the GPU scheduler base
+// (kpz/schedulerBase.cu:35-99).  Differences by design: one CUDA stream per handle, no
+// busy-wait event loop, integer status codes instead of exceptions/exit, counter-based RNG
+// keyed by (seed, stream) instead of per-thread TinyMT/SLCG state.
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+
+#include "../../include/kpzb.h"
+#include "kpzb_api_internal.h"
+#include "kpzb_common.cuh"
+#include "kpzb_internal.h"
+
+namespace kpzb {
+thread_local std::string g_err;
+
+kpzb_status fail(kpzb_status s, const char* what)
+{
+    g_err = what;
+    return s;
+}
+
+kpzb_status cuda_fail(cudaError_t e, const char* where)
+{
+    g_err = std::string(where) + ": " + cudaGetErrorString(e);
+    return e == cudaErrorMemoryAllocation ? KPZB_ENOMEM : KPZB_ECUDA;
+}
+
+int sm_count_of(int device)
+{
+    int n = 148;
+    cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, device);
+    return n;
+}
+}  // namespace kpzb
+
+using namespace kpzb;
+
+struct kpzb_handle {
+    int lx = 0, ly = 0, dyn = 0, device = 0, sm_count = 148;
+    cudaStream_t st = nullptr;      // stream in use
+    cudaStream_t own_st = nullptr;  // stream created by the handle
+    uint32_t* d_sys = nullptr;   // internal layout: CBBIT (SCA, SCABIT) or LOCAL (DT)
+    uint32_t* d_tmp = nullptr;   // scratch lattice (transcoding, fused double buffer)
+    uint32_t* d_snap = nullptr;  // correlator snapshot, CBBIT
+    double snap_mean = 0.0;
+    bool has_snap = false;
+    uint64_t seed = 0;
+    uint32_t stream_id = 0;
+    double p = 1.0, q = 0.0;
+    uint64_t tdev = 0;
+    int fusion = 0;
+    bool count = false;
+    unsigned long long* d_counters = nullptr;
+    AnalysisScratch an{};
+    ScabitShape shape{};
+    DtState dt{};
+    size_t words() const { return (size_t)1 << (lx + ly - 4); }
+    int encoding() const { return dyn == KPZB_DYN_SCABIT ? KPZB_ENC_CBBIT : KPZB_ENC_LOCAL; }
+};
+
+#define KPZB_CHECK_H(h)                                              \
+    do {                                                             \
+        if (!(h)) return fail(KPZB_EINVAL, "null handle");           \
+        cudaError_t _e = cudaSetDevice((h)->device);                 \
+        if (_e != cudaSuccess) return cuda_fail(_e, "cudaSetDevice"); \
+    } while (0)
+
+#define KPZB_CU(call, where)                                   \
+    do {                                                       \
+        cudaError_t _e = (call);                               \
+        if (_e != cudaSuccess) return cuda_fail(_e, where);    \
+    } while (0)
+
+extern "C" const char* kpzb_last_error(void) { return g_err.c_str(); }
+extern "C" const char* kpzb_version(void) { return "kpzb200 1.0 (sm_100a)"; }
+
+static kpzb_status ensure_tmp(kpzb_handle* h)
+{
+    if (!h->d_tmp) KPZB_CU(cudaMalloc(&h->d_tmp, h->words() * 4), "cudaMalloc(tmp)");
+    return KPZB_OK;
+}
+
+extern "C" kpzb_status kpzb_create(kpzb_handle** out, int lx, int ly, int dynamics, int device)
+{
+    if (!out) return fail(KPZB_EINVAL, "null output pointer");
+    *out = nullptr;
+    if (dynamics < KPZB_DYN_SCA || dynamics > KPZB_DYN_DT) return fail(KPZB_EINVAL, "bad dynamics");
+    // lx >= 8: a quadrant row holds at least one 4-word Philox group; lx + ly >= 14: every
+    // launch is made of whole warps (the kernels' shuffles use full-warp masks)
+    if (lx < 8 || lx > 30 || ly < 2 || ly > 30 || lx + ly > 38 || lx + ly < 14)
+        return fail(KPZB_EINVAL,
+                    "lattice size out of range (8<=lx<=30, 2<=ly<=30, 14<=lx+ly<=38)");
+    if (dynamics == KPZB_DYN_DT && (lx < 10 || ly < 10))
+        return fail(KPZB_EINVAL, "DT needs lx, ly >= 10 (one double tile of 512x512 sites)");
+    int dev = device;
+    if (dev < 0) {
+        cudaError_t e = cudaGetDevice(&dev);
+        if (e != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
+    }
+    cudaError_t e = cudaSetDevice(dev);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaSetDevice");
+    kpzb_handle* h = new kpzb_handle();
+    h->lx = lx;
+    h->ly = ly;
+    h->dyn = dynamics;
+    h->device = dev;
+    h->sm_count = sm_count_of(dev);
+    h->shape = scabit_shape(lx, ly, h->sm_count);
+    auto bail = [&](kpzb_status s) {
+        kpzb_destroy(h);
+        return s;
+    };
+    if ((e = cudaStreamCreateWithFlags(&h->own_st, cudaStreamNonBlocking)) != cudaSuccess)
+        return bail(cuda_fail(e, "cudaStreamCreate"));
+    h->st = h->own_st;
+    if ((e = cudaMalloc(&h->d_sys, h->words() * 4)) != cudaSuccess)
+        return bail(cuda_fail(e, "cudaMalloc(lattice)"));
+    if ((e = cudaMalloc(&h->d_counters, 4 * sizeof(unsigned long long))) != cudaSuccess)
+        return bail(cuda_fail(e, "cudaMalloc(counters)"));
+    cudaMemsetAsync(h->d_counters, 0, 4 * sizeof(unsigned long long), h->st);
+    if ((e = analysis_alloc(&h->an, ly)) != cudaSuccess) return bail(cuda_fail(e, "analysis_alloc"));
+    if (dynamics == KPZB_DYN_DT) {
+        kpzb_status s = dt_init(&h->dt, lx, ly, h->sm_count);
+        if (s != KPZB_OK) return bail(s);
+    }
+    kpzb_status s = kpzb_init_homogeneous(h);
+    if (s != KPZB_OK) return bail(s);
+    if ((e = cudaStreamSynchronize(h->st)) != cudaSuccess) return bail(cuda_fail(e, "create sync"));
+    *out = h;
+    return KPZB_OK;
+}
+
+extern "C" kpzb_status kpzb_destroy(kpzb_handle* h)
+{
+    if (!h) return KPZB_OK;
+    cudaSetDevice(h->device);
+    if (h->st) cudaStreamSynchronize(h->st);
+    cudaFree(h->d_sys);
+    cudaFree(h->d_tmp);
+    cudaFree(h->d_snap);
+    cudaFree(h->d_counters);
+    if (h->an.rowinfo) analysis_free(&h->an);
+    dt_free(&h->dt);
+    if (h->own_st) cudaStreamDestroy(h->own_st);
+    delete h;
+    return KPZB_OK;
+}
+
+extern "C" kpzb_status kpzb_init_homogeneous(kpzb_handle* h)
+{
+    KPZB_CHECK_H(h);
+    // SCA keeps ENC_CBBIT internally; the flat start is the same surface in both encodings
+    const int internal = h->dyn == KPZB_DYN_DT ? KPZB_ENC_LOCAL : KPZB_ENC_CBBIT;
+    KPZB_CU(init_homogeneous_dev(h->d_sys, h->lx, h->ly, internal, h->st), "init_homogeneous");
+    return KPZB_OK;
+}
+
+extern "C" kpzb_status kpzb_set_pq(kpzb_handle* h, double p, double q)
+{
+    if (!h) return fail(KPZB_EINVAL, "null handle");
+    if (!(p >= 0.0 && p <= 1.0 && q >= 0.0 && q <= 1.0)) return fail(KPZB_EINVAL, "p, q must lie in [0,1]");
+    h->p = p;
+    h->q = q;
+    return KPZB_OK;
+}
+
+extern "C" kpzb_status kpzb_seed(kpzb_handle* h, uint64_t seed, uint32_t stream)
+{
+    if (!h) return fail(KPZB_EINVAL, "null handle");
+    h->seed = seed;
+    h->stream_id = stream;
+    h->tdev = 0;
+    return KPZB_OK;
+}
+
+extern "C" kpzb_status kpzb_set_fusion(kpzb_handle* h, int mcs_per_pass)
+{
+    if (!h) return fail(KPZB_EINVAL, "null handle");
+    if (mcs_per_pass < 0 || mcs_per_pass > 64) return fail(KPZB_EINVAL, "fusion must be in [0,64]");
+    h->fusion = mcs_per_pass;
+    return KPZB_OK;
+}
+
+extern "C" kpzb_status kpzb_get_fusion(const kpzb_handle* h, int* mcs_per_pass)
+{
+    if (!h || !mcs_per_pass) return fail(KPZB_EINVAL, "null argument");
+    if (h->dyn == KPZB_DYN_DT) {
+        *mcs_per_pass = 1;
+        return KPZB_OK;
+    }
+    int k = h->fusion ? h->fusion : auto_fusion(h->lx, h->ly);
+    if (k > 1 && !scabit_fused_shape(h->lx, h->ly, k, h->sm_count, 0).ok) k = 1;
+    *mcs_per_pass = k;
+    return KPZB_OK;
+}
+
+static uint64_t thresh_of(double p)
+{
+    if (!(p > 0.0)) return 0;
+    if (p >= 1.0) return 1ull << 32;
+    double t = std::ceil(p * 4294967296.0);
+    if (t >= 4294967296.0) return 1ull << 32;
+    return (uint64_t)t;
+}
+
+static kpzb_status enqueue_sca(kpzb_handle* h, int n)
+{
+    const uint64_t Tp = thresh_of(h->p), Tq = thresh_of(h->q);
+    unsigned long long* cnt = h->count ? h->d_counters : nullptr;
+    int done = 0;
+    int k = h->fusion;
+    if (k == 0) k = auto_fusion(h->lx, h->ly);
+    if (k > 1) {
+        FusedShape fs = scabit_fused_shape(h->lx, h->ly, k, h->sm_count, 0);
+        if (fs.ok) {
+            kpzb_status s = ensure_tmp(h);
+            if (s != KPZB_OK) return s;
+            while (n - done >= k) {
+                KPZB_CU(scabit_fused(h->d_sys, h->d_tmp, h->lx, h->ly, (uint32_t)(h->tdev + done),
+                                     h->seed, h->stream_id, Tp, Tq, fs, cnt,
+                                     reinterpret_cast<unsigned int*>(h->d_counters + 2), h->st),
+                        "scabit_fused");
+                std::swap(h->d_sys, h->d_tmp);
+                done += k;
+            }
+        }
+    }
+    for (; done < n; ++done) {
+        const uint64_t t = h->tdev + done;
+        for (int sg = 0; sg < 2; ++sg)
+            KPZB_CU(scabit_half(h->d_sys, h->lx, h->ly, sg, (uint32_t)(2 * t + sg), h->seed,
+                                h->stream_id, Tp, Tq, h->shape, cnt, h->st),
+                    "scabit_half");
+    }
+    return KPZB_OK;
+}
+
+extern "C" kpzb_status kpzb_mcs_async(kpzb_handle* h, int n)
+{
+    KPZB_CHECK_H(h);
+    if (n < 0) return fail(KPZB_EINVAL, "negative MCS count");
+    if (n == 0) return KPZB_OK;
+    if (h->tdev + (uint64_t)n >= (1ull << 31)) return fail(KPZB_EINVAL, "device MCS counter limit 2^31");
+    kpzb_status s;
+    if (h->dyn == KPZB_DYN_DT)
+        s = dt_enqueue(&h->dt, h->d_sys, h->lx, h->ly, h->tdev, n, h->p, h->q, h->seed, h->stream_id,
+                       h->st);
+    else
+        s = enqueue_sca(h, n);
+    if (s != KPZB_OK) return s;
+    h->tdev += (uint64_t)n;
+    return KPZB_OK;
+}
+
+extern "C" kpzb_status kpzb_join(kpzb_handle* h)
+{
+    KPZB_CHECK_H(h);
+    unsigned int flag = 0;
+    KPZB_CU(cudaMemcpyAsync(&flag, h->d_counters + 2, sizeof flag, cudaMemcpyDeviceToHost, h->st),
+            "join flag");
+    KPZB_CU(cudaStreamSynchronize(h->st), "join");
+    KPZB_CU(cudaGetLastError(), "join");
+    if (flag) {
+        cudaMemsetAsync(h->d_counters + 2, 0, sizeof(unsigned long long), h->st);
+        cudaStreamSynchronize(h->st);
+        return fail(KPZB_ETIMEOUT, "a bounded device wait (TMA mbarrier) expired");
+    }
+    return KPZB_OK;
+}
+
+extern "C" kpzb_status kpzb_mcs(kpzb_handle* h, int n)
+{
+    kpzb_status s = kpzb_mcs_async(h, n);
+    if (s != KPZB_OK) return s;
+    return kpzb_join(h);
+}
+
+extern "C" size_t kpzb_size_words(const kpzb_handle* h) { return h ? h->words() : 0; }
+extern "C" int kpzb_encoding(const kpzb_handle* h) { return h ? h->encoding() : -1; }
+
+static kpzb_status push_from(kpzb_handle* h, const uint32_t* src, cudaMemcpyKind kind)
+{
+    if (h->dyn == KPZB_DYN_SCA) {
+        kpzb_status s = ensure_tmp(h);
+        if (s != KPZB_OK) return s;
+        KPZB_CU(cudaMemcpyAsync(h->d_tmp, src, h->words() * 4, kind, h->st), "push copy");
+        KPZB_CU(local_to_cbbit_dev(h->d_tmp, h->d_sys, h->lx, h->ly, h->st), "local_to_cbbit");
+    } else {
+        KPZB_CU(cudaMemcpyAsync(h->d_sys, src, h->words() * 4, kind, h->st), "push copy");
+    }
+    KPZB_CU(cudaStreamSynchronize(h->st), "push sync");
+    return KPZB_OK;
+}
+
+static kpzb_status pop_to(kpzb_handle* h, uint32_t* dst, cudaMemcpyKind kind)
+{
+    if (h->dyn == KPZB_DYN_SCA) {
+        kpzb_status s = ensure_tmp(h);
+        if (s != KPZB_OK) return s;
+        KPZB_CU(cbbit_to_local_dev(h->d_sys, h->d_tmp, h->lx, h->ly, h->st), "cbbit_to_local");
+        KPZB_CU(cudaMemcpyAsync(dst, h->d_tmp, h->words() * 4, kind, h->st), "pop copy");
+    } else {
+        KPZB_CU(cudaMemcpyAsync(dst, h->d_sys, h->words() * 4, kind, h->st), "pop copy");
+    }
+    KPZB_CU(cudaStreamSynchronize(h->st), "pop sync");
+    return KPZB_OK;
+}
+
+extern "C" kpzb_status kpzb_push(kpzb_handle* h, const uint32_t* words)
+{
+    KPZB_CHECK_H(h);
+    if (!words) return fail(KPZB_EINVAL, "null buffer");
+    return push_from(h, words, cudaMemcpyHostToDevice);
+}
+extern "C" kpzb_status kpzb_pop(kpzb_handle* h, uint32_t* words)
+{
+    KPZB_CHECK_H(h);
+    if (!words) return fail(KPZB_EINVAL, "null buffer");
+    return pop_to(h, words, cudaMemcpyDeviceToHost);
+}
+extern "C" kpzb_status kpzb_push_device(kpzb_handle* h, const uint32_t* d_words)
+{
+    KPZB_CHECK_H(h);
+    if (!d_words) return fail(KPZB_EINVAL, "null buffer");
+    return push_from(h, d_words, cudaMemcpyDeviceToDevice);
+}
+extern "C" kpzb_status kpzb_pop_device(kpzb_handle* h, uint32_t* d_words)
+{
+    KPZB_CHECK_H(h);
+    if (!d_words) return fail(KPZB_EINVAL, "null buffer");
+    return pop_to(h, d_words, cudaMemcpyDeviceToDevice);
+}
+
+// CBBIT view of the current lattice (DT keeps ENC_LOCAL and is transcoded into d_tmp).
+static kpzb_status cbbit_view(kpzb_handle* h, const uint32_t** view)
+{
+    if (h->dyn != KPZB_DYN_DT) {
+        *view = h->d_sys;
+        return KPZB_OK;
+    }
+    kpzb_status s = ensure_tmp(h);
+    if (s != KPZB_OK) return s;
+    KPZB_CU(local_to_cbbit_dev(h->d_sys, h->d_tmp, h->lx, h->ly, h->st), "local_to_cbbit");
+    *view = h->d_tmp;
+    return KPZB_OK;
+}
+
+static void fill_roughness(const MomentsOut& m, int lx, int ly, double out[8], long double* h0)
+{
+    const long double N = (long double)((uint64_t)1 << (lx + ly));
+    long double h[7];
+    h[0] = (long double)m.s1 / N;
+    h[1] = (long double)m.s2 / N;
+    for (int k = 0; k < 5; ++k) h[2 + k] = (long double)m.s3to7[k] / N;
+    out[0] = (double)(h[1] - h[0] * h[0]);
+    for (int k = 0; k < 7; ++k) out[1 + k] = (double)h[k];
+    if (h0) *h0 = h[0];
+}
+
+extern "C" kpzb_status kpzb_roughness(kpzb_handle* h, double out[8])
+{
+    KPZB_CHECK_H(h);
+    if (!out) return fail(KPZB_EINVAL, "null output");
+    const uint32_t* v;
+    kpzb_status s = cbbit_view(h, &v);
+    if (s != KPZB_OK) return s;
+    MomentsOut m;
+    KPZB_CU(analysis_moments(v, nullptr, h->lx, h->ly, &h->an, &m, h->st), "roughness");
+    fill_roughness(m, h->lx, h->ly, out, nullptr);
+    return KPZB_OK;
+}
+
+extern "C" kpzb_status kpzb_height_sums(kpzb_handle* h, int64_t s12[2], int64_t hminmax[2])
+{
+    KPZB_CHECK_H(h);
+    if (!s12 || !hminmax) return fail(KPZB_EINVAL, "null output");
+    const uint32_t* v;
+    kpzb_status s = cbbit_view(h, &v);
+    if (s != KPZB_OK) return s;
+    MomentsOut m;
+    KPZB_CU(analysis_moments(v, nullptr, h->lx, h->ly, &h->an, &m, h->st), "height sums");
+    s12[0] = m.s1;
+    s12[1] = m.s2;
+    hminmax[0] = m.hmin;
+    hminmax[1] = m.hmax;
+    return KPZB_OK;
+}
+
+extern "C" kpzb_status kpzb_corr_tag(kpzb_handle* h, double out[8])
+{
+    KPZB_CHECK_H(h);
+    const uint32_t* v;
+    kpzb_status s = cbbit_view(h, &v);
+    if (s != KPZB_OK) return s;
+    if (!h->d_snap) KPZB_CU(cudaMalloc(&h->d_snap, h->words() * 4), "cudaMalloc(snapshot)");
+    KPZB_CU(cudaMemcpyAsync(h->d_snap, v, h->words() * 4, cudaMemcpyDeviceToDevice, h->st), "snapshot");
+    MomentsOut m;
+    KPZB_CU(analysis_moments(h->d_snap, nullptr, h->lx, h->ly, &h->an, &m, h->st), "snapshot moments");
+    double r[8];
+    long double h0;
+    fill_roughness(m, h->lx, h->ly, r, &h0);
+    h->snap_mean = (double)h0;
+    h->has_snap = true;
+    if (out) memcpy(out, r, sizeof r);
+    return KPZB_OK;
+}
+
+extern "C" kpzb_status kpzb_correlate(kpzb_handle* h, double out[10])
+{
+    KPZB_CHECK_H(h);
+    if (!out) return fail(KPZB_EINVAL, "null output");
+    if (!h->has_snap) return fail(KPZB_ESTATE, "no correlator snapshot (call kpzb_corr_tag first)");
+    const uint32_t* v;
+    kpzb_status s = cbbit_view(h, &v);
+    if (s != KPZB_OK) return s;
+    MomentsOut m;
+    KPZB_CU(analysis_moments(v, h->d_snap, h->lx, h->ly, &h->an, &m, h->st), "correlate");
+    long double h0;
+    fill_roughness(m, h->lx, h->ly, out, &h0);
+    const long double N = (long double)((uint64_t)1 << (h->lx + h->ly));
+    out[8] = (double)((long double)(double)m.cross / N - h0 * (long double)h->snap_mean);
+    out[9] = (double)((long double)m.agree / N / 2.0L);
+    return KPZB_OK;
+}
+
+extern "C" kpzb_status kpzb_get_mcs(const kpzb_handle* h, uint64_t* device_mcs)
+{
+    if (!h || !device_mcs) return fail(KPZB_EINVAL, "null argument");
+    *device_mcs = h->tdev;
+    return KPZB_OK;
+}
+extern "C" kpzb_status kpzb_set_mcs(kpzb_handle* h, uint64_t device_mcs)
+{
+    if (!h) return fail(KPZB_EINVAL, "null handle");
+    if (device_mcs >= (1ull << 31)) return fail(KPZB_EINVAL, "device MCS counter limit 2^31");
+    h->tdev = device_mcs;
+    return KPZB_OK;
+}
+
+extern "C" kpzb_status kpzb_enable_counters(kpzb_handle* h, int on)
+{
+    if (!h) return fail(KPZB_EINVAL, "null handle");
+    h->count = on != 0;
+    return KPZB_OK;
+}
+
+extern "C" kpzb_status kpzb_counters(kpzb_handle* h, int64_t dep_des[2], int reset)
+{
+    KPZB_CHECK_H(h);
+    if (!dep_des) return fail(KPZB_EINVAL, "null output");
+    unsigned long long c[2];
+    KPZB_CU(cudaMemcpyAsync(c, h->d_counters, sizeof c, cudaMemcpyDeviceToHost, h->st), "counters");
+    if (reset) KPZB_CU(cudaMemsetAsync(h->d_counters, 0, sizeof c, h->st), "counters reset");
+    KPZB_CU(cudaStreamSynchronize(h->st), "counters sync");
+    dep_des[0] = (int64_t)c[0];
+    dep_des[1] = (int64_t)c[1];
+    return KPZB_OK;
+}
+
+extern "C" kpzb_status kpzb_check_invariants(kpzb_handle* h, int64_t rep[3])
+{
+    KPZB_CHECK_H(h);
+    if (!rep) return fail(KPZB_EINVAL, "null output");
+    const uint32_t* v;
+    kpzb_status s = cbbit_view(h, &v);
+    if (s != KPZB_OK) return s;
+    KPZB_CU(analysis_invariants(v, h->lx, h->ly, &h->an, rep, h->st), "invariants");
+    return KPZB_OK;
+}
+
+extern "C" kpzb_status kpzb_device_ptr(kpzb_handle* h, uint32_t** d_words, size_t* nwords)
+{
+    if (!h || !d_words) return fail(KPZB_EINVAL, "null argument");
+    *d_words = h->d_sys;
+    if (nwords) *nwords = h->words();
+    return KPZB_OK;
+}
+
+extern "C" void* kpzb_stream(kpzb_handle* h) { return h ? (void*)h->st : nullptr; }
+
+extern "C" kpzb_status kpzb_set_stream(kpzb_handle* h, void* stream)
+{
+    KPZB_CHECK_H(h);
+    KPZB_CU(cudaStreamSynchronize(h->st), "set_stream sync");
+    h->st = stream ? (cudaStream_t)stream : h->own_st;
+    return KPZB_OK;
+}

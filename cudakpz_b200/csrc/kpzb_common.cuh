@@ -1,0 +1,128 @@
+// kpzb_common.cuh -- device helpers shared by the kpzb kernels (sm_100a).
+//
+// Counter-based random stream (the one the CPU oracle restates):
+//   Philox4x32-10 (Salmon et al., SC'11), key = (seed lo, seed hi),
+//   counter = (qword >> 2, step, plane | tag << 8, stream); output word qword & 3.
+//   qword: word index inside an ENC_CBBIT quadrant; step = 2*t + sublattice;
+//   plane k supplies bit (31-k) of each site's 32-bit uniform u.
+// Decision: local minimum flips iff u < T(p), local maximum iff u < T(q),
+//   T(x) = min(2^32, ceil(x * 2^32)).  Evaluated bit-serially from the MSB
+//   plane, 32 sites per word at once, stopping when no site is undecided.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace kpzb {
+
+constexpr uint32_t TAG_SCA = 1u;
+constexpr uint32_t TAG_DT = 2u;
+constexpr uint32_t TAG_DT_ORIGIN = 3u;
+
+struct Key {
+    uint32_t k0, k1;
+};
+
+__host__ __device__ __forceinline__ Key make_key(uint64_t seed)
+{
+    return Key{(uint32_t)seed, (uint32_t)(seed >> 32)};
+}
+
+// Philox4x32-10 round function and Weyl key schedule (SC'11, sec. 3.2).
+__device__ __forceinline__ uint4 philox4x32_10(uint4 c, Key k)
+{
+    uint32_t k0 = k.k0, k1 = k.k1;
+#pragma unroll
+    for (int r = 0; r < 10; ++r) {
+        if (r) {
+            k0 += 0x9E3779B9u;
+            k1 += 0xBB67AE85u;
+        }
+        const uint32_t lo0 = 0xD2511F53u * c.x;
+        const uint32_t hi0 = __umulhi(0xD2511F53u, c.x);
+        const uint32_t lo1 = 0xCD9E8D57u * c.z;
+        const uint32_t hi1 = __umulhi(0xCD9E8D57u, c.z);
+        c = make_uint4(hi1 ^ c.y ^ k0, lo1, hi0 ^ c.w ^ k1, lo0);
+    }
+    return c;
+}
+
+// Threshold as (flag, low 32 bits): always = T >= 2^32; never = T == 0;
+// planes = number of MSB planes that can decide (32 - ctz(T)).
+struct Thresh {
+    uint32_t t;      // low 32 bits of T (T < 2^32 when !always)
+    int planes;      // 0 when always or never
+    bool always;
+};
+
+__host__ __device__ inline Thresh make_thresh(uint64_t T)
+{
+    Thresh r;
+    r.always = T >= (1ull << 32);
+    r.t = r.always ? 0u : (uint32_t)T;
+    int planes = 0;
+    if (!r.always && r.t) {
+        uint32_t v = r.t;
+        int ctz = 0;
+        while (!(v & 1u)) {
+            v >>= 1;
+            ++ctz;
+        }
+        planes = 32 - ctz;
+    }
+    r.planes = planes;
+    return r;
+}
+
+// Four-word decision for the 128 sites of one Philox group (qgroup = qword >> 2).
+// cp: local-minimum candidates, cq: local-maximum candidates. Returns the flip mask.
+__device__ __forceinline__ uint4 decide4(uint4 cp, uint4 cq, Thresh tp, Thresh tq, Key key,
+                                         uint32_t qgroup, uint32_t step, uint32_t stream)
+{
+    uint4 ltp, eqp, ltq, eqq;
+    if (tp.always) {
+        ltp = cp;
+        eqp = make_uint4(0, 0, 0, 0);
+    } else {
+        ltp = make_uint4(0, 0, 0, 0);
+        eqp = tp.planes ? cp : make_uint4(0, 0, 0, 0);
+    }
+    if (tq.always) {
+        ltq = cq;
+        eqq = make_uint4(0, 0, 0, 0);
+    } else {
+        ltq = make_uint4(0, 0, 0, 0);
+        eqq = tq.planes ? cq : make_uint4(0, 0, 0, 0);
+    }
+    const int kmax = max(tp.planes, tq.planes);
+    for (int k = 0; k < kmax; ++k) {
+        const uint32_t any = eqp.x | eqp.y | eqp.z | eqp.w | eqq.x | eqq.y | eqq.z | eqq.w;
+        if (!any) break;
+        const uint4 r = philox4x32_10(make_uint4(qgroup, step, (uint32_t)k | (TAG_SCA << 8), stream), key);
+        const uint32_t bp = (tp.t >> (31 - k)) & 1u;
+        const uint32_t bq = (tq.t >> (31 - k)) & 1u;
+        // bit of T is 1: sites with u-bit 0 are below T (decided), u-bit 1 stay equal.
+        // bit of T is 0: sites with u-bit 1 are above T (drop), u-bit 0 stay equal.
+        if (bp) {
+            ltp.x |= eqp.x & ~r.x; ltp.y |= eqp.y & ~r.y; ltp.z |= eqp.z & ~r.z; ltp.w |= eqp.w & ~r.w;
+            eqp.x &= r.x; eqp.y &= r.y; eqp.z &= r.z; eqp.w &= r.w;
+        } else {
+            eqp.x &= ~r.x; eqp.y &= ~r.y; eqp.z &= ~r.z; eqp.w &= ~r.w;
+        }
+        if (bq) {
+            ltq.x |= eqq.x & ~r.x; ltq.y |= eqq.y & ~r.y; ltq.z |= eqq.z & ~r.z; ltq.w |= eqq.w & ~r.w;
+            eqq.x &= r.x; eqq.y &= r.y; eqq.z &= r.z; eqq.w &= r.w;
+        } else {
+            eqq.x &= ~r.x; eqq.y &= ~r.y; eqq.z &= ~r.z; eqq.w &= ~r.w;
+        }
+        if (k + 1 >= tp.planes) eqp = make_uint4(0, 0, 0, 0);
+        if (k + 1 >= tq.planes) eqq = make_uint4(0, 0, 0, 0);
+    }
+    return make_uint4(ltp.x | ltq.x, ltp.y | ltq.y, ltp.z | ltq.z, ltp.w | ltq.w);
+}
+
+__device__ __forceinline__ uint4 operator^(uint4 a, uint4 b)
+{
+    return make_uint4(a.x ^ b.x, a.y ^ b.y, a.z ^ b.z, a.w ^ b.w);
+}
+
+}  // namespace kpzb

@@ -1,0 +1,64 @@
+// kpzb_internal.h -- host-side declarations shared by the kpzb translation units.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace kpzb {
+
+struct ScabitShape {
+    int TX, TY, grid;
+};
+
+ScabitShape scabit_shape(int lx, int ly, int sm_count);
+cudaError_t scabit_half(uint32_t* d_sys, int lx, int ly, int sigma, uint32_t step, uint64_t seed,
+                        uint32_t stream_id, uint64_t Tp, uint64_t Tq, const ScabitShape& sh,
+                        unsigned long long* d_counters, cudaStream_t st);
+
+// Temporal-blocked SCABit: k MCS (2k half-steps) per HBM pass over a band of rows.
+struct FusedShape {
+    int band;      // output rows per CTA band
+    int halo;      // halo rows each side (= 2 * mcs_per_pass)
+    int mcs;       // MCS per pass
+    int threads;   // threads per CTA
+    size_t smem;   // dynamic shared memory bytes
+    int grid;
+    bool ok;
+};
+FusedShape scabit_fused_shape(int lx, int ly, int mcs_per_pass, int sm_count, size_t smem_optin);
+cudaError_t scabit_fused(const uint32_t* d_src, uint32_t* d_dst, int lx, int ly, uint32_t t0,
+                         uint64_t seed, uint32_t stream_id, uint64_t Tp, uint64_t Tq,
+                         const FusedShape& sh, unsigned long long* d_counters, unsigned int* d_err,
+                         cudaStream_t st);
+
+// codec / init
+cudaError_t init_homogeneous_dev(uint32_t* d, int lx, int ly, int encoding, cudaStream_t st);
+cudaError_t local_to_cbbit_dev(const uint32_t* local, uint32_t* cbbit, int lx, int ly, cudaStream_t st);
+cudaError_t cbbit_to_local_dev(const uint32_t* cbbit, uint32_t* local, int lx, int ly, cudaStream_t st);
+
+// analysis on ENC_CBBIT lattices
+struct AnalysisScratch {
+    int32_t* rowinfo;      // 2 * rows: y-slope step at x=0 and x-slope row sum
+    int64_t* rowstart;     // rows: height at the start of each row walk
+    unsigned long long* acc;  // accumulators (see analysis.cu)
+    size_t rows_cap;
+};
+cudaError_t analysis_alloc(AnalysisScratch* s, int ly);
+void analysis_free(AnalysisScratch* s);
+// out_i64[0..2]: S1, S2, hmin/hmax packed; out_f64[0..4]: S3..S7; corr outputs optional
+struct MomentsOut {
+    int64_t s1, s2;
+    double s3to7[5];
+    int64_t hmin, hmax;
+    int64_t cross;   // sum h_sys * h_snap (correlate mode)
+    int64_t agree;   // sum of +-1 slope agreements (correlate mode)
+    int64_t snap_s1; // sum h_snap (correlate mode)
+};
+cudaError_t analysis_moments(const uint32_t* d_sys, const uint32_t* d_snap, int lx, int ly,
+                             AnalysisScratch* s, MomentsOut* out, cudaStream_t st);
+cudaError_t analysis_heights(const uint32_t* d_sys, int lx, int ly, AnalysisScratch* s,
+                             int32_t* d_heights, cudaStream_t st);
+// invariants: rep[0] bad rows, rep[1] bad columns, rep[2] bad plaquettes
+cudaError_t analysis_invariants(const uint32_t* d_sys, int lx, int ly, AnalysisScratch* s,
+                                int64_t rep[3], cudaStream_t st);
+
+}  // namespace kpzb

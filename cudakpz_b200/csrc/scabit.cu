@@ -1,0 +1,437 @@
+// scabit.cu -- bit-vectorised SCA half-step on the ENC_CBBIT lattice (sm_100a).
+//
+// Reference behaviour: kpz/kpzSCABit.cu:112-290 (kernel), kpz/kpzSCABitCores.cu:69-74,139-145
+// (mask algebra), kpz/schedulerSCABit.cu:46-73 (sublattice 0 then 1 per MCS).
+//
+// Layout (kpz/systemSize.h:143-165): four quadrants of Q = N/64 words,
+//   [sub0.X | sub0.Y | sub1.X | sub1.Y], row y of a quadrant is Wr = L/64 words,
+//   bit b of word j holds site x = 2*(32*j+b) + ((sigma ^ y) & 1).
+// A half-step on sublattice sigma updates every "this" site of row y from
+//   thisX, thisY (row y), otherX (row y; shifted right by one bit with carry from the
+//   next word when sigma != (y & 1)), otherY (row y+1), and xors the flip mask into all
+//   four (otherX with the inverse shift).  Rows are independent within a half-step.
+//
+// Work split: a CTA owns TY rows at a time; TX threads cover a row segment of 4*TX words
+// with 128-bit loads/stores (one Philox group of 4 words per thread).  Rows longer than
+// one segment are walked segment by segment with the one-bit mask carry kept in shared
+// memory; the carry out of the last word wraps into bit 0 of word 0 (periodic x).
+#include "kpzb_api_internal.h"
+#include "kpzb_common.cuh"
+#include "kpzb_internal.h"
+
+namespace kpzb {
+
+constexpr int SCABIT_THREADS = 256;
+
+template <bool COUNT>
+__global__ void __launch_bounds__(SCABIT_THREADS)
+scabit_half_kernel(uint32_t* __restrict__ sys, int lx, int ly, int sigma, uint32_t step, Key key,
+                   uint32_t stream, Thresh tp, Thresh tq, int TX, int TY,
+                   unsigned long long* __restrict__ counters)
+{
+    __shared__ uint32_t nxt_s[SCABIT_THREADS];
+    __shared__ uint32_t carry_s[2][SCABIT_THREADS];
+
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    const int lin = ty * TX + tx;
+    const uint64_t Wr = 1ull << (lx - 6);
+    const uint64_t Q = 1ull << (lx + ly - 6);
+    const uint64_t rows = 1ull << ly;
+    const int nseg = (int)(Wr / (4ull * TX));
+    const uint64_t rowgroups = rows / TY;
+
+    const uint64_t bthisX = sigma ? 2 * Q : 0;
+    const uint64_t bthisY = bthisX + Q;
+    const uint64_t botherX = sigma ? 0 : 2 * Q;
+    const uint64_t botherY = botherX + Q;
+
+    unsigned long long ndep = 0, ndes = 0;
+
+    for (uint64_t rg = blockIdx.x; rg < rowgroups; rg += gridDim.x) {
+        const uint64_t y = rg * TY + ty;
+        const bool shifted = sigma != (int)(y & 1);
+        const uint64_t roff = y * Wr;
+        const uint64_t roff1 = ((y + 1) & (rows - 1)) * Wr;
+        for (int seg = 0; seg < nseg; ++seg) {
+            const uint64_t wi = (uint64_t)seg * 4 * TX + 4 * (uint64_t)tx;
+            uint4* ptX = reinterpret_cast<uint4*>(sys + bthisX + roff + wi);
+            uint4* ptY = reinterpret_cast<uint4*>(sys + bthisY + roff + wi);
+            uint4* poX = reinterpret_cast<uint4*>(sys + botherX + roff + wi);
+            uint4* poY = reinterpret_cast<uint4*>(sys + botherY + roff1 + wi);
+            uint4 tX = *ptX, tY = *ptY, oX = *poX, oY = *poY;
+            nxt_s[lin] = oX.x;
+            __syncthreads();
+            uint4 xX = oX;
+            if (shifted) {
+                uint32_t nb;
+                if (tx + 1 < TX) nb = nxt_s[lin + 1];
+                else nb = sys[botherX + roff + ((wi + 4) & (Wr - 1))];
+                xX.x = (oX.x >> 1) | (oX.y << 31);
+                xX.y = (oX.y >> 1) | (oX.z << 31);
+                xX.z = (oX.z >> 1) | (oX.w << 31);
+                xX.w = (oX.w >> 1) | (nb << 31);
+            }
+            // deposition: this site's slopes both 0, right-x and up-y slopes both 1;
+            // desorption: the complement (kpz/kpzSCABitCores.cu:69-74,139-145)
+            uint4 cp, cq;
+            cp.x = ~(tX.x | tY.x) & xX.x & oY.x;
+            cp.y = ~(tX.y | tY.y) & xX.y & oY.y;
+            cp.z = ~(tX.z | tY.z) & xX.z & oY.z;
+            cp.w = ~(tX.w | tY.w) & xX.w & oY.w;
+            cq.x = tX.x & tY.x & ~(xX.x | oY.x);
+            cq.y = tX.y & tY.y & ~(xX.y | oY.y);
+            cq.z = tX.z & tY.z & ~(xX.z | oY.z);
+            cq.w = tX.w & tY.w & ~(xX.w | oY.w);
+            const uint4 m = decide4(cp, cq, tp, tq, key, (uint32_t)((roff + wi) >> 2), step, stream);
+            if (COUNT) {
+                ndep += __popc(m.x & cp.x) + __popc(m.y & cp.y) + __popc(m.z & cp.z) + __popc(m.w & cp.w);
+                ndes += __popc(m.x & cq.x) + __popc(m.y & cq.y) + __popc(m.z & cq.z) + __popc(m.w & cq.w);
+            }
+            tX = tX ^ m;
+            tY = tY ^ m;
+            oY = oY ^ m;
+            carry_s[seg & 1][lin] = m.w >> 31;
+            __syncthreads();
+            if (shifted) {
+                uint32_t cin = 0;
+                if (tx > 0) cin = carry_s[seg & 1][lin - 1];
+                else if (seg > 0) cin = carry_s[(seg - 1) & 1][lin + TX - 1];
+                oX.x ^= (m.x << 1) | cin;
+                oX.y ^= (m.y << 1) | (m.x >> 31);
+                oX.z ^= (m.z << 1) | (m.y >> 31);
+                oX.w ^= (m.w << 1) | (m.z >> 31);
+            } else {
+                oX = oX ^ m;
+            }
+            *ptX = tX;
+            *ptY = tY;
+            *poX = oX;
+            *poY = oY;
+        }
+        if (shifted && tx == 0) {
+            // periodic wrap: the last word's bit-31 flip lands on bit 0 of word 0
+            if (carry_s[(nseg - 1) & 1][lin + TX - 1]) sys[botherX + roff] ^= 1u;
+        }
+    }
+    if (COUNT) {
+        for (int o = 16; o > 0; o >>= 1) {
+            ndep += __shfl_xor_sync(0xffffffffu, ndep, o);
+            ndes += __shfl_xor_sync(0xffffffffu, ndes, o);
+        }
+        if ((lin & 31) == 0 && (ndep | ndes)) {
+            atomicAdd(&counters[0], ndep);
+            atomicAdd(&counters[1], ndes);
+        }
+    }
+}
+
+ScabitShape scabit_shape(int lx, int ly, int sm_count)
+{
+    ScabitShape s;
+    const uint64_t Wr = 1ull << (lx - 6);
+    uint64_t tx = Wr / 4;
+    if (tx > SCABIT_THREADS) tx = SCABIT_THREADS;
+    uint64_t ty = SCABIT_THREADS / tx;
+    const uint64_t rows = 1ull << ly;
+    if (ty > rows) ty = rows;
+    s.TX = (int)tx;
+    s.TY = (int)ty;
+    const uint64_t rowgroups = rows / ty;
+    uint64_t grid = (uint64_t)sm_count * 8;
+    if (grid > rowgroups) grid = rowgroups;
+    s.grid = (int)grid;
+    return s;
+}
+
+cudaError_t scabit_half(uint32_t* d_sys, int lx, int ly, int sigma, uint32_t step, uint64_t seed,
+                        uint32_t stream_id, uint64_t Tp, uint64_t Tq, const ScabitShape& sh,
+                        unsigned long long* d_counters, cudaStream_t st)
+{
+    const Key key = make_key(seed);
+    const Thresh tp = make_thresh(Tp), tq = make_thresh(Tq);
+    dim3 block(sh.TX, sh.TY);
+    if (d_counters)
+        scabit_half_kernel<true><<<sh.grid, block, 0, st>>>(d_sys, lx, ly, sigma, step, key,
+                                                            stream_id, tp, tq, sh.TX, sh.TY,
+                                                            d_counters);
+    else
+        scabit_half_kernel<false><<<sh.grid, block, 0, st>>>(d_sys, lx, ly, sigma, step, key,
+                                                             stream_id, tp, tq, sh.TX, sh.TY,
+                                                             nullptr);
+    return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------------
+// Temporal blocking.  A CTA loads a band of R = B + 4k full-width rows of all four
+// quadrants into shared memory with TMA bulk copies (cp.async.bulk, local HBM only),
+// runs 2k half-steps there, and writes its B middle rows to the destination buffer.
+// Half-step h updates local rows [h, R-1-h); after 2k half-steps rows [2k, R-2k) are
+// exact (each half-step invalidates at most one row per side), so neighbouring bands
+// overlap by 2k halo rows on each side.  The one-bit carry of shifted rows crosses
+// thread boundaries only in the first word of each 4-word group, which is updated
+// with shared-memory atomicXor; all other words have a single writer.
+// ---------------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t smem_u32(const void* p)
+{
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
+                 "r"(bytes)
+                 : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity)
+{
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar)
+{
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+            smem_u32(dst)),
+        "l"(src), "r"(bytes), "r"(smem_u32(bar))
+        : "memory");
+}
+
+__device__ __forceinline__ void bulk_s2g(void* dst, const void* src, uint32_t bytes)
+{
+    asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(dst),
+                 "r"(smem_u32(src)), "r"(bytes)
+                 : "memory");
+}
+
+constexpr int FUSED_THREADS = 512;
+// bounded spin on the TMA mbarrier: ~2^26 polls (far above any real copy time)
+constexpr uint32_t MBAR_SPIN_LIMIT = 1u << 26;
+
+template <bool COUNT>
+__global__ void __launch_bounds__(FUSED_THREADS)
+scabit_fused_kernel(const uint32_t* __restrict__ src, uint32_t* __restrict__ dst, int lx, int ly,
+                    uint32_t t0, Key key, uint32_t stream, Thresh tp, Thresh tq, int B, int k,
+                    unsigned long long* __restrict__ counters, unsigned int* __restrict__ err)
+{
+    extern __shared__ __align__(128) uint32_t smem[];
+    __shared__ __align__(8) uint64_t bar;
+    __shared__ int abort_flag;
+
+    const uint64_t Wr = 1ull << (lx - 6);
+    const uint64_t Q = 1ull << (lx + ly - 6);
+    const int64_t rows = 1ll << ly;
+    const int H = 2 * k;
+    const int R = B + 2 * H;
+    const int G = (int)(Wr / 4);
+    const uint64_t qsz = (uint64_t)R * Wr;  // words per quadrant slab in smem
+    const int64_t y0 = (int64_t)blockIdx.x * B;
+    const int Bc = (int)(rows - y0 < B ? rows - y0 : B);  // rows this CTA writes
+    const int64_t ylo = y0 - H;                       // global row of local row 0
+
+    if (threadIdx.x == 0) {
+        abort_flag = 0;
+        mbar_init(&bar, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const uint32_t total = (uint32_t)(4ull * qsz * 4ull);
+        mbar_expect_tx(&bar, total);
+        // rows [ylo, ylo + R) mod rows: at most two contiguous pieces per quadrant
+        int64_t r0 = ((ylo % rows) + rows) % rows;
+        int done = 0;
+        while (done < R) {
+            const int piece = (int)((int64_t)(R - done) < rows - r0 ? (int64_t)(R - done) : rows - r0);
+            for (int qd = 0; qd < 4; ++qd)
+                bulk_g2s(smem + qd * qsz + (uint64_t)done * Wr, src + qd * Q + (uint64_t)r0 * Wr,
+                         (uint32_t)((uint64_t)piece * Wr * 4), &bar);
+            done += piece;
+            r0 = 0;
+        }
+        uint32_t spins = 0;
+        while (!mbar_try_wait(&bar, 0)) {
+            if (++spins > MBAR_SPIN_LIMIT) {
+                abort_flag = 1;
+                break;
+            }
+        }
+    }
+    __syncthreads();
+    if (abort_flag) {
+        // leave dst untouched for this band and report; the in-flight copy targets this
+        // CTA's shared memory only, so keep waiting (bounded) before the CTA retires
+        if (threadIdx.x == 0) {
+            atomicExch(err, 1u);
+            uint32_t spins = 0;
+            while (!mbar_try_wait(&bar, 0) && ++spins < MBAR_SPIN_LIMIT) {
+            }
+        }
+        return;
+    }
+
+    unsigned long long ndep = 0, ndes = 0;
+    for (int h = 0; h < 2 * k; ++h) {
+        const int sigma = h & 1;
+        const uint32_t step = 2u * (t0 + (uint32_t)(h >> 1)) + (uint32_t)sigma;
+        uint32_t* StX = smem + (sigma ? 2 : 0) * qsz;
+        uint32_t* StY = StX + qsz;
+        uint32_t* SoX = smem + (sigma ? 0 : 2) * qsz;
+        uint32_t* SoY = SoX + qsz;
+        const int ra = h, rb = R - 1 - h;
+        const int items = (rb - ra) * G;
+        for (int it = threadIdx.x; it < items; it += FUSED_THREADS) {
+            const int lr = ra + it / G;
+            const int g = it - (lr - ra) * G;
+            const uint64_t w0 = 4ull * g;
+            const int64_t gy = (((ylo + lr) % rows) + rows) % rows;
+            const bool shifted = sigma != (int)(gy & 1);
+            uint4* ptX = reinterpret_cast<uint4*>(StX + (uint64_t)lr * Wr + w0);
+            uint4* ptY = reinterpret_cast<uint4*>(StY + (uint64_t)lr * Wr + w0);
+            uint4* poX = reinterpret_cast<uint4*>(SoX + (uint64_t)lr * Wr + w0);
+            uint4* poY = reinterpret_cast<uint4*>(SoY + (uint64_t)(lr + 1) * Wr + w0);
+            uint4 tX = *ptX, tY = *ptY, oX = *poX, oY = *poY;
+            uint4 xX = oX;
+            uint32_t* nbp = SoX + (uint64_t)lr * Wr + ((w0 + 4) & (Wr - 1));
+            if (shifted) {
+                const uint32_t nb = *nbp;
+                xX.x = (oX.x >> 1) | (oX.y << 31);
+                xX.y = (oX.y >> 1) | (oX.z << 31);
+                xX.z = (oX.z >> 1) | (oX.w << 31);
+                xX.w = (oX.w >> 1) | (nb << 31);
+            }
+            uint4 cp, cq;
+            cp.x = ~(tX.x | tY.x) & xX.x & oY.x;
+            cp.y = ~(tX.y | tY.y) & xX.y & oY.y;
+            cp.z = ~(tX.z | tY.z) & xX.z & oY.z;
+            cp.w = ~(tX.w | tY.w) & xX.w & oY.w;
+            cq.x = tX.x & tY.x & ~(xX.x | oY.x);
+            cq.y = tX.y & tY.y & ~(xX.y | oY.y);
+            cq.z = tX.z & tY.z & ~(xX.z | oY.z);
+            cq.w = tX.w & tY.w & ~(xX.w | oY.w);
+            const uint4 m = decide4(cp, cq, tp, tq, key, (uint32_t)(((uint64_t)gy * Wr + w0) >> 2),
+                                    step, stream);
+            if (COUNT && lr >= H && lr < H + Bc) {
+                ndep += __popc(m.x & cp.x) + __popc(m.y & cp.y) + __popc(m.z & cp.z) + __popc(m.w & cp.w);
+                ndes += __popc(m.x & cq.x) + __popc(m.y & cq.y) + __popc(m.z & cq.z) + __popc(m.w & cq.w);
+            }
+            *ptX = tX ^ m;
+            *ptY = tY ^ m;
+            *poY = oY ^ m;
+            if (shifted) {
+                uint32_t* ox = SoX + (uint64_t)lr * Wr + w0;
+                atomicXor(ox, m.x << 1);
+                ox[1] = oX.y ^ ((m.y << 1) | (m.x >> 31));
+                ox[2] = oX.z ^ ((m.z << 1) | (m.y >> 31));
+                ox[3] = oX.w ^ ((m.w << 1) | (m.z >> 31));
+                if (m.w >> 31) atomicXor(nbp, 1u);
+            } else {
+                *poX = oX ^ m;
+            }
+        }
+        __syncthreads();
+    }
+
+    // write the band's own rows [H, H + Bc) of each quadrant
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int qd = 0; qd < 4; ++qd)
+            bulk_s2g(dst + qd * Q + (uint64_t)y0 * Wr, smem + qd * qsz + (uint64_t)H * Wr,
+                     (uint32_t)((uint64_t)Bc * Wr * 4));
+        asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+        asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
+    }
+    if (COUNT) {
+        for (int o = 16; o > 0; o >>= 1) {
+            ndep += __shfl_xor_sync(0xffffffffu, ndep, o);
+            ndes += __shfl_xor_sync(0xffffffffu, ndes, o);
+        }
+        if ((threadIdx.x & 31) == 0 && (ndep | ndes)) {
+            atomicAdd(&counters[0], ndep);
+            atomicAdd(&counters[1], ndes);
+        }
+    }
+}
+
+// MCS per HBM pass when the caller leaves the choice to the library: the deepest pass whose
+// band still holds at least as many output rows as halo rows (redundant work <= 2x).
+int auto_fusion(int lx, int ly)
+{
+    int best = 1;
+    for (int k = 2; k <= 8; ++k) {
+        FusedShape f = scabit_fused_shape(lx, ly, k, 148, 0);
+        if (f.ok && f.band >= 4 * k) best = k;
+    }
+    return best;
+}
+
+FusedShape scabit_fused_shape(int lx, int ly, int mcs_per_pass, int sm_count, size_t smem_optin)
+{
+    FusedShape f{};
+    f.ok = false;
+    if (smem_optin == 0) smem_optin = 227 * 1024;
+    const uint64_t Wr = 1ull << (lx - 6);
+    const uint64_t row_bytes = 16ull * Wr;  // four quadrants
+    const int64_t rows = 1ll << ly;
+    const int k = mcs_per_pass;
+    if (k < 1) return f;
+    // two CTAs per SM when the band stays at least as tall as the halo, else one
+    const size_t budget2 = (228 * 1024) / 2 - 2048;
+    const size_t budget1 = smem_optin - 1024;
+    int R = (int)(budget2 / row_bytes);
+    if (R - 4 * k < 4 * k) R = (int)(budget1 / row_bytes);
+    int B = R - 4 * k;
+    if (B < 1) return f;
+    if (B > rows) B = (int)rows;
+    R = B + 4 * k;
+    if ((uint64_t)R * Wr * 16 > 0xFFFFFFFFull) return f;
+    f.band = B;
+    f.halo = 2 * k;
+    f.mcs = k;
+    f.threads = FUSED_THREADS;
+    f.smem = (size_t)R * row_bytes;
+    f.grid = (int)((rows + B - 1) / B);
+    f.ok = true;  // the load loop handles halos that wrap the lattice more than once
+    (void)sm_count;
+    return f;
+}
+
+cudaError_t scabit_fused(const uint32_t* d_src, uint32_t* d_dst, int lx, int ly, uint32_t t0,
+                         uint64_t seed, uint32_t stream_id, uint64_t Tp, uint64_t Tq,
+                         const FusedShape& sh, unsigned long long* d_counters, unsigned int* d_err,
+                         cudaStream_t st)
+{
+    const Key key = make_key(seed);
+    const Thresh tp = make_thresh(Tp), tq = make_thresh(Tq);
+    cudaError_t e;
+    if (d_counters) {
+        e = cudaFuncSetAttribute(scabit_fused_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)sh.smem);
+        if (e != cudaSuccess) return e;
+        scabit_fused_kernel<true><<<sh.grid, sh.threads, sh.smem, st>>>(
+            d_src, d_dst, lx, ly, t0, key, stream_id, tp, tq, sh.band, sh.mcs, d_counters, d_err);
+    } else {
+        e = cudaFuncSetAttribute(scabit_fused_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)sh.smem);
+        if (e != cudaSuccess) return e;
+        scabit_fused_kernel<false><<<sh.grid, sh.threads, sh.smem, st>>>(
+            d_src, d_dst, lx, ly, t0, key, stream_id, tp, tq, sh.band, sh.mcs, d_counters, d_err);
+    }
+    return cudaGetLastError();
+}
+
+}  // namespace kpzb

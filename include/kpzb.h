@@ -1,0 +1,178 @@
+/*
+ * kpzb.h -- C ABI of libkpzb200.so, a B200 (sm_100a) implementation of the CudaKpz
+ * octahedron-model KMC hot path.  Plain pointers and sizes only; every call returns a
+ * kpzb_status; no exceptions, no exit().  File:line references point into CudaKpz.
+ *
+ * Lattices use the reference's word layouts exactly:
+ *   ENC_LOCAL  (kpz/systemSize.h:94-124): 4x4 sites per uint32, word (y>>2)*(L/4)+(x>>2),
+ *              bit ((x&3)<<1)|((y&3)<<3); bit0 = x-slope, bit1 = y-slope.
+ *   ENC_CBBIT  (kpz/systemSize.h:143-165): quadrants [sub0.X|sub0.Y|sub1.X|sub1.Y] of
+ *              N/64 words; site (x,y) of sublattice (x^y)&1 at word (y*L+x)>>6 of its
+ *              quadrant, bit (x>>1)&31.
+ *
+ * Random numbers come from a counter-based stream (Philox4x32-10 keyed by the 64-bit
+ * seed; counter = quadrant word group, half-step, bit plane, stream id), so results do
+ * not depend on the launch geometry and a CPU restatement reproduces them bit for bit.
+ *
+ * Handles are not thread-safe; distinct handles are independent.  Each handle owns one
+ * CUDA stream and all of its device memory.
+ */
+#ifndef KPZB_H
+#define KPZB_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+    KPZB_OK = 0,
+    KPZB_EINVAL = 1,      /* bad argument (size out of range, bad encoding, null pointer) */
+    KPZB_ENOMEM = 2,      /* device or pinned allocation failed */
+    KPZB_ECUDA = 3,       /* CUDA runtime error; kpzb_last_error() has the text */
+    KPZB_ETIMEOUT = 4,    /* a bounded device wait expired */
+    KPZB_ESTATE = 5,      /* call not valid in the current state (e.g. no snapshot) */
+    KPZB_EUNSUPPORTED = 6 /* combination not implemented (e.g. DT on ENC_CBBIT) */
+} kpzb_status;
+
+/* Encodings, as Kpz::SchedulerService::Encoding (kpz/schedulerService.h:71). */
+enum { KPZB_ENC_LOCAL = 0, KPZB_ENC_CBBIT = 1 };
+
+/* Dynamics, as the GPU schedulers picked by SchedulerConfig::mkSchedulerGPU
+ * (kpz/kpzFrontend.cpp:355-403). */
+enum {
+    KPZB_DYN_SCA = 0,    /* Kpz::SchedulerSCA: checkerboard SCA, ENC_LOCAL push/pop      */
+    KPZB_DYN_SCABIT = 1, /* Kpz::SchedulerSCABit: bit-vectorised SCA, ENC_CBBIT push/pop */
+    KPZB_DYN_DT = 2      /* Kpz::SchedulerDT: double-tiling random-sequential, ENC_LOCAL */
+};
+
+typedef struct kpzb_handle kpzb_handle;
+
+/* Text of the last error on this thread (empty when none). Replaces the mixed
+ * KmcExcept::CUDAError throws / stderr messages (kpz/schedulerSCABit.cu:66-72). */
+const char* kpzb_last_error(void);
+/* Library version string. */
+const char* kpzb_version(void);
+
+/* Create a scheduler for a 2^lx x 2^ly lattice on `device` (-1: current device).
+ * Replaces SchedulerSCA/SchedulerSCABit/SchedulerDT constructors + SchedulerBase::initCUDA
+ * (kpz/schedulerSCABit.cu:84-88, kpz/schedulerBase.cu:65-74, kpz/schedulerDT.cu:93-118).
+ * Limits: 8 <= lx <= 30 (SCA/SCABit), 8 <= lx (DT: lx, ly >= 10), 2 <= ly <= 30,
+ * lx + ly <= 38.  The lattice starts flat. */
+kpzb_status kpzb_create(kpzb_handle** h, int lx, int ly, int dynamics, int device);
+kpzb_status kpzb_destroy(kpzb_handle* h);
+
+/* SchedulerService::initHomogeneous (kpz/schedulerService.cpp:156-175), in the handle's
+ * encoding. Does not reset the MCS counters. */
+kpzb_status kpzb_init_homogeneous(kpzb_handle* h);
+/* SchedulerService::setPQ(p, q, 0) (kpz/schedulerService.h:186-192). 0 <= p,q <= 1. */
+kpzb_status kpzb_set_pq(kpzb_handle* h, double p, double q);
+/* Seeds the counter stream and resets the device MCS counter to 0. Replaces
+ * SchedulerService::supplySeed + randomize (kpz/schedulerService.cpp:472-482,
+ * kpz/GPUTinyMT.cu:74-103). `stream` separates replicas sharing a seed. */
+kpzb_status kpzb_seed(kpzb_handle* h, uint64_t seed, uint32_t stream);
+
+/* SchedulerService::mcsPQSyncRng(n) (kpz/schedulerService.h:211; SCA/SCABit doMcs at
+ * kpz/schedulerSCA.cu:43-70, kpz/schedulerSCABit.cu:46-73; DT at kpz/schedulerDT.cu:38-78):
+ * n Monte-Carlo steps with the rates from kpzb_set_pq. Synchronous. */
+kpzb_status kpzb_mcs(kpzb_handle* h, int n);
+/* mcsPQSyncRngAsync (kpz/schedulerService.h:212): enqueue and return; kpzb_join waits
+ * (SchedulerService::join, kpz/schedulerService.h:161-171). */
+kpzb_status kpzb_mcs_async(kpzb_handle* h, int n);
+kpzb_status kpzb_join(kpzb_handle* h);
+/* SCA/SCABit only: MCS per HBM pass of the temporally blocked kernel (1 = one launch per
+ * half-step; 0 = automatic).  Results are identical for every value. */
+kpzb_status kpzb_set_fusion(kpzb_handle* h, int mcs_per_pass);
+/* The MCS per pass the handle actually uses (the automatic choice resolved). */
+kpzb_status kpzb_get_fusion(const kpzb_handle* h, int* mcs_per_pass);
+
+/* SchedulerService::pushSystem / popSystem (kpz/schedulerBase.cu:35-52): copy host words
+ * in the handle's encoding (kpzb_size_words words) to / from the device. */
+kpzb_status kpzb_push(kpzb_handle* h, const uint32_t* words);
+kpzb_status kpzb_pop(kpzb_handle* h, uint32_t* words);
+/* Same, with device buffers of the caller (cudaMemcpyDeviceToDevice on the handle's stream). */
+kpzb_status kpzb_push_device(kpzb_handle* h, const uint32_t* d_words);
+kpzb_status kpzb_pop_device(kpzb_handle* h, uint32_t* d_words);
+size_t kpzb_size_words(const kpzb_handle* h);
+int kpzb_encoding(const kpzb_handle* h);
+
+/* SchedulerService::roughness (kpz/schedulerService.cpp:292-297, kpz/correlator.cpp:607-697):
+ * out[0] = W^2, out[1..7] = <h^k> of the path-relative heights (kpz/correlator.cpp:47-96). */
+kpzb_status kpzb_roughness(kpzb_handle* h, double out[8]);
+/* Exact power sums of the relative heights: s12[0] = sum h, s12[1] = sum h^2,
+ * hminmax[0..1] = min/max height. */
+kpzb_status kpzb_height_sums(kpzb_handle* h, int64_t s12[2], int64_t hminmax[2]);
+
+/* SchedulerService::correlateTag (kpz/schedulerService.cpp:200-213, Correlator::set at
+ * kpz/correlator.cpp:37-106): store the current lattice as the snapshot; out[8] as roughness. */
+kpzb_status kpzb_corr_tag(kpzb_handle* h, double out[8]);
+/* SchedulerService::correlate with one tag (Correlator::correlate, kpz/correlator.cpp:463-477):
+ * out[0..7] roughness of the current lattice, out[8] = ch, out[9] = cs. */
+kpzb_status kpzb_correlate(kpzb_handle* h, double out[10]);
+
+/* Device-side MCS counter (m_deviceMcs, kpz/schedulerService.h:244) and the reported MCS
+ * (SchedulerService::mcs/setMcs, kpz/schedulerService.h:242-243). */
+kpzb_status kpzb_get_mcs(const kpzb_handle* h, uint64_t* device_mcs);
+kpzb_status kpzb_set_mcs(kpzb_handle* h, uint64_t device_mcs);
+
+/* Deposition / desorption counters accumulated by the SCA/SCABit kernels since the last
+ * reset (for the height-balance invariant sum(dh) = 2*(dep - des)). */
+kpzb_status kpzb_counters(kpzb_handle* h, int64_t dep_des[2], int reset);
+kpzb_status kpzb_enable_counters(kpzb_handle* h, int on);
+
+/* SchedulerService::consitencyCheck (kpz/schedulerService.cpp:721-854) for both encodings:
+ * rep[0] rows with nonzero x-slope sum, rep[1] columns with nonzero y-slope sum,
+ * rep[2] plaquettes whose height loop does not close. All zero for a valid lattice. */
+kpzb_status kpzb_check_invariants(kpzb_handle* h, int64_t rep[3]);
+
+/* Device pointer to the lattice in the handle's internal layout (ENC_CBBIT for SCA and
+ * SCABit, ENC_LOCAL for DT) for tests and zero-copy callers. */
+kpzb_status kpzb_device_ptr(kpzb_handle* h, uint32_t** d_words, size_t* nwords);
+/* The CUDA stream the handle enqueues on (as void*, a cudaStream_t). */
+void* kpzb_stream(kpzb_handle* h);
+/* Enqueue on the caller's stream from now on (NULL: back to the handle's own stream).
+ * The caller keeps ownership of the stream and must keep it alive while the handle uses it. */
+kpzb_status kpzb_set_stream(kpzb_handle* h, void* stream);
+
+/* ---------------- batched replicas ----------------
+ * Many independent SCABit lattices of uneven size advance together: one launch per
+ * half-step over a work list of (replica, row) items, replayed from a CUDA graph per MCS
+ * chunk.  Per-replica results are bit-identical to single runs with the same
+ * (lx, p, q, seed, stream).  Replaces the per-lattice loop of kpz/kpzScaling.cpp:194-215
+ * run once per replica. */
+typedef struct kpzb_batch kpzb_batch;
+kpzb_status kpzb_batch_create(kpzb_batch** b, int n, const int* lx, const double* p,
+                              const double* q, const uint64_t* seed, const uint32_t* stream,
+                              int device);
+kpzb_status kpzb_batch_destroy(kpzb_batch* b);
+kpzb_status kpzb_batch_init_homogeneous(kpzb_batch* b);
+kpzb_status kpzb_batch_mcs(kpzb_batch* b, int n);
+kpzb_status kpzb_batch_push(kpzb_batch* b, int i, const uint32_t* words);
+kpzb_status kpzb_batch_pop(kpzb_batch* b, int i, uint32_t* words);
+/* W^2 of every replica, out[n]. */
+kpzb_status kpzb_batch_roughness(kpzb_batch* b, double* w2);
+
+/* ---------------- exact height autocorrelator ----------------
+ * Snapshots of one lattice (ENC_CBBIT words) are turned into relative heights, shifted by
+ * a common integer offset and split into signed int8 limbs; the full Gram
+ * G[s][t] = sum_sites h_s * h_t is computed on tcgen05 INT8 tensor cores with int32
+ * accumulation and exact int64 recombination.  Replaces the per-pair loop of
+ * Correlator::correlateThreaded (kpz/correlator.cpp:491-593) and correlateKernelCBBit
+ * (kpz/correlatorCuda.cu:276-369). */
+typedef struct kpzb_gram kpzb_gram;
+kpzb_status kpzb_gram_create(kpzb_gram** g, int lx, int ly, int max_snapshots, int device);
+kpzb_status kpzb_gram_destroy(kpzb_gram* g);
+/* Add a snapshot from a device ENC_CBBIT lattice (e.g. kpzb_device_ptr of an SCABit handle). */
+kpzb_status kpzb_gram_add_device(kpzb_gram* g, const uint32_t* d_cbbit);
+kpzb_status kpzb_gram_add_host(kpzb_gram* g, const uint32_t* cbbit);
+/* G (n x n, row-major int64) of the n snapshots added so far, and the per-snapshot sums
+ * S1[s] = sum h_s. method 0 = tcgen05 INT8 tensor cores, 1 = int64 CUDA-core reference. */
+kpzb_status kpzb_gram_compute(kpzb_gram* g, int method, int64_t* G, int64_t* S1);
+int kpzb_gram_count(const kpzb_gram* g);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* KPZB_H */

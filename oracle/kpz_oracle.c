@@ -1,0 +1,458 @@
+/*
+ * kpz_oracle.c -- CPU restatement of the CudaKpz hot path.
+ *
+ * TEST INFRASTRUCTURE ONLY (the checker): loaded by tests/, by
+ * __graft_entry__.smoke() and by bench.py's cpu_baseline leg, never by the
+ * product library.  Each function cites the reference file:line it restates.
+ * Written for clarity, not speed: per-site loops, full 32-plane uniforms.
+ */
+#include "kpz_oracle.h"
+
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+
+/* ------------------------------------------------------------------------ */
+/* Philox4x32-10, from Salmon et al., "Parallel random numbers: as easy as   */
+/* 1, 2, 3" (SC'11), section 3.2: Feistel-like rounds with two 32x32->64     */
+/* multiplies, Weyl key schedule.                                            */
+/* ------------------------------------------------------------------------ */
+void ko_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4])
+{
+    uint32_t c0 = ctr[0], c1 = ctr[1], c2 = ctr[2], c3 = ctr[3];
+    uint32_t k0 = key[0], k1 = key[1];
+    for (int r = 0; r < 10; ++r) {
+        if (r) { k0 += 0x9E3779B9u; k1 += 0xBB67AE85u; }
+        uint64_t p0 = (uint64_t)0xD2511F53u * c0;
+        uint64_t p1 = (uint64_t)0xCD9E8D57u * c2;
+        uint32_t hi0 = (uint32_t)(p0 >> 32), lo0 = (uint32_t)p0;
+        uint32_t hi1 = (uint32_t)(p1 >> 32), lo1 = (uint32_t)p1;
+        uint32_t n0 = hi1 ^ c1 ^ k0;
+        uint32_t n2 = hi0 ^ c3 ^ k1;
+        c0 = n0; c1 = lo1; c2 = n2; c3 = lo0;
+    }
+    out[0] = c0; out[1] = c1; out[2] = c2; out[3] = c3;
+}
+
+uint32_t ko_plane_word(uint64_t seed, uint32_t stream, uint32_t tag, uint32_t step,
+                       uint32_t plane, uint64_t qword)
+{
+    uint32_t ctr[4] = {(uint32_t)(qword >> 2), step, plane | (tag << 8), stream};
+    uint32_t key[2] = {(uint32_t)seed, (uint32_t)(seed >> 32)};
+    uint32_t out[4];
+    ko_philox4x32_10(ctr, key, out);
+    return out[qword & 3];
+}
+
+uint32_t ko_site_u(uint64_t seed, uint32_t stream, uint32_t tag, uint32_t step,
+                   uint64_t qword, int bit)
+{
+    uint32_t u = 0;
+    for (uint32_t k = 0; k < 32; ++k) {
+        uint32_t w = ko_plane_word(seed, stream, tag, step, k, qword);
+        u |= ((w >> bit) & 1u) << (31 - k);
+    }
+    return u;
+}
+
+uint64_t ko_threshold(double p)
+{
+    if (!(p > 0.0)) return 0;
+    if (p >= 1.0) return (uint64_t)1 << 32;
+    double t = ceil(p * 4294967296.0);
+    if (t >= 4294967296.0) return (uint64_t)1 << 32;
+    return (uint64_t)t;
+}
+
+/* ------------------------------------------------------------------------ */
+/* Geometry: kpz/systemSize.h:94-165                                         */
+/* ------------------------------------------------------------------------ */
+uint64_t ko_size_words(int lx, int ly) { return (uint64_t)1 << (lx + ly - 4); }
+
+/* index(x,y) = (y>>2 << lDimXW) + (x>>2); shift = ((x&3)<<1)|((y&3)<<3)   (systemSize.h:94-100) */
+static inline uint64_t local_index(int lx, int x, int y)
+{
+    return ((uint64_t)(y >> 2) << (lx - 2)) + (uint64_t)(x >> 2);
+}
+static inline int local_shift(int x, int y) { return ((x & 3) << 1) | ((y & 3) << 3); }
+
+int ko_local_get(const uint32_t* w, int lx, int x, int y)
+{
+    return (int)((w[local_index(lx, x, y)] >> local_shift(x, y)) & 3u);
+}
+
+void ko_local_flip(uint32_t* w, int lx, int x, int y, int bits)
+{
+    w[local_index(lx, x, y)] ^= (uint32_t)bits << local_shift(x, y);
+}
+
+/* quadrantIndex_CBBit = (y << (lDimX-6)) + (x >> 6); sublattice = (x^y)&1;
+ * X quadrant base = sublattice * sizeW/2, Y base = sublattice*sizeW/2 + sizeW/4;
+ * bit = (x>>1)&31   (systemSize.h:143-165) */
+uint64_t ko_cbbit_xindex(int lx, int ly, int x, int y)
+{
+    uint64_t sw = ko_size_words(lx, ly);
+    uint64_t qi = ((uint64_t)y << (lx - 6)) + (uint64_t)(x >> 6);
+    return qi + (((x ^ y) & 1) ? (sw >> 1) : 0);
+}
+uint64_t ko_cbbit_yindex(int lx, int ly, int x, int y)
+{
+    return ko_cbbit_xindex(lx, ly, x, y) + (ko_size_words(lx, ly) >> 2);
+}
+int ko_cbbit_get(const uint32_t* w, int lx, int ly, int x, int y)
+{
+    int b = (x >> 1) & 31;
+    int sx = (int)((w[ko_cbbit_xindex(lx, ly, x, y)] >> b) & 1u);
+    int sy = (int)((w[ko_cbbit_yindex(lx, ly, x, y)] >> b) & 1u);
+    return sx | (sy << 1);
+}
+static void cbbit_flip(uint32_t* w, int lx, int ly, int x, int y, int bits)
+{
+    int b = (x >> 1) & 31;
+    if (bits & 1) w[ko_cbbit_xindex(lx, ly, x, y)] ^= 1u << b;
+    if (bits & 2) w[ko_cbbit_yindex(lx, ly, x, y)] ^= 1u << b;
+}
+
+/* kpz/schedulerService.cpp:156-175 */
+void ko_init_homogeneous(uint32_t* w, int lx, int ly, int encoding)
+{
+    uint64_t sw = ko_size_words(lx, ly);
+    if (encoding == 0) {
+        for (uint64_t i = 0; i < sw; ++i) w[i] = 0x33CC33CCu;
+    } else {
+        for (uint64_t i = 0; i < sw / 2; ++i) w[i] = 0u;
+        for (uint64_t i = sw / 2; i < sw; ++i) w[i] = 0xFFFFFFFFu;
+    }
+}
+
+void ko_local_to_cbbit(const uint32_t* local, uint32_t* cbbit, int lx, int ly)
+{
+    memset(cbbit, 0, ko_size_words(lx, ly) * 4);
+    int L = 1 << lx, M = 1 << ly;
+    for (int y = 0; y < M; ++y)
+        for (int x = 0; x < L; ++x) {
+            int v = ko_local_get(local, lx, x, y);
+            cbbit_flip(cbbit, lx, ly, x, y, v);
+        }
+}
+
+void ko_cbbit_to_local(const uint32_t* cbbit, uint32_t* local, int lx, int ly)
+{
+    memset(local, 0, ko_size_words(lx, ly) * 4);
+    int L = 1 << lx, M = 1 << ly;
+    for (int y = 0; y < M; ++y)
+        for (int x = 0; x < L; ++x) {
+            int v = ko_cbbit_get(cbbit, lx, ly, x, y);
+            ko_local_flip(local, lx, x, y, v);
+        }
+}
+
+static int get_site(const uint32_t* w, int lx, int ly, int enc, int x, int y)
+{
+    return enc == 0 ? ko_local_get(w, lx, x, y) : ko_cbbit_get(w, lx, ly, x, y);
+}
+static void flip_site(uint32_t* w, int lx, int ly, int enc, int x, int y, int bits)
+{
+    if (enc == 0) ko_local_flip(w, lx, x, y, bits);
+    else cbbit_flip(w, lx, ly, x, y, bits);
+}
+
+/* ------------------------------------------------------------------------ */
+/* SCA half-step, per-site form of kpz/kpzSCACores.cu:121-144 and           */
+/* kpz/schedulerCPUCBBit_nested.inl:261-295: config = c | s_x(x+1,y)<<2 |     */
+/* s_y(x,y+1)<<3; 12 -> deposit with prob p, 3 -> desorb with prob q; a flip */
+/* xors both bits of (x,y), the x-bit of (x+1,y) and the y-bit of (x,y+1).   */
+/* All sites of one sublattice are independent, so loop order is free.     */
+/* ------------------------------------------------------------------------ */
+void ko_sca_halfstep(uint32_t* w, int lx, int ly, int encoding, int sigma,
+                     uint64_t seed, uint32_t stream, uint32_t step,
+                     uint64_t Tp, uint64_t Tq, int64_t* dep, int64_t* des)
+{
+    int L = 1 << lx, M = 1 << ly;
+    int64_t nd = 0, nr = 0;
+    for (int y = 0; y < M; ++y)
+        for (int x = 0; x < L; ++x) {
+            if (((x ^ y) & 1) != sigma) continue;
+            int c = get_site(w, lx, ly, encoding, x, y);
+            int r = get_site(w, lx, ly, encoding, (x + 1) & (L - 1), y) & 1;
+            int l = (get_site(w, lx, ly, encoding, x, (y + 1) & (M - 1)) >> 1) & 1;
+            int config = c | (r << 2) | (l << 3);
+            uint64_t T;
+            if (config == 12) T = Tp;
+            else if (config == 3) T = Tq;
+            else continue;
+            if (T == 0) continue;
+            if (T < ((uint64_t)1 << 32)) {
+                /* the site's uniform: CBBit quadrant word index and bit (systemSize.h:143-165) */
+                uint64_t qword = ((uint64_t)y << (lx - 6)) + (uint64_t)(x >> 6);
+                uint32_t u = ko_site_u(seed, stream, KO_TAG_SCA, step, qword, (x >> 1) & 31);
+                if ((uint64_t)u >= T) continue;
+            }
+            flip_site(w, lx, ly, encoding, x, y, 3);
+            flip_site(w, lx, ly, encoding, (x + 1) & (L - 1), y, 1);
+            flip_site(w, lx, ly, encoding, x, (y + 1) & (M - 1), 2);
+            if (config == 12) ++nd; else ++nr;
+        }
+    if (dep) *dep += nd;
+    if (des) *des += nr;
+}
+
+/* kpz/schedulerSCABit.cu:46-73 (caller(0); caller(1); per MCS) */
+void ko_sca_mcs(uint32_t* w, int lx, int ly, int encoding, uint64_t seed, uint32_t stream,
+                uint64_t t0, int n, double p, double q, int64_t* dep, int64_t* des)
+{
+    uint64_t Tp = ko_threshold(p), Tq = ko_threshold(q);
+    for (int i = 0; i < n; ++i) {
+        uint64_t t = t0 + (uint64_t)i;
+        for (int s = 0; s < 2; ++s)
+            ko_sca_halfstep(w, lx, ly, encoding, s, seed, stream, (uint32_t)(2 * t + s), Tp, Tq,
+                            dep, des);
+    }
+}
+
+/* ------------------------------------------------------------------------ */
+/* Heights: kpz/correlator.cpp:47-96. Start of row y adds s_y(0,y); then     */
+/* x = 1..L-1 adds s_x(x,y); then the wrap adds s_x(0,y) giving h(0,y).     */
+/* h(0,y) is recorded last; the value carried into row y+1 is h(0,y).       */
+/* ------------------------------------------------------------------------ */
+void ko_heights(const uint32_t* w, int lx, int ly, int encoding, int32_t* h)
+{
+    int L = 1 << lx, M = 1 << ly;
+    int32_t cur = 0;
+    for (int y = 0; y < M; ++y) {
+        int row = get_site(w, lx, ly, encoding, 0, y);
+        cur += (row & 2) ? 1 : -1;
+        for (int x = 1; x < L; ++x) {
+            cur += (get_site(w, lx, ly, encoding, x, y) & 1) ? 1 : -1;
+            h[(size_t)y * L + x] = cur;
+        }
+        cur += (row & 1) ? 1 : -1;
+        h[(size_t)y * L] = cur;
+    }
+}
+
+void ko_power_sums(const int32_t* h, uint64_t n, int64_t lo[7], int64_t hi[7])
+{
+    __int128 s[7] = {0, 0, 0, 0, 0, 0, 0};
+    for (uint64_t i = 0; i < n; ++i) {
+        __int128 v = h[i], a = v;
+        for (int k = 0; k < 7; ++k) {
+            s[k] += a;
+            a *= v;
+        }
+    }
+    for (int k = 0; k < 7; ++k) {
+        unsigned __int128 u = (unsigned __int128)s[k];
+        lo[k] = (int64_t)(uint64_t)u;
+        hi[k] = (int64_t)(uint64_t)(u >> 64);
+    }
+}
+
+/* Roughness::addH / normAndSetW2 (kpz/schedulerService.h:58-64, kpz/roughness.cpp:38-43):
+ * long double accumulation of double-valued powers, then division by N. */
+static void add_h(long double acc[7], double ph)
+{
+    acc[0] += ph;
+    double a = ph;
+    for (int k = 1; k < 7; ++k) acc[k] += (a *= ph);
+}
+
+void ko_roughness(const uint32_t* w, int lx, int ly, int encoding, double out[8])
+{
+    uint64_t n = (uint64_t)1 << (lx + ly);
+    int32_t* h = (int32_t*)malloc(n * sizeof(int32_t));
+    ko_heights(w, lx, ly, encoding, h);
+    long double acc[7] = {0, 0, 0, 0, 0, 0, 0};
+    /* the reference visits x = 1..L-1 then x = 0 per row; same order here */
+    int L = 1 << lx, M = 1 << ly;
+    for (int y = 0; y < M; ++y) {
+        for (int x = 1; x < L; ++x) add_h(acc, h[(size_t)y * L + x]);
+        add_h(acc, h[(size_t)y * L]);
+    }
+    for (int k = 0; k < 7; ++k) acc[k] /= (long double)n;
+    out[0] = (double)(acc[1] - acc[0] * acc[0]);
+    for (int k = 0; k < 7; ++k) out[1 + k] = (double)acc[k];
+    free(h);
+}
+
+/* Correlator::correlate (kpz/correlator.cpp:463-477) with CorrelateData::correlateCBBit /
+ * correlateCO (:180-263, :337-399): ch = sum h_snap*h_sys / N - <h_sys><h_snap>,
+ * cs = (number of equal slope bits - number of different slope bits) / N / 2. */
+void ko_correlate(const uint32_t* sys, const uint32_t* snap, int lx, int ly, int encoding,
+                  double snap_mean, double out[10])
+{
+    uint64_t n = (uint64_t)1 << (lx + ly);
+    int L = 1 << lx, M = 1 << ly;
+    int32_t* hs = (int32_t*)malloc(n * sizeof(int32_t));
+    int32_t* ht = (int32_t*)malloc(n * sizeof(int32_t));
+    ko_heights(sys, lx, ly, encoding, hs);
+    ko_heights(snap, lx, ly, encoding, ht);
+    long double acc[7] = {0, 0, 0, 0, 0, 0, 0};
+    double ch = 0.0;
+    long long tcs = 0;
+    for (int y = 0; y < M; ++y) {
+        for (int xi = 1; xi <= L; ++xi) {
+            int x = xi & (L - 1);
+            size_t i = (size_t)y * L + x;
+            add_h(acc, hs[i]);
+            ch += ht[i] * (double)hs[i];
+            int a = get_site(sys, lx, ly, encoding, x, y);
+            int b = get_site(snap, lx, ly, encoding, x, y);
+            tcs += ((a & 1) == (b & 1)) ? 1 : -1;
+            tcs += ((a & 2) == (b & 2)) ? 1 : -1;
+        }
+    }
+    for (int k = 0; k < 7; ++k) acc[k] /= (long double)n;
+    out[0] = (double)(acc[1] - acc[0] * acc[0]);
+    for (int k = 0; k < 7; ++k) out[1 + k] = (double)acc[k];
+    out[8] = ch / (double)n - (double)acc[0] * snap_mean;
+    out[9] = (double)tcs / (double)n / 2.0;
+    free(hs);
+    free(ht);
+}
+
+/* SchedulerService::consitencyCheckThread (kpz/schedulerService.cpp:733-810), for both
+ * encodings: row sums of x-slopes, column sums of y-slopes, plaquette loops
+ * s_x(x,y) - s_y(x,y) + s_y(x-1,y) - s_x(x,y-1) (as +-1) = 0. */
+void ko_check_invariants(const uint32_t* w, int lx, int ly, int encoding, int64_t rep[3])
+{
+    int L = 1 << lx, M = 1 << ly;
+    int64_t badrows = 0, badcols = 0, badloops = 0;
+    int64_t* colsum = (int64_t*)calloc((size_t)L, sizeof(int64_t));
+    for (int y = 0; y < M; ++y) {
+        int64_t rs = 0;
+        for (int x = 0; x < L; ++x) {
+            int c = get_site(w, lx, ly, encoding, x, y);
+            int sx = (c & 1) ? 1 : -1, sy = (c & 2) ? 1 : -1;
+            rs += sx;
+            colsum[x] += sy;
+            int syl = (get_site(w, lx, ly, encoding, (x + L - 1) & (L - 1), y) & 2) ? 1 : -1;
+            int sxd = (get_site(w, lx, ly, encoding, x, (y + M - 1) & (M - 1)) & 1) ? 1 : -1;
+            if (sx - sy + syl - sxd != 0) ++badloops;
+        }
+        if (rs != 0) ++badrows;
+    }
+    for (int x = 0; x < L; ++x)
+        if (colsum[x] != 0) ++badcols;
+    free(colsum);
+    rep[0] = badrows;
+    rep[1] = badcols;
+    rep[2] = badloops;
+}
+
+/* ------------------------------------------------------------------------ */
+/* dSFMT-19937 (vendored BSD third-party code in the reference,             */
+/* inc/dSFMT/dSFMT.{h,cpp}, parameters inc/dSFMT/dSFMT-params19937.h;       */
+/* Saito & Matsumoto, "A PRNG specialized in double precision floating      */
+/* point numbers using an affine transition", MCQMC 2008). Restated here:   */
+/* 128-bit lung recursion, MT-style 32-bit seeding, exponent masking and    */
+/* period certification, [1,2) doubles minus 1.                             */
+/* ------------------------------------------------------------------------ */
+#define KD_N 191
+#define KD_POS1 117
+#define KD_SL1 19
+#define KD_SR 12
+#define KD_MSK1 0x000ffafffffffb3fULL
+#define KD_MSK2 0x000ffdfffc90fffdULL
+#define KD_FIX1 0x90014964b32f4329ULL
+#define KD_FIX2 0x3b8d12ac548a7c7aULL
+#define KD_PCV1 0x3d84e1ac0dc82880ULL
+#define KD_PCV2 0x0000000000000001ULL
+
+struct ko_dsfmt {
+    uint64_t st[KD_N + 1][2];
+    int idx;
+};
+
+size_t ko_dsfmt_size(void) { return sizeof(struct ko_dsfmt); }
+
+static void kd_recursion(uint64_t r[2], const uint64_t a[2], const uint64_t b[2], uint64_t lung[2])
+{
+    uint64_t t0 = a[0], t1 = a[1], L0 = lung[0], L1 = lung[1];
+    lung[0] = (t0 << KD_SL1) ^ (L1 >> 32) ^ (L1 << 32) ^ b[0];
+    lung[1] = (t1 << KD_SL1) ^ (L0 >> 32) ^ (L0 << 32) ^ b[1];
+    r[0] = (lung[0] >> KD_SR) ^ (lung[0] & KD_MSK1) ^ t0;
+    r[1] = (lung[1] >> KD_SR) ^ (lung[1] & KD_MSK2) ^ t1;
+}
+
+static void kd_gen_all(ko_dsfmt* s)
+{
+    uint64_t lung[2] = {s->st[KD_N][0], s->st[KD_N][1]};
+    int i;
+    for (i = 0; i < KD_N - KD_POS1; ++i) kd_recursion(s->st[i], s->st[i], s->st[i + KD_POS1], lung);
+    for (; i < KD_N; ++i) kd_recursion(s->st[i], s->st[i], s->st[i + KD_POS1 - KD_N], lung);
+    s->st[KD_N][0] = lung[0];
+    s->st[KD_N][1] = lung[1];
+}
+
+void ko_dsfmt_init(ko_dsfmt* s, uint32_t seed)
+{
+    uint32_t v[(KD_N + 1) * 4];
+    v[0] = seed;
+    for (uint32_t i = 1; i < (KD_N + 1) * 4; ++i)
+        v[i] = 1812433253u * (v[i - 1] ^ (v[i - 1] >> 30)) + i;
+    for (int i = 0; i < KD_N + 1; ++i)
+        for (int j = 0; j < 2; ++j)
+            s->st[i][j] = (uint64_t)v[4 * i + 2 * j] | ((uint64_t)v[4 * i + 2 * j + 1] << 32);
+    for (int i = 0; i < KD_N; ++i)
+        for (int j = 0; j < 2; ++j)
+            s->st[i][j] = (s->st[i][j] & 0x000FFFFFFFFFFFFFULL) | 0x3FF0000000000000ULL;
+    /* period certification; PCV2 is odd, so a failing check flips bit 0 of the lung's high word */
+    uint64_t t0 = s->st[KD_N][0] ^ KD_FIX1, t1 = s->st[KD_N][1] ^ KD_FIX2;
+    uint64_t inner = (t0 & KD_PCV1) ^ (t1 & KD_PCV2);
+    for (int i = 32; i > 0; i >>= 1) inner ^= inner >> i;
+    if ((inner & 1) != 1) s->st[KD_N][1] ^= 1;
+    s->idx = KD_N * 2;
+}
+
+double ko_dsfmt_close_open(ko_dsfmt* s)
+{
+    if (s->idx >= KD_N * 2) {
+        kd_gen_all(s);
+        s->idx = 0;
+    }
+    uint64_t bits = s->st[s->idx >> 1][s->idx & 1];
+    s->idx++;
+    double d;
+    memcpy(&d, &bits, sizeof d);
+    return d - 1.0;
+}
+
+/* SchedulerService::reSeed (kpz/schedulerService.cpp:460-470) */
+void ko_dsfmt_reseed(ko_dsfmt* s, uint32_t seed)
+{
+    ko_dsfmt_init(s, seed);
+    for (int a = 0; a < 100000; ++a) ko_dsfmt_close_open(s);
+}
+
+/* SchedulerCPU::mcs / mcsPQ (kpz/schedulerCPU.inl:21-88, kpz/schedulerCPU.cpp:35-46) */
+void ko_rs_mcs(uint32_t* w, int lx, int ly, ko_dsfmt* s, int n, int pq, double p, double q)
+{
+    int L = 1 << lx, M = 1 << ly;
+    uint64_t N = (uint64_t)1 << (lx + ly);
+    int oneone = pq && p == 1.0 && q == 1.0;
+    for (; n > 0; --n) {
+        for (uint64_t a = 0; a < N; ++a) {
+            int x = (int)(ko_dsfmt_close_open(s) * L);
+            int y = (int)(ko_dsfmt_close_open(s) * M);
+            int c = ko_local_get(w, lx, x, y);
+            int r = ko_local_get(w, lx, (x + 1) & (L - 1), y) & 1;
+            int l = (ko_local_get(w, lx, x, (y + 1) & (M - 1)) >> 1) & 1;
+            int config = c | (r << 2) | (l << 3);
+            if (!pq) {
+                if (config != 12) continue;
+            } else if (oneone) {
+                if (config != 12 && config != 3) continue;
+            } else {
+                if (config == 12) {
+                    if (ko_dsfmt_close_open(s) >= p) continue;
+                } else if (config == 3) {
+                    if (ko_dsfmt_close_open(s) >= q) continue;
+                } else continue;
+            }
+            ko_local_flip(w, lx, x, y, 3);
+            ko_local_flip(w, lx, (x + 1) & (L - 1), y, 1);
+            ko_local_flip(w, lx, x, (y + 1) & (M - 1), 2);
+        }
+    }
+}

@@ -1,0 +1,167 @@
+"""GPU parity of the SCA / SCABit path against the CPU oracle, through the C ABI.
+
+Bit-exact: both sides consume the same counter-based stream (Philox4x32-10, see
+oracle/kpz_oracle.h), so every lattice word must match.  Reference behaviour:
+kpz/kpzSCABit.cu:112-290, kpz/kpzSCABitCores.cu:69-74,139-145, kpz/kpzSCACores.cu:121-144,
+kpz/schedulerSCABit.cu:46-73.
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+PQ = [(1.0, 0.0), (0.5, 0.5), (0.95, 0.05), (0.3, 0.7), (0.5, 0.0), (0.75, 0.25), (1.0, 1.0),
+      (0.0, 0.0)]
+
+
+def first_diff(a, b):
+    d = np.nonzero(a != b)[0]
+    return None if d.size == 0 else (int(d[0]), hex(int(a[d[0]])), hex(int(b[d[0]])), int(d.size))
+
+
+def run_gpu(kpzb, lx, ly, sched, p, q, seed, n, init=None, fusion=1, stream=0):
+    s = kpzb.Scheduler(lx, ly, scheduler=sched)
+    s.setPQ(p, q)
+    s.supplySeed(seed, stream)
+    s.setFusion(fusion)
+    if init is not None:
+        s.pushSystem(init)
+    s.mcsPQSyncRng(n)
+    out = s.popSystem()
+    s.close()
+    return out
+
+
+@pytest.mark.parametrize("p,q", PQ)
+@pytest.mark.parametrize("lx,ly", [(8, 8), (9, 9), (10, 7)])
+def test_scabit_flat_start_bit_exact(kpzb, oracle, lx, ly, p, q):
+    n = 6
+    ref = oracle.homogeneous(lx, ly, oracle.ENC_CBBIT)
+    oracle.sca_mcs(ref, lx, ly, oracle.ENC_CBBIT, 42, 0, 0, n, p, q)
+    got = run_gpu(kpzb, lx, ly, "scaBit", p, q, 42, n)
+    assert first_diff(got, ref) is None, first_diff(got, ref)
+
+
+@pytest.mark.parametrize("lx,ly", [(11, 9), (12, 8), (14, 4)])
+def test_scabit_wide_rows_segment_carry(kpzb, oracle, lx, ly):
+    """Rows longer than one CTA segment (4*256 words) exercise the carried one-bit mask."""
+    p, q = 0.6, 0.4
+    init = oracle.random_lattice(lx, ly, oracle.ENC_CBBIT, seed=5, mcs=3)
+    ref = init.copy()
+    oracle.sca_mcs(ref, lx, ly, oracle.ENC_CBBIT, 9, 3, 0, 3, p, q)
+    got = run_gpu(kpzb, lx, ly, "scaBit", p, q, 9, 3, init=init, stream=3)
+    assert first_diff(got, ref) is None, first_diff(got, ref)
+
+
+@pytest.mark.parametrize("fusion", [2, 3, 5])
+@pytest.mark.parametrize("lx,ly,p,q", [(9, 9, 0.5, 0.5), (10, 10, 1.0, 0.0), (8, 10, 0.9, 0.1),
+                                       (11, 6, 0.5, 0.5)])
+def test_fused_bit_exact(kpzb, oracle, lx, ly, p, q, fusion):
+    n = 2 * fusion + 1  # whole fused passes plus a single-step remainder
+    init = oracle.random_lattice(lx, ly, oracle.ENC_CBBIT, seed=11, mcs=2)
+    ref = init.copy()
+    oracle.sca_mcs(ref, lx, ly, oracle.ENC_CBBIT, 77, 0, 0, n, p, q)
+    got = run_gpu(kpzb, lx, ly, "scaBit", p, q, 77, n, init=init, fusion=fusion)
+    assert first_diff(got, ref) is None, first_diff(got, ref)
+
+
+@pytest.mark.parametrize("p,q", [(0.95, 0.0), (0.5, 0.5), (1.0, 0.0)])
+def test_sca_local_encoding_bit_exact(kpzb, oracle, p, q):
+    """SchedulerSCA: ENC_LOCAL push/pop; dynamics identical to the per-site ENC_LOCAL oracle."""
+    lx = ly = 9
+    init = oracle.cbbit_to_local(oracle.random_lattice(lx, ly, oracle.ENC_CBBIT, seed=3), lx, ly)
+    ref = init.copy()
+    oracle.sca_mcs(ref, lx, ly, oracle.ENC_LOCAL, 1234, 0, 0, 4, p, q)
+    got = run_gpu(kpzb, lx, ly, "sca", p, q, 1234, 4, init=init)
+    assert first_diff(got, ref) is None, first_diff(got, ref)
+
+
+def test_sca_flat_start_local_words(kpzb, oracle):
+    s = kpzb.Scheduler(9, 9, scheduler="sca")
+    w = s.popSystem()
+    assert np.all(w == 0x33CC33CC)
+    s.close()
+    s = kpzb.Scheduler(9, 9, scheduler="scaBit")
+    w = s.popSystem()
+    assert np.all(w[: w.size // 2] == 0) and np.all(w[w.size // 2:] == 0xFFFFFFFF)
+    s.close()
+
+
+def test_mcs_split_equals_single_call(kpzb, oracle):
+    lx = ly = 10
+    a = kpzb.Scheduler(lx, ly)
+    a.setPQ(0.7, 0.2)
+    a.supplySeed(5)
+    a.mcsPQSyncRng(7)
+    b = kpzb.Scheduler(lx, ly)
+    b.setPQ(0.7, 0.2)
+    b.supplySeed(5)
+    for k in (1, 2, 4):
+        b.mcsPQSyncRng(k)
+    assert np.array_equal(a.popSystem(), b.popSystem())
+    assert a.deviceMcs() == b.deviceMcs() == 7
+
+
+def test_counters_height_balance(kpzb, oracle):
+    """sum of relative heights changes by 2*(dep - des) modulo 2N (the reference point moves)."""
+    lx = ly = 10
+    N = 1 << (lx + ly)
+    s = kpzb.Scheduler(lx, ly)
+    s.setPQ(0.8, 0.3)
+    s.supplySeed(2)
+    s.enableCounters(True)
+    (s1a, _), _ = s.heightSums()
+    s.mcsPQSyncRng(5)
+    dep, des = s.counters(reset=True)
+    (s1b, _), _ = s.heightSums()
+    assert dep > 0 and des > 0
+    assert (s1b - s1a - 2 * (dep - des)) % (2 * N) == 0
+    ref = oracle.homogeneous(lx, ly, oracle.ENC_CBBIT)
+    rdep, rdes = oracle.sca_mcs(ref, lx, ly, oracle.ENC_CBBIT, 2, 0, 0, 5, 0.8, 0.3)
+    assert (dep, des) == (rdep, rdes)
+
+
+@pytest.mark.parametrize("fusion", [1, 4])
+def test_counters_fused(kpzb, oracle, fusion):
+    lx, ly = 10, 9
+    s = kpzb.Scheduler(lx, ly)
+    s.setPQ(0.6, 0.4)
+    s.supplySeed(8)
+    s.setFusion(fusion)
+    s.enableCounters(True)
+    s.mcsPQSyncRng(8)
+    ref = oracle.homogeneous(lx, ly, oracle.ENC_CBBIT)
+    assert s.counters() == oracle.sca_mcs(ref, lx, ly, oracle.ENC_CBBIT, 8, 0, 0, 8, 0.6, 0.4)
+
+
+def test_full_size_16384_properties(kpzb, oracle):
+    """16384^2 (C2 size): fused == unfused bit for bit, invariants hold, height balance."""
+    lx = ly = 14
+    N = 1 << 28
+    res = {}
+    for fusion in (1, 0):
+        s = kpzb.Scheduler(lx, ly)
+        s.setPQ(0.5, 0.5)
+        s.supplySeed(42)
+        s.setFusion(fusion)
+        s.enableCounters(True)
+        (s1a, _), _ = s.heightSums()
+        s.mcsPQSyncRng(12)
+        ok, rep = s.consitencyCheck()
+        assert ok, rep
+        dep, des = s.counters()
+        (s1b, _), _ = s.heightSums()
+        assert dep > 0 and des > 0
+        assert (s1b - s1a - 2 * (dep - des)) % (2 * N) == 0
+        res[fusion] = s.popSystem()
+        s.close()
+    assert first_diff(res[1], res[0]) is None
+
+
+def test_full_size_first_mcs_vs_oracle(kpzb, oracle):
+    """16384^2 at (p,q)=(1,0): the first 2 MCS match the oracle word for word."""
+    lx = ly = 14
+    ref = oracle.homogeneous(lx, ly, oracle.ENC_CBBIT)
+    oracle.sca_mcs(ref, lx, ly, oracle.ENC_CBBIT, 42, 0, 0, 2, 1.0, 0.0)
+    got = run_gpu(kpzb, lx, ly, "scaBit", 1.0, 0.0, 42, 2, fusion=0)
+    assert first_diff(got, ref) is None, first_diff(got, ref)

@@ -1,0 +1,155 @@
+#!/usr/bin/env python
+"""Build the reference's own CPU schedulers into oracle/_ref/kpz_ref -- TEST INFRASTRUCTURE.
+
+Compiles CudaKpz sources where they lie (read from /root/reference, never copied into this
+repository) together with oracle/ref_driver.cpp.  The reference's own build system needs
+MPI, HDF5/libSplash and a TinyMT parameter table that is not shipped, and its code falls off
+the end of several non-void functions, which current g++ turns into traps.  So this recipe:
+
+  1. copies kpz/ and inc/ to a scratch directory under /tmp (outside this repository),
+  2. removes the HDF5/libSplash/MPI include lines and the I/O function bodies that need them
+     (writeH5/readH5/collectH5/retrieveH5/mcsH5/closeH5/syncRNGMPI, Correlator::save/fromH5,
+     SystemSize::splashDimensions) -- none is on the hot path,
+  3. adds the missing return statements,
+  4. writes a placeholder TinyMT parameter table (TinyMT's published default parameter set
+     repeated; the reference's table is absent, so TinyMT streams are not the reference's),
+  5. compiles with g++ -O2 and writes the binary to oracle/_ref/kpz_ref.
+
+Only code paths that do not depend on the TinyMT table are used as golden vectors
+(p = 1 or q = 1 deterministic SCA, dSFMT random-sequential, roughness, correlator).
+"""
+from __future__ import annotations
+
+import os
+import re
+import shutil
+import subprocess
+import sys
+from pathlib import Path
+
+REF = Path(os.environ.get("KPZ_REFERENCE", "/root/reference"))
+HERE = Path(__file__).resolve().parent
+OUT = HERE / "_ref"
+WORK = Path("/tmp/kpzb_refbuild")
+
+SOURCES = [
+    "kpz/systemSize.cpp", "kpz/threadLayout.cpp", "kpz/roughness.cpp", "kpz/schedulerService.cpp",
+    "kpz/schedulerServiceStash.cpp", "kpz/correlator.cpp", "kpz/correlatorLines.cpp",
+    "kpz/schedulerCPU.cpp", "kpz/schedulerCPUBase.cpp", "kpz/schedulerCPUBaseThreaded.cpp",
+    "kpz/CPURngIface.cpp", "kpz/schedulerCPUCBBit_instances.cpp", "kpz/schedulerCPUCB_instances.cpp",
+    "inc/dSFMT/dSFMT.cpp", "inc/tinyMT/tinymt32.c", "inc/timer.cpp",
+]
+
+STUB = """// forward declarations replacing the HDF5/libSplash/MPI headers (I/O is not built)
+#pragma once
+#include <string>
+#include <sstream>
+namespace splash { class DataCollector; class Dimensions; class Selection; }
+namespace MPI { class Comm; }
+"""
+
+
+def cut_between(text: str, start: str, end: str | None) -> str:
+    a = text.index(start)
+    b = text.index(end, a) if end else len(text)
+    return text[:a] + text[b:]
+
+
+def add_return(text: str, signature: str, stmt: str) -> str:
+    """Insert `stmt` before the closing brace of the function whose header starts with signature."""
+    a = text.index(signature)
+    i = text.index("{", a)
+    depth = 0
+    for j in range(i, len(text)):
+        if text[j] == "{":
+            depth += 1
+        elif text[j] == "}":
+            depth -= 1
+            if depth == 0:
+                return text[:j] + "\t" + stmt + "\n" + text[j:]
+    raise ValueError(signature)
+
+
+def patch(work: Path) -> None:
+    for p in list(work.rglob("*.cpp")) + list(work.rglob("*.h")) + list(work.rglob("*.inl")):
+        t = p.read_text(errors="replace")
+        t2 = re.sub(r"#include\s*<(mpi\.h|splash/splash\.h|KMCsplash\.h)>", "", t)
+        if t2 != t:
+            p.write_text(t2)
+    ss = work / "kpz/schedulerService.cpp"
+    t = ss.read_text()
+    t = cut_between(t, "splash::DataCollector* Kpz::SchedulerService::writeH5",
+                    "void* Kpz::SchedulerService::callMcs")
+    t = cut_between(t, "int Kpz::SchedulerService::syncRNGMPI", "void Kpz::SchedulerService::setMcs")
+    ss.write_text(t)
+    co = work / "kpz/correlator.cpp"
+    t = co.read_text()
+    t = cut_between(t, "void Kpz::Correlator::save", "std::ostream& operator<< (std::ostream& o, const Kpz::Correlator& c)")
+    for fn in ("correlateThreadCO", "correlateThreadCBBit", "roughnessThreadCO", "roughnessThreadCBBit"):
+        t = add_return(t, f"void* Kpz::Correlator::{fn}(void* cd)", "return 0;")
+    co.write_text(t)
+    sz = work / "kpz/systemSize.cpp"
+    t = sz.read_text()
+    t = cut_between(t, "splash::Dimensions Kpz::SystemSize::splashDimensions", None)
+    t = add_return(t, "bool Kpz::SystemSizeBase::set(int lx, int ly)", "return true;")
+    t = add_return(t, "std::ostream& Kpz::operator<<(std::ostream& o, const Kpz::SystemSize& s)", "return o;")
+    sz.write_text(t)
+    ro = work / "kpz/roughness.cpp"
+    t = ro.read_text()
+    t = add_return(t, "const Kpz::Roughness& Kpz::Roughness::operator+=", "return *this;")
+    t = add_return(t, "const Kpz::Roughness& Kpz::Roughness::operator/=", "return *this;")
+    ro.write_text(t)
+    bt = work / "kpz/schedulerCPUBaseThreaded.cpp"
+    t = bt.read_text()
+    m = re.search(r"\n(\w[^\n]*joinAllWorkers\([^)]*\))", t)
+    if m and not m.group(1).startswith("void"):
+        t = add_return(t, m.group(1), "return 0;")
+    bt.write_text(t)
+    for hdr in ("kpz/schedulerCPUBaseThreaded.h", "kpz/schedulerCPUpThread.h"):
+        p = work / hdr
+        t = p.read_text()
+        m = re.search(r"(static void\* func_mcs\([^)]*\))", t)
+        if m:
+            t = add_return(t, m.group(1), "return 0;")
+        p.write_text(t)
+    tmt = work / "inc/tinyMT/tinymt32_param.h"
+    n = 4096
+    tmt.write_text(
+        "// placeholder TinyMT32 parameter table: TinyMT's published default set, repeated\n"
+        f"#pragma once\n#define KMC_N_TMT_PARAM_SETS {n}\n"
+        + "".join(f"static const unsigned int {name}[{n}] = {{" + ",".join([val] * n) + "};\n"
+                  for name, val in (("tinyMTmat1", "0x8f7011eeu"), ("tinyMTmat2", "0xfc78ff1fu"),
+                                    ("tinyMTtmat", "0x3793fdffu"))))
+    (work / "stub_io.h").write_text(STUB)
+
+
+def main() -> int:
+    if not REF.is_dir():
+        print(f"{REF} not present; skipping the reference build", file=sys.stderr)
+        return 0
+    if WORK.exists():
+        shutil.rmtree(WORK)
+    WORK.mkdir(parents=True)
+    shutil.copytree(REF / "kpz", WORK / "kpz")
+    shutil.copytree(REF / "inc", WORK / "inc")
+    patch(WORK)
+    OUT.mkdir(exist_ok=True)
+    objs = []
+    flags = ["-O2", "-std=c++14", "-w", "-DDSFMT_MEXP=19937", "-DKPZ_SWITCH_RNG=SLCG64",
+             f"-I{WORK / 'kpz'}", f"-I{WORK / 'inc'}", "-include", str(WORK / "stub_io.h"), "-pthread"]
+    for src in SOURCES:
+        path = WORK / src
+        obj = WORK / (path.stem + ".o")
+        cc = ["gcc", "-O2", "-w", f"-I{WORK / 'inc'}"] if src.endswith(".c") else ["g++", *flags]
+        extra = ["-Dprotected=public"] if "schedulerCPUCB_instances" in src else []
+        subprocess.run([*cc, *extra, "-c", str(path), "-o", str(obj)], check=True)
+        objs.append(str(obj))
+    drv = WORK / "ref_driver.o"
+    subprocess.run(["g++", *flags, "-c", str(HERE / "ref_driver.cpp"), "-o", str(drv)], check=True)
+    subprocess.run(["g++", "-pthread", "-o", str(OUT / "kpz_ref"), str(drv), *objs], check=True)
+    print(f"built {OUT / 'kpz_ref'}")
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

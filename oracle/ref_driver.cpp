@@ -1,0 +1,227 @@
+// ref_driver.cpp -- command-line driver around the reference's own CPU code (CudaKpz),
+// compiled with it by oracle/build_ref.py into oracle/_ref/kpz_ref.  TEST INFRASTRUCTURE
+// ONLY: it produces golden vectors (tests/golden/) and times the reference CPU schedulers
+// for bench.py's reference arm.  It never links into the product.
+//
+// Commands (lattice files are raw little-endian uint32 words in the reference layout):
+//   rs LX SEED T1 [T2 ...] OUT      SchedulerCPU::mcs (kpz/schedulerCPU.cpp:35-38), flat ENC_LOCAL
+//                                   start, supplySeed(1, SEED); prints "t W2 h1..h7" at each T;
+//                                   writes the final lattice to OUT
+//   cbbit LX P Q N IN|flat OUT THR  SchedulerCPUCBBit<TinyMT32>::mcsPQSyncRng(N) (ENC_CBBIT)
+//   cb LX P Q N IN|flat OUT THR     SchedulerCPUCB<TinyMT32>::mcsPQSyncRng(N) (ENC_LOCAL SCA)
+//   rough ENC LX IN                 SchedulerService::roughness() (Correlator::roughnessThreaded)
+//   corr ENC LX SNAP SYS            Correlator::set(SNAP) then Correlator::correlate() on SYS;
+//                                   prints W2 h1..h7 ch cs
+//   check ENC LX IN                 SchedulerService::consitencyCheck(); prints 1/0
+//   bench-cbbit LX P Q N THR        time mcsPQSyncRng(N) of SchedulerCPUCBBit; prints upd/ns
+//   bench-rs LX N                   time SchedulerCPU::mcs(N); prints upd/ns
+#include <chrono>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <fstream>
+#include <iomanip>
+#include <iostream>
+#include <string>
+#include <vector>
+
+#include "CPURngIface.h"
+#include "correlator.h"
+#include "schedulerCPU.h"
+#include "schedulerCPUCB.h"
+#include "schedulerCPUCBBit.h"
+#include "schedulerService.h"
+
+// The HDF5/libSplash and MPI entry points of SchedulerService are outside the hot path;
+// the build strips their definitions, and these keep the vtables complete.
+bool Kpz::SchedulerService::collectH5(splash::DataCollector*, const std::string&) { return false; }
+bool Kpz::SchedulerService::retrieveH5(splash::DataCollector*, const std::string&) { return false; }
+
+namespace {
+
+std::vector<uint32_t> load(const char* path, size_t n)
+{
+    std::vector<uint32_t> v(n);
+    std::ifstream f(path, std::ios::binary);
+    f.read(reinterpret_cast<char*>(v.data()), n * 4);
+    if ((size_t)f.gcount() != n * 4) {
+        std::cerr << "short read " << path << "\n";
+        std::exit(2);
+    }
+    return v;
+}
+
+void save(const char* path, const uint32_t* w, size_t n)
+{
+    std::ofstream f(path, std::ios::binary);
+    f.write(reinterpret_cast<const char*>(w), n * 4);
+}
+
+void print_r(const Kpz::Roughness& r)
+{
+    std::cout << std::setprecision(17) << (double)r.w2;
+    for (int k = 0; k < Kpz::Roughness::H_ORDERS; ++k) std::cout << ' ' << (double)r.h[k];
+}
+
+template <class S>
+void setup(S& s, const char* in, Kpz::SchedulerService::Encoding enc)
+{
+    if (std::string(in) == "flat") {
+        s.initHomogeneous(enc);
+    } else {
+        s.initHomogeneous(enc);
+        auto v = load(in, s.size().sizeW());
+        std::memcpy(s.system(), v.data(), v.size() * 4);
+    }
+    s.pushSystem();
+}
+
+double now()
+{
+    return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+}  // namespace
+
+int main(int argc, char** argv)
+{
+    std::cout.setf(std::ios::unitbuf);
+    if (argc < 2) {
+        std::cerr << "usage: see header\n";
+        return 2;
+    }
+    const std::string cmd = argv[1];
+    // silence the reference's banners on stdout
+    std::streambuf* keep = std::cout.rdbuf();
+    std::ostringstream sink;
+    auto quiet = [&]() { std::cout.rdbuf(sink.rdbuf()); };
+    auto loud = [&]() { std::cout.rdbuf(keep); };
+
+    if (cmd == "rs") {
+        const int lx = std::atoi(argv[2]);
+        const int seed = std::atoi(argv[3]);
+        quiet();
+        Kpz::SchedulerCPU s(lx, lx);
+        s.supplySeed(1, seed);
+        s.initHomogeneous(Kpz::SchedulerService::ENC_LOCAL);
+        s.pushSystem();
+        loud();
+        int t = 0;
+        for (int i = 4; i < argc - 1; ++i) {
+            const int target = std::atoi(argv[i]);
+            quiet();
+            s.mcs(target - t);
+            s.popSystem();
+            loud();
+            t = target;
+            std::cout << t << ' ';
+            print_r(s.roughness());
+            std::cout << '\n';
+        }
+        save(argv[argc - 1], s.system(), s.size().sizeW());
+        return 0;
+    }
+    if (cmd == "cbbit" || cmd == "cb") {
+        const int lx = std::atoi(argv[2]);
+        const double p = std::atof(argv[3]), q = std::atof(argv[4]);
+        const int n = std::atoi(argv[5]);
+        const int thr = argc > 8 ? std::atoi(argv[8]) : 1;
+        quiet();
+        if (cmd == "cbbit") {
+            Kpz::SchedulerCPUCBBit<Kpz::RngIface::TinyMT32> s(lx, lx, thr);
+            s.supplySeed(1, 1);
+            s.randomize();
+            setup(s, argv[6], Kpz::SchedulerService::ENC_CBBIT);
+            s.setPQ(p, q);
+            s.mcsPQSyncRng(n);
+            s.popSystem();
+            loud();
+            save(argv[7], s.system(), s.size().sizeW());
+        } else {
+            Kpz::SchedulerCPUCB<Kpz::RngIface::TinyMT32> s(lx, lx, thr);
+            s.supplySeed(1, 1);
+            s.randomize();
+            setup(s, argv[6], Kpz::SchedulerService::ENC_LOCAL);
+            s.setPQ(p, q);
+            s.mcsPQSyncRng(n);
+            s.popSystem();
+            loud();
+            save(argv[7], s.system(), s.size().sizeW());
+        }
+        return 0;
+    }
+    if (cmd == "rough" || cmd == "check" || cmd == "corr") {
+        const int enc = std::atoi(argv[2]);
+        const int lx = std::atoi(argv[3]);
+        quiet();
+        Kpz::SchedulerCPU s(lx, lx);
+        const auto e = enc ? Kpz::SchedulerService::ENC_CBBIT : Kpz::SchedulerService::ENC_LOCAL;
+        s.initHomogeneous(e);
+        // consitencyCheck divides by Correlator::nThreads(); setNThreads(n<=1) stores 0
+        // (kpz/correlator.cpp:699-705, kpz/schedulerService.cpp:812-814)
+        Kpz::Correlator::setNThreads(cmd == "check" ? 2 : 1);
+        loud();
+        if (cmd == "rough") {
+            auto v = load(argv[4], s.size().sizeW());
+            std::memcpy(s.system(), v.data(), v.size() * 4);
+            print_r(s.roughness());
+            std::cout << '\n';
+        } else if (cmd == "check") {
+            auto v = load(argv[4], s.size().sizeW());
+            std::memcpy(s.system(), v.data(), v.size() * 4);
+            quiet();
+            const bool ok = s.consitencyCheck(false, sink);
+            loud();
+            std::cout << (ok ? 1 : 0) << '\n';
+        } else {
+            auto snap = load(argv[4], s.size().sizeW());
+            auto sys = load(argv[5], s.size().sizeW());
+            std::memcpy(s.system(), snap.data(), snap.size() * 4);
+            Kpz::Correlator c(&s);
+            c.set(0);
+            std::memcpy(s.system(), sys.data(), sys.size() * 4);
+            Kpz::Roughness r = c.correlate();
+            print_r(r);
+            std::cout << ' ' << std::setprecision(17) << c.ch() << ' ' << c.cs() << '\n';
+        }
+        return 0;
+    }
+    if (cmd == "bench-cbbit") {
+        const int lx = std::atoi(argv[2]);
+        const double p = std::atof(argv[3]), q = std::atof(argv[4]);
+        const int n = std::atoi(argv[5]);
+        const int thr = std::atoi(argv[6]);
+        quiet();
+        Kpz::SchedulerCPUCBBit<Kpz::RngIface::TinyMT32> s(lx, lx, thr);
+        s.supplySeed(1, 1);
+        s.randomize();
+        s.initHomogeneous(Kpz::SchedulerService::ENC_CBBIT);
+        s.pushSystem();
+        s.setPQ(p, q);
+        const double t0 = now();
+        s.mcsPQSyncRng(n);
+        const double t1 = now();
+        loud();
+        std::cout << std::setprecision(9) << (double)s.size().size() * n / ((t1 - t0) * 1e9) << ' '
+                  << (t1 - t0) << '\n';
+        return 0;
+    }
+    if (cmd == "bench-rs") {
+        const int lx = std::atoi(argv[2]);
+        const int n = std::atoi(argv[3]);
+        quiet();
+        Kpz::SchedulerCPU s(lx, lx);
+        s.supplySeed(1, 1);
+        s.initHomogeneous(Kpz::SchedulerService::ENC_LOCAL);
+        s.pushSystem();
+        const double t0 = now();
+        s.mcs(n);
+        const double t1 = now();
+        loud();
+        std::cout << std::setprecision(9) << (double)s.size().size() * n / ((t1 - t0) * 1e9) << ' '
+                  << (t1 - t0) << '\n';
+        return 0;
+    }
+    std::cerr << "unknown command " << cmd << "\n";
+    return 2;
+}

@@ -49,6 +49,7 @@ SIGNATURES = {
     "kpzb_join": (C.c_int, [_vp]),
     "kpzb_set_fusion": (C.c_int, [_vp, C.c_int]),
     "kpzb_get_fusion": (C.c_int, [_vp, _intp]),
+    "kpzb_autotune": (C.c_int, [_vp, _intp, _intp, C.POINTER(C.c_float)]),
     "kpzb_push": (C.c_int, [_vp, _vp]),
     "kpzb_pop": (C.c_int, [_vp, _vp]),
     "kpzb_push_device": (C.c_int, [_vp, _vp]),

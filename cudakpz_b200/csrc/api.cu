@@ -5,6 +5,7 @@
 // busy-wait event loop, integer status codes instead of exceptions/exit, counter-based RNG
 // keyed by (seed, stream) instead of per-thread TinyMT/SLCG state.
 #include <cmath>
+#include <cstdlib>
 #include <cstdio>
 #include <cstring>
 #include <string>
@@ -185,15 +186,20 @@ extern "C" kpzb_status kpzb_set_fusion(kpzb_handle* h, int mcs_per_pass)
     return KPZB_OK;
 }
 
-extern "C" kpzb_status kpzb_get_fusion(const kpzb_handle* h, int* mcs_per_pass)
+static kpzb_status resolve_plan(kpzb_handle* h, Plan* plan);
+
+extern "C" kpzb_status kpzb_get_fusion(kpzb_handle* h, int* mcs_per_pass)
 {
     if (!h || !mcs_per_pass) return fail(KPZB_EINVAL, "null argument");
     if (h->dyn == KPZB_DYN_DT) {
         *mcs_per_pass = 1;
         return KPZB_OK;
     }
-    int k = h->fusion ? h->fusion : auto_fusion(h->lx, h->ly);
-    if (k > 1 && !scabit_fused_shape(h->lx, h->ly, k, h->sm_count, 0).ok) k = 1;
+    Plan p;
+    kpzb_status s = resolve_plan(h, &p);
+    if (s != KPZB_OK) return s;
+    int k = p.k;
+    if (k > 1 && !scabit_fused_shape_cps(h->lx, h->ly, k, p.cps, 0).ok) k = 1;
     *mcs_per_pass = k;
     return KPZB_OK;
 }
@@ -207,15 +213,53 @@ static uint64_t thresh_of(double p)
     return (uint64_t)t;
 }
 
+// The pass shape used for the current rates: the caller's choice, else the tuner's cached
+// or freshly measured choice (KPZB_AUTOTUNE=0 disables measuring), else the heuristic.
+static kpzb_status resolve_plan(kpzb_handle* h, Plan* plan)
+{
+    if (h->fusion > 0) {
+        *plan = Plan{h->fusion, 0, 0.f, false};
+        return KPZB_OK;
+    }
+    const uint64_t Tp = thresh_of(h->p), Tq = thresh_of(h->q);
+    if (lookup_plan(h->lx, h->ly, Tp, Tq, h->sm_count, plan)) return KPZB_OK;
+    const char* env = getenv("KPZB_AUTOTUNE");
+    if (env && env[0] == '0') {
+        *plan = default_plan(h->lx, h->ly);
+        return KPZB_OK;
+    }
+    KPZB_CU(tune_plan(h->d_sys, h->lx, h->ly, h->seed, h->stream_id, Tp, Tq, h->sm_count,
+                      reinterpret_cast<unsigned int*>(h->d_counters + 2), h->st, plan),
+            "autotune");
+    return KPZB_OK;
+}
+
+extern "C" kpzb_status kpzb_autotune(kpzb_handle* h, int* mcs_per_pass, int* ctas_per_sm,
+                                     float* ms_per_mcs)
+{
+    KPZB_CHECK_H(h);
+    if (h->dyn == KPZB_DYN_DT) return fail(KPZB_EUNSUPPORTED, "the tuner covers SCA/SCABit passes");
+    Plan p;
+    KPZB_CU(tune_plan(h->d_sys, h->lx, h->ly, h->seed, h->stream_id, thresh_of(h->p), thresh_of(h->q),
+                      h->sm_count, reinterpret_cast<unsigned int*>(h->d_counters + 2), h->st, &p),
+            "autotune");
+    if (mcs_per_pass) *mcs_per_pass = p.k;
+    if (ctas_per_sm) *ctas_per_sm = p.cps;
+    if (ms_per_mcs) *ms_per_mcs = p.ms_per_mcs;
+    return KPZB_OK;
+}
+
 static kpzb_status enqueue_sca(kpzb_handle* h, int n)
 {
     const uint64_t Tp = thresh_of(h->p), Tq = thresh_of(h->q);
     unsigned long long* cnt = h->count ? h->d_counters : nullptr;
     int done = 0;
-    int k = h->fusion;
-    if (k == 0) k = auto_fusion(h->lx, h->ly);
+    Plan plan;
+    kpzb_status ps = resolve_plan(h, &plan);
+    if (ps != KPZB_OK) return ps;
+    const int k = plan.k;
     if (k > 1) {
-        FusedShape fs = scabit_fused_shape(h->lx, h->ly, k, h->sm_count, 0);
+        FusedShape fs = scabit_fused_shape_cps(h->lx, h->ly, k, plan.cps, 0);
         if (fs.ok) {
             kpzb_status s = ensure_tmp(h);
             if (s != KPZB_OK) return s;

@@ -14,6 +14,20 @@ int sm_count_of(int device);
 // MCS per HBM pass picked for a lattice when the caller leaves fusion at 0.
 int auto_fusion(int lx, int ly);
 
+// SCABit pass shape: k MCS per HBM pass (1 = one launch per half-step), cps CTAs per SM
+// (0 = shape heuristic), and the measured cost when it came from the tuner.
+struct Plan {
+    int k;
+    int cps;
+    float ms_per_mcs;
+    bool tuned;
+};
+bool lookup_plan(int lx, int ly, uint64_t Tp, uint64_t Tq, int sm_count, Plan* out);
+Plan default_plan(int lx, int ly);
+cudaError_t tune_plan(uint32_t* d_src, int lx, int ly, uint64_t seed, uint32_t stream_id,
+                      uint64_t Tp, uint64_t Tq, int sm_count, unsigned int* d_err,
+                      cudaStream_t st, Plan* out);
+
 // Double-tiling random-sequential scheduler state (dt.cu).
 struct DtState {
     int grid = 0;

@@ -25,6 +25,8 @@ struct FusedShape {
     bool ok;
 };
 FusedShape scabit_fused_shape(int lx, int ly, int mcs_per_pass, int sm_count, size_t smem_optin);
+FusedShape scabit_fused_shape_cps(int lx, int ly, int mcs_per_pass, int ctas_per_sm,
+                                  size_t smem_optin);
 cudaError_t scabit_fused(const uint32_t* d_src, uint32_t* d_dst, int lx, int ly, uint32_t t0,
                          uint64_t seed, uint32_t stream_id, uint64_t Tp, uint64_t Tq,
                          const FusedShape& sh, unsigned long long* d_counters, unsigned int* d_err,

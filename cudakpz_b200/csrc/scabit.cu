@@ -236,7 +236,8 @@ scabit_fused_kernel(const uint32_t* __restrict__ src, uint32_t* __restrict__ dst
     const int64_t rows = 1ll << ly;
     const int H = 2 * k;
     const int R = B + 2 * H;
-    const int G = (int)(Wr / 4);
+    const int G = (int)(Wr / 4);  // 4-word groups per row
+    const int lgG = lx - 8;
     const uint64_t qsz = (uint64_t)R * Wr;  // words per quadrant slab in smem
     const int64_t y0 = (int64_t)blockIdx.x * B;
     const int Bc = (int)(rows - y0 < B ? rows - y0 : B);  // rows this CTA writes
@@ -292,12 +293,12 @@ scabit_fused_kernel(const uint32_t* __restrict__ src, uint32_t* __restrict__ dst
         uint32_t* SoX = smem + (sigma ? 0 : 2) * qsz;
         uint32_t* SoY = SoX + qsz;
         const int ra = h, rb = R - 1 - h;
-        const int items = (rb - ra) * G;
+        const int items = (rb - ra) << lgG;
         for (int it = threadIdx.x; it < items; it += FUSED_THREADS) {
-            const int lr = ra + it / G;
-            const int g = it - (lr - ra) * G;
+            const int lr = ra + (it >> lgG);
+            const int g = it & (G - 1);
             const uint64_t w0 = 4ull * g;
-            const int64_t gy = (((ylo + lr) % rows) + rows) % rows;
+            const int64_t gy = (ylo + lr) & (rows - 1);  // periodic in y (rows is 2^ly)
             const bool shifted = sigma != (int)(gy & 1);
             uint4* ptX = reinterpret_cast<uint4*>(StX + (uint64_t)lr * Wr + w0);
             uint4* ptY = reinterpret_cast<uint4*>(StY + (uint64_t)lr * Wr + w0);
@@ -381,6 +382,14 @@ int auto_fusion(int lx, int ly)
 
 FusedShape scabit_fused_shape(int lx, int ly, int mcs_per_pass, int sm_count, size_t smem_optin)
 {
+    return scabit_fused_shape_cps(lx, ly, mcs_per_pass, 0, smem_optin);
+}
+
+// ctas_per_sm: 1 or 2 CTAs resident per SM (2 lets one CTA's TMA load overlap the other's
+// compute); 0 picks 2 when the band stays at least as tall as the halo, else 1.
+FusedShape scabit_fused_shape_cps(int lx, int ly, int mcs_per_pass, int ctas_per_sm,
+                                  size_t smem_optin)
+{
     FusedShape f{};
     f.ok = false;
     if (smem_optin == 0) smem_optin = 227 * 1024;
@@ -389,11 +398,15 @@ FusedShape scabit_fused_shape(int lx, int ly, int mcs_per_pass, int sm_count, si
     const int64_t rows = 1ll << ly;
     const int k = mcs_per_pass;
     if (k < 1) return f;
-    // two CTAs per SM when the band stays at least as tall as the halo, else one
     const size_t budget2 = (228 * 1024) / 2 - 2048;
     const size_t budget1 = smem_optin - 1024;
-    int R = (int)(budget2 / row_bytes);
-    if (R - 4 * k < 4 * k) R = (int)(budget1 / row_bytes);
+    int R;
+    if (ctas_per_sm == 2) R = (int)(budget2 / row_bytes);
+    else if (ctas_per_sm == 1) R = (int)(budget1 / row_bytes);
+    else {
+        R = (int)(budget2 / row_bytes);
+        if (R - 4 * k < 4 * k) R = (int)(budget1 / row_bytes);
+    }
     int B = R - 4 * k;
     if (B < 1) return f;
     if (B > rows) B = (int)rows;
@@ -406,7 +419,6 @@ FusedShape scabit_fused_shape(int lx, int ly, int mcs_per_pass, int sm_count, si
     f.smem = (size_t)R * row_bytes;
     f.grid = (int)((rows + B - 1) / B);
     f.ok = true;  // the load loop handles halos that wrap the lattice more than once
-    (void)sm_count;
     return f;
 }
 

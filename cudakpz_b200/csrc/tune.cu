@@ -1,0 +1,162 @@
+// tune.cu -- autotuner for the SCABit pass shape (MCS per HBM pass, CTAs per SM).
+//
+// Every shape produces bit-identical lattices (the random stream is indexed by site and
+// half-step, not by thread), so the tuner is free to time real passes on scratch copies of
+// the lattice and keep the fastest.  Results are cached per (lattice size, rate class,
+// SM count) in memory and, when KPZB_TUNE_CACHE names a file, in that file
+// (one "key k cps ms_per_mcs" line per entry).
+#include <cstdio>
+#include <cstdlib>
+#include <map>
+#include <mutex>
+#include <string>
+#include <utility>
+#include <vector>
+
+#include "kpzb_api_internal.h"
+#include "kpzb_common.cuh"
+#include "kpzb_internal.h"
+
+namespace kpzb {
+
+namespace {
+std::mutex g_mu;
+std::map<std::string, Plan> g_plans;
+bool g_file_loaded = false;
+
+std::string plan_key(int lx, int ly, uint64_t Tp, uint64_t Tq, int sm_count)
+{
+    // rates enter the cost only through the number of random planes the decision needs
+    const Thresh a = make_thresh(Tp), b = make_thresh(Tq);
+    const int planes = a.planes > b.planes ? a.planes : b.planes;
+    const int pclass = planes == 0 ? 0 : planes == 1 ? 1 : planes <= 4 ? 2 : 3;
+    char buf[96];
+    snprintf(buf, sizeof buf, "scabit:%d:%d:rng%d:sm%d", lx, ly, pclass, sm_count);
+    return buf;
+}
+
+void load_file()
+{
+    if (g_file_loaded) return;
+    g_file_loaded = true;
+    const char* path = getenv("KPZB_TUNE_CACHE");
+    if (!path) return;
+    FILE* f = fopen(path, "r");
+    if (!f) return;
+    char key[96];
+    int k, cps;
+    float ms;
+    while (fscanf(f, "%95s %d %d %f", key, &k, &cps, &ms) == 4) g_plans[key] = Plan{k, cps, ms, true};
+    fclose(f);
+}
+
+void save_file()
+{
+    const char* path = getenv("KPZB_TUNE_CACHE");
+    if (!path) return;
+    FILE* f = fopen(path, "w");
+    if (!f) return;
+    for (const auto& kv : g_plans)
+        fprintf(f, "%s %d %d %.6f\n", kv.first.c_str(), kv.second.k, kv.second.cps, kv.second.ms_per_mcs);
+    fclose(f);
+}
+}  // namespace
+
+bool lookup_plan(int lx, int ly, uint64_t Tp, uint64_t Tq, int sm_count, Plan* out)
+{
+    std::lock_guard<std::mutex> lk(g_mu);
+    load_file();
+    auto it = g_plans.find(plan_key(lx, ly, Tp, Tq, sm_count));
+    if (it == g_plans.end()) return false;
+    *out = it->second;
+    return true;
+}
+
+Plan default_plan(int lx, int ly)
+{
+    const int k = auto_fusion(lx, ly);
+    return Plan{k, 0, 0.f, false};
+}
+
+cudaError_t tune_plan(uint32_t* d_src, int lx, int ly, uint64_t seed, uint32_t stream_id,
+                      uint64_t Tp, uint64_t Tq, int sm_count, unsigned int* d_err,
+                      cudaStream_t st, Plan* out)
+{
+    const size_t bytes = (size_t)1 << (lx + ly - 2);
+    uint32_t *a = nullptr, *b = nullptr;
+    cudaError_t e;
+    if ((e = cudaMallocAsync(&a, bytes, st)) != cudaSuccess) return e;
+    if ((e = cudaMallocAsync(&b, bytes, st)) != cudaSuccess) {
+        cudaFreeAsync(a, st);
+        return e;
+    }
+    cudaMemcpyAsync(a, d_src, bytes, cudaMemcpyDeviceToDevice, st);
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+
+    struct Cand {
+        int k, cps;
+    };
+    std::vector<Cand> cands{{1, 0}};
+    for (int k = 2; k <= 8; ++k)
+        for (int cps = 1; cps <= 2; ++cps) {
+            FusedShape f = scabit_fused_shape_cps(lx, ly, k, cps, 0);
+            if (f.ok && f.band >= 2) cands.push_back({k, cps});
+        }
+    Plan best{1, 0, 1e30f, true};
+    const ScabitShape hs = scabit_shape(lx, ly, sm_count);
+    for (const Cand& c : cands) {
+        // enough MCS per measurement to dwarf launch overhead, capped by lattice size
+        const int target = (lx + ly >= 26) ? 8 : 32;
+        auto run = [&](int mcs) -> cudaError_t {
+            if (c.k == 1) {
+                for (int m = 0; m < mcs; ++m)
+                    for (int sg = 0; sg < 2; ++sg) {
+                        cudaError_t r = scabit_half(a, lx, ly, sg, (uint32_t)(2 * m + sg), seed,
+                                                    stream_id, Tp, Tq, hs, nullptr, st);
+                        if (r != cudaSuccess) return r;
+                    }
+                return cudaSuccess;
+            }
+            const FusedShape f = scabit_fused_shape_cps(lx, ly, c.k, c.cps, 0);
+            uint32_t *s = a, *d = b;
+            for (int m = 0; m + c.k <= mcs; m += c.k) {
+                cudaError_t r = scabit_fused(s, d, lx, ly, (uint32_t)m, seed, stream_id, Tp, Tq, f,
+                                             nullptr, d_err, st);
+                if (r != cudaSuccess) return r;
+                std::swap(s, d);
+            }
+            return cudaSuccess;
+        };
+        int mcs = c.k == 1 ? target / 2 : c.k * ((target + c.k - 1) / c.k);
+        if ((e = run(c.k == 1 ? 1 : c.k)) != cudaSuccess) break;  // warm-up
+        cudaEventRecord(e0, st);
+        if ((e = run(mcs)) != cudaSuccess) break;
+        cudaEventRecord(e1, st);
+        if ((e = cudaEventSynchronize(e1)) != cudaSuccess) break;
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        const float per = ms / (float)mcs;
+        if (getenv("KPZB_TUNE_VERBOSE"))
+            fprintf(stderr, "kpzb tune lx=%d ly=%d k=%d cps=%d: %.4f ms/MCS, %.1f upd/ns\n", lx, ly,
+                    c.k, c.cps, per, (double)(1ull << (lx + ly)) / (per * 1e6));
+        if (per < best.ms_per_mcs) best = Plan{c.k, c.cps, per, true};
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaFreeAsync(a, st);
+    cudaFreeAsync(b, st);
+    cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return e;
+    {
+        std::lock_guard<std::mutex> lk(g_mu);
+        load_file();
+        g_plans[plan_key(lx, ly, Tp, Tq, sm_count)] = best;
+        save_file();
+    }
+    *out = best;
+    return cudaSuccess;
+}
+
+}  // namespace kpzb

@@ -119,6 +119,13 @@ class Scheduler:
         check(lib.kpzb_get_fusion(self._h, C.byref(v)), "kpzb_get_fusion")
         return int(v.value)
 
+    def autotune(self):
+        """Measure the pass shapes for the current rates; returns (mcs_per_pass, ctas_per_sm,
+        ms_per_mcs) of the fastest."""
+        k, c, ms = C.c_int(), C.c_int(), C.c_float()
+        check(lib.kpzb_autotune(self._h, C.byref(k), C.byref(c), C.byref(ms)), "kpzb_autotune")
+        return int(k.value), int(c.value), float(ms.value)
+
     def enableCounters(self, on: bool = True) -> None:
         check(lib.kpzb_enable_counters(self._h, int(on)), "kpzb_enable_counters")
 

@@ -83,10 +83,17 @@ kpzb_status kpzb_mcs(kpzb_handle* h, int n);
 kpzb_status kpzb_mcs_async(kpzb_handle* h, int n);
 kpzb_status kpzb_join(kpzb_handle* h);
 /* SCA/SCABit only: MCS per HBM pass of the temporally blocked kernel (1 = one launch per
- * half-step; 0 = automatic).  Results are identical for every value. */
+ * half-step; 0 = automatic: the autotuner's choice).  Results are identical for every value. */
 kpzb_status kpzb_set_fusion(kpzb_handle* h, int mcs_per_pass);
-/* The MCS per pass the handle actually uses (the automatic choice resolved). */
-kpzb_status kpzb_get_fusion(const kpzb_handle* h, int* mcs_per_pass);
+/* The MCS per pass the handle uses for its current rates (resolving the automatic choice,
+ * which may run the autotuner once). */
+kpzb_status kpzb_get_fusion(kpzb_handle* h, int* mcs_per_pass);
+/* Time every pass shape (MCS per pass x CTAs per SM) on scratch copies of the current
+ * lattice and cache the fastest for this size and rate class (in memory, and in the file
+ * named by KPZB_TUNE_CACHE if set).  The lattice itself is not modified.  No reference
+ * counterpart: replaces the fixed LocalLayout presets (kpz/schedulerDT.h:32-47) and the
+ * per-architecture block counts (kpz/kpzSCABit.cu:63-106) with measured choices. */
+kpzb_status kpzb_autotune(kpzb_handle* h, int* mcs_per_pass, int* ctas_per_sm, float* ms_per_mcs);
 
 /* SchedulerService::pushSystem / popSystem (kpz/schedulerBase.cu:35-52): copy host words
  * in the handle's encoding (kpzb_size_words words) to / from the device. */

@@ -186,6 +186,17 @@ int main(int argc, char** argv)
         }
         return 0;
     }
+    if (cmd == "dsfmt") {
+        // dSFMT-19937 draws of the reference's vendored generator: SEED N [reseed]
+        dsfmt_t d;
+        dsfmt_init_gen_rand(&d, (uint32_t)std::atoi(argv[2]));
+        if (argc > 4)
+            for (int a = 0; a < 100000; ++a) dsfmt_genrand_close_open(&d);
+        const int n = std::atoi(argv[3]);
+        for (int i = 0; i < n; ++i)
+            std::cout << std::setprecision(17) << dsfmt_genrand_close_open(&d) << '\n';
+        return 0;
+    }
     if (cmd == "bench-cbbit") {
         const int lx = std::atoi(argv[2]);
         const double p = std::atof(argv[3]), q = std::atof(argv[4]);

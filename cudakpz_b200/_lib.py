@@ -73,6 +73,8 @@ SIGNATURES = {
     "kpzb_batch_destroy": (C.c_int, [_vp]),
     "kpzb_batch_init_homogeneous": (C.c_int, [_vp]),
     "kpzb_batch_mcs": (C.c_int, [_vp, C.c_int]),
+    "kpzb_batch_set_fusion": (C.c_int, [_vp, C.c_int, C.c_int]),
+    "kpzb_batch_get_mcs": (C.c_int, [_vp, _u64p]),
     "kpzb_batch_push": (C.c_int, [_vp, C.c_int, _vp]),
     "kpzb_batch_pop": (C.c_int, [_vp, C.c_int, _vp]),
     "kpzb_batch_roughness": (C.c_int, [_vp, _dblp]),

@@ -95,8 +95,8 @@ extern "C" kpzb_status kpzb_create(kpzb_handle** out, int lx, int ly, int dynami
     if (lx < 8 || lx > 30 || ly < 2 || ly > 30 || lx + ly > 38 || lx + ly < 14)
         return fail(KPZB_EINVAL,
                     "lattice size out of range (8<=lx<=30, 2<=ly<=30, 14<=lx+ly<=38)");
-    if (dynamics == KPZB_DYN_DT && (lx < 10 || ly < 10))
-        return fail(KPZB_EINVAL, "DT needs lx, ly >= 10 (one double tile of 512x512 sites)");
+    if (dynamics == KPZB_DYN_DT && (lx < 9 || ly < 8))
+        return fail(KPZB_EINVAL, "DT needs lx >= 9 and ly >= 8 (one double tile of 512x256 sites)");
     int dev = device;
     if (dev < 0) {
         cudaError_t e = cudaGetDevice(&dev);
@@ -292,7 +292,7 @@ extern "C" kpzb_status kpzb_mcs_async(kpzb_handle* h, int n)
     kpzb_status s;
     if (h->dyn == KPZB_DYN_DT)
         s = dt_enqueue(&h->dt, h->d_sys, h->lx, h->ly, h->tdev, n, h->p, h->q, h->seed, h->stream_id,
-                       h->st);
+                       h->st, h->count ? h->d_counters : nullptr);
     else
         s = enqueue_sca(h, n);
     if (s != KPZB_OK) return s;

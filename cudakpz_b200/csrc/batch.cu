@@ -1,21 +1,386 @@
-// batch.cu -- batched replicas (placeholder until the batched kernel lands).
+// batch.cu -- many independent SCABit lattices of uneven size in one persistent kernel.
+//
+// Replaces the per-lattice launch loop (one SchedulerSCABit per lattice, two launches per
+// MCS each: kpz/schedulerSCABit.cu:46-73, driven by kpz/kpzScaling.cpp:194-215) with a work
+// queue: every pass advances ALL replicas by k MCS.  Work items are (replica, band) pairs,
+// sorted by cost, pulled by persistent CTAs (one per SM) from a global atomic counter.
+// Lattices that fit in shared memory are resident (whole lattice, periodic, no halo);
+// larger ones are cut into bands with a 2k-row halo (scabit_band.cuh).  The pass index
+// (t, buffer parity) lives in device memory and a one-thread kernel advances it after each
+// pass, so a chunk of passes is captured once as a CUDA graph and replayed.
+// Per-replica results are bit-identical to single runs: the random stream depends only on
+// (seed, stream, half-step, site).
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
 #include "kpzb_api_internal.h"
+#include "kpzb_common.cuh"
+#include "kpzb_internal.h"
+#include "scabit_band.cuh"
+
+namespace kpzb {
+
+constexpr int BATCH_THREADS = 512;
+constexpr size_t BATCH_SMEM = 227 * 1024 - 1024;
+
+struct RepDesc {
+    uint32_t* buf[2];  // double buffer; buf[parity] holds the current state
+    int lx, ly;
+    int B;             // band rows (rows when resident)
+    int resident;
+    Key key;
+    uint32_t stream;
+    Thresh tp, tq;
+};
+
+struct Item {
+    int rep;
+    int band;
+};
+
+struct PassState {
+    uint32_t t;       // MCS index of the next pass
+    uint32_t parity;  // buffer holding the current state
+    uint32_t queue;   // work-queue head for the running pass
+    uint32_t err;     // set when a bounded wait expired
+};
+
+__global__ void __launch_bounds__(BATCH_THREADS)
+batch_pass_kernel(const RepDesc* __restrict__ reps, const Item* __restrict__ items, int nitems,
+                  PassState* st, int k)
+{
+    extern __shared__ __align__(128) uint32_t smem[];
+    __shared__ __align__(8) uint64_t bar;
+    __shared__ int abort_flag;
+    __shared__ int cur;
+    if (threadIdx.x == 0) {
+        mbar_init(&bar, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    const uint32_t t0 = st->t;
+    const uint32_t par = st->parity;
+    uint32_t phase = 0;
+    unsigned long long nd = 0, nr = 0;
+    for (;;) {
+        if (threadIdx.x == 0) cur = (int)atomicAdd(&st->queue, 1u);
+        __syncthreads();
+        const int i = cur;
+        __syncthreads();
+        if (i >= nitems) break;
+        const Item it = items[i];
+        const RepDesc r = reps[it.rep];
+        const BandCtl ctl{&bar, &abort_flag, phase};
+        const BandGeom g{r.buf[par], r.buf[par ^ 1u], r.lx, r.ly, (int64_t)it.band * r.B, r.B, k,
+                         r.resident != 0, t0, r.key, r.stream, r.tp, r.tq};
+        if (!scabit_band<false, BATCH_THREADS>(smem, ctl, g, nd, nr, &st->err)) return;
+        phase ^= 1u;
+    }
+}
+
+__global__ void batch_advance_kernel(PassState* st, int k)
+{
+    st->t += (uint32_t)k;
+    st->parity ^= 1u;
+    st->queue = 0;
+}
+
+}  // namespace kpzb
 
 using namespace kpzb;
+
 struct kpzb_batch {
-    int n;
+    int n = 0, device = 0, sm_count = 148;
+    cudaStream_t st = nullptr;
+    std::vector<int> lx;
+    std::vector<double> p, q;
+    std::vector<uint64_t> seed;
+    std::vector<uint32_t> stream;
+    std::vector<RepDesc> reps;  // host copy
+    RepDesc* d_reps = nullptr;
+    Item* d_items = nullptr;
+    int nitems = 0;
+    PassState* d_state = nullptr;
+    uint32_t t = 0, parity = 0;  // host mirror of the pass state
+    int k = 8;                   // MCS per pass
+    int chunk = 8;               // passes per graph replay
+    cudaGraphExec_t graph = nullptr;
+    AnalysisScratch an{};
+    int max_ly = 0;
 };
-extern "C" {
-kpzb_status kpzb_batch_create(kpzb_batch** b, int, const int*, const double*, const double*,
-                              const uint64_t*, const uint32_t*, int)
+
+static uint64_t thresh_b(double p)
 {
-    if (b) *b = nullptr;
-    return fail(KPZB_EUNSUPPORTED, "batch not built yet");
+    if (!(p > 0.0)) return 0;
+    if (p >= 1.0) return 1ull << 32;
+    const double t = std::ceil(p * 4294967296.0);
+    return t >= 4294967296.0 ? (1ull << 32) : (uint64_t)t;
 }
-kpzb_status kpzb_batch_destroy(kpzb_batch*) { return KPZB_OK; }
-kpzb_status kpzb_batch_init_homogeneous(kpzb_batch*) { return fail(KPZB_EUNSUPPORTED, "batch"); }
-kpzb_status kpzb_batch_mcs(kpzb_batch*, int) { return fail(KPZB_EUNSUPPORTED, "batch"); }
-kpzb_status kpzb_batch_push(kpzb_batch*, int, const uint32_t*) { return fail(KPZB_EUNSUPPORTED, "batch"); }
-kpzb_status kpzb_batch_pop(kpzb_batch*, int, uint32_t*) { return fail(KPZB_EUNSUPPORTED, "batch"); }
-kpzb_status kpzb_batch_roughness(kpzb_batch*, double*) { return fail(KPZB_EUNSUPPORTED, "batch"); }
+
+// (Re)build the band layout and work list for MCS-per-pass k.
+static kpzb_status batch_layout(kpzb_batch* b)
+{
+    // passes in flight read the descriptor table and the work list
+    if (b->st) {
+        const cudaError_t se = cudaStreamSynchronize(b->st);
+        if (se != cudaSuccess) return cuda_fail(se, "batch sync");
+    }
+    std::vector<std::pair<double, Item>> work;
+    for (int i = 0; i < b->n; ++i) {
+        RepDesc& r = b->reps[i];
+        const uint64_t Wr = 1ull << (r.lx - 6);
+        const uint64_t row_bytes = 16ull * Wr;
+        const int64_t rows = 1ll << r.ly;
+        if ((uint64_t)rows * row_bytes <= BATCH_SMEM) {
+            r.resident = 1;
+            r.B = (int)rows;
+            work.push_back({(double)rows * Wr, Item{i, 0}});
+            continue;
+        }
+        r.resident = 0;
+        const int Rmax = (int)(BATCH_SMEM / row_bytes);
+        const int Bmax = Rmax - 4 * b->k;
+        if (Bmax < 1) return fail(KPZB_EINVAL, "batch: lattice rows too wide for the pass depth");
+        const int nb = (int)((rows + Bmax - 1) / Bmax);
+        r.B = (int)((rows + nb - 1) / nb);
+        for (int band = 0; band < nb; ++band)
+            work.push_back({(double)(r.B + 4 * b->k) * Wr, Item{i, band}});
+    }
+    std::stable_sort(work.begin(), work.end(),
+                     [](const std::pair<double, Item>& a, const std::pair<double, Item>& c) {
+                         return a.first > c.first;
+                     });
+    std::vector<Item> items;
+    for (auto& w : work) items.push_back(w.second);
+    b->nitems = (int)items.size();
+    cudaFree(b->d_items);
+    b->d_items = nullptr;
+    cudaError_t e;
+    if ((e = cudaMalloc(&b->d_items, items.size() * sizeof(Item))) != cudaSuccess)
+        return cuda_fail(e, "cudaMalloc(items)");
+    cudaMemcpy(b->d_items, items.data(), items.size() * sizeof(Item), cudaMemcpyHostToDevice);
+    cudaMemcpy(b->d_reps, b->reps.data(), b->reps.size() * sizeof(RepDesc), cudaMemcpyHostToDevice);
+    if (b->graph) {
+        cudaGraphExecDestroy(b->graph);
+        b->graph = nullptr;
+    }
+    return KPZB_OK;
+}
+
+static cudaError_t enqueue_pass(kpzb_batch* b)
+{
+    batch_pass_kernel<<<b->sm_count, BATCH_THREADS, BATCH_SMEM, b->st>>>(b->d_reps, b->d_items,
+                                                                         b->nitems, b->d_state, b->k);
+    batch_advance_kernel<<<1, 1, 0, b->st>>>(b->d_state, b->k);
+    return cudaGetLastError();
+}
+
+#define BCHECK(b)                                                       \
+    do {                                                                \
+        if (!(b)) return fail(KPZB_EINVAL, "null batch");               \
+        cudaError_t _e = cudaSetDevice((b)->device);                    \
+        if (_e != cudaSuccess) return cuda_fail(_e, "cudaSetDevice");   \
+    } while (0)
+
+extern "C" kpzb_status kpzb_batch_create(kpzb_batch** out, int n, const int* lx, const double* p,
+                                         const double* q, const uint64_t* seed,
+                                         const uint32_t* stream, int device)
+{
+    if (!out || n <= 0 || !lx || !p || !q || !seed) return fail(KPZB_EINVAL, "bad batch arguments");
+    *out = nullptr;
+    for (int i = 0; i < n; ++i) {
+        if (lx[i] < 8 || lx[i] > 16 || 2 * lx[i] < 14)
+            return fail(KPZB_EINVAL, "batch lattices are square with 8 <= lx <= 16");
+        if (!(p[i] >= 0 && p[i] <= 1 && q[i] >= 0 && q[i] <= 1)) return fail(KPZB_EINVAL, "p, q in [0,1]");
+    }
+    int dev = device;
+    if (dev < 0 && cudaGetDevice(&dev) != cudaSuccess) return fail(KPZB_ECUDA, "cudaGetDevice");
+    cudaError_t e = cudaSetDevice(dev);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaSetDevice");
+    kpzb_batch* b = new kpzb_batch();
+    b->n = n;
+    b->device = dev;
+    b->sm_count = sm_count_of(dev);
+    auto bail = [&](kpzb_status s) {
+        kpzb_batch_destroy(b);
+        return s;
+    };
+    if ((e = cudaStreamCreateWithFlags(&b->st, cudaStreamNonBlocking)) != cudaSuccess)
+        return bail(cuda_fail(e, "cudaStreamCreate"));
+    b->reps.resize(n);
+    for (int i = 0; i < n; ++i) {
+        b->lx.push_back(lx[i]);
+        b->p.push_back(p[i]);
+        b->q.push_back(q[i]);
+        b->seed.push_back(seed[i]);
+        b->stream.push_back(stream ? stream[i] : 0u);
+        RepDesc& r = b->reps[i];
+        r.lx = r.ly = lx[i];
+        r.key = make_key(seed[i]);
+        r.stream = stream ? stream[i] : 0u;
+        r.tp = make_thresh(thresh_b(p[i]));
+        r.tq = make_thresh(thresh_b(q[i]));
+        const size_t bytes = (size_t)1 << (2 * lx[i] - 2);
+        for (int s = 0; s < 2; ++s)
+            if ((e = cudaMalloc(&r.buf[s], bytes)) != cudaSuccess) return bail(cuda_fail(e, "cudaMalloc(replica)"));
+        b->max_ly = std::max(b->max_ly, lx[i]);
+    }
+    if ((e = cudaMalloc(&b->d_reps, n * sizeof(RepDesc))) != cudaSuccess)
+        return bail(cuda_fail(e, "cudaMalloc(reps)"));
+    if ((e = cudaMalloc(&b->d_state, sizeof(PassState))) != cudaSuccess)
+        return bail(cuda_fail(e, "cudaMalloc(state)"));
+    cudaMemset(b->d_state, 0, sizeof(PassState));
+    if ((e = analysis_alloc(&b->an, b->max_ly)) != cudaSuccess) return bail(cuda_fail(e, "analysis_alloc"));
+    if ((e = cudaFuncSetAttribute(batch_pass_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)BATCH_SMEM)) != cudaSuccess)
+        return bail(cuda_fail(e, "smem attribute"));
+    kpzb_status s = batch_layout(b);
+    if (s != KPZB_OK) return bail(s);
+    s = kpzb_batch_init_homogeneous(b);
+    if (s != KPZB_OK) return bail(s);
+    *out = b;
+    return KPZB_OK;
+}
+
+extern "C" kpzb_status kpzb_batch_destroy(kpzb_batch* b)
+{
+    if (!b) return KPZB_OK;
+    cudaSetDevice(b->device);
+    if (b->st) cudaStreamSynchronize(b->st);
+    if (b->graph) cudaGraphExecDestroy(b->graph);
+    for (auto& r : b->reps) {
+        cudaFree(r.buf[0]);
+        cudaFree(r.buf[1]);
+    }
+    cudaFree(b->d_reps);
+    cudaFree(b->d_items);
+    cudaFree(b->d_state);
+    if (b->an.rowinfo) analysis_free(&b->an);
+    if (b->st) cudaStreamDestroy(b->st);
+    delete b;
+    return KPZB_OK;
+}
+
+extern "C" kpzb_status kpzb_batch_init_homogeneous(kpzb_batch* b)
+{
+    BCHECK(b);
+    for (auto& r : b->reps) {
+        cudaError_t e = init_homogeneous_dev(r.buf[b->parity], r.lx, r.ly, KPZB_ENC_CBBIT, b->st);
+        if (e != cudaSuccess) return cuda_fail(e, "batch init");
+    }
+    const cudaError_t e = cudaStreamSynchronize(b->st);
+    return e == cudaSuccess ? KPZB_OK : cuda_fail(e, "batch init sync");
+}
+
+extern "C" kpzb_status kpzb_batch_set_fusion(kpzb_batch* b, int mcs_per_pass, int passes_per_graph)
+{
+    BCHECK(b);
+    if (mcs_per_pass < 1 || mcs_per_pass > 32 || passes_per_graph < 1 || passes_per_graph > 256)
+        return fail(KPZB_EINVAL, "batch fusion: 1 <= mcs_per_pass <= 32, 1 <= passes_per_graph <= 256");
+    b->k = mcs_per_pass;
+    b->chunk = passes_per_graph;
+    return batch_layout(b);
+}
+
+// n MCS for every replica: whole passes of k MCS (graph replays of `chunk` passes, then
+// single passes), and a final pass of n mod k MCS.
+extern "C" kpzb_status kpzb_batch_mcs(kpzb_batch* b, int n)
+{
+    BCHECK(b);
+    if (n < 0) return fail(KPZB_EINVAL, "negative MCS count");
+    if ((uint64_t)b->t + (uint64_t)n >= (1ull << 31)) return fail(KPZB_EINVAL, "MCS counter limit 2^31");
+    cudaError_t e;
+    int passes = n / b->k;
+    const int rem = n % b->k;
+    while (passes >= b->chunk) {
+        if (!b->graph) {
+            cudaGraph_t g;
+            if ((e = cudaStreamBeginCapture(b->st, cudaStreamCaptureModeThreadLocal)) != cudaSuccess)
+                return cuda_fail(e, "begin capture");
+            for (int i = 0; i < b->chunk; ++i) enqueue_pass(b);
+            if ((e = cudaStreamEndCapture(b->st, &g)) != cudaSuccess) return cuda_fail(e, "end capture");
+            e = cudaGraphInstantiate(&b->graph, g, 0);
+            cudaGraphDestroy(g);
+            if (e != cudaSuccess) return cuda_fail(e, "graph instantiate");
+        }
+        if ((e = cudaGraphLaunch(b->graph, b->st)) != cudaSuccess) return cuda_fail(e, "graph launch");
+        passes -= b->chunk;
+        b->t += (uint32_t)(b->chunk * b->k);
+        b->parity ^= (uint32_t)(b->chunk & 1);
+    }
+    for (; passes > 0; --passes) {
+        if ((e = enqueue_pass(b)) != cudaSuccess) return cuda_fail(e, "batch pass");
+        b->t += (uint32_t)b->k;
+        b->parity ^= 1u;
+    }
+    if (rem) {
+        // one shorter pass: temporarily rebuild the bands for depth rem
+        const int k = b->k;
+        b->k = rem;
+        kpzb_status s = batch_layout(b);
+        if (s == KPZB_OK) {
+            e = enqueue_pass(b);
+            b->t += (uint32_t)rem;
+            b->parity ^= 1u;
+        }
+        b->k = k;
+        kpzb_status s2 = batch_layout(b);
+        if (s != KPZB_OK) return s;
+        if (s2 != KPZB_OK) return s2;
+        if (e != cudaSuccess) return cuda_fail(e, "batch pass");
+    }
+    PassState hs;
+    if ((e = cudaMemcpyAsync(&hs, b->d_state, sizeof hs, cudaMemcpyDeviceToHost, b->st)) != cudaSuccess)
+        return cuda_fail(e, "batch state");
+    if ((e = cudaStreamSynchronize(b->st)) != cudaSuccess) return cuda_fail(e, "batch sync");
+    if (hs.err) return fail(KPZB_ETIMEOUT, "a bounded device wait (TMA mbarrier) expired");
+    if (hs.t != b->t || hs.parity != b->parity) return fail(KPZB_ESTATE, "batch pass state out of step");
+    return KPZB_OK;
+}
+
+extern "C" kpzb_status kpzb_batch_push(kpzb_batch* b, int i, const uint32_t* words)
+{
+    BCHECK(b);
+    if (i < 0 || i >= b->n || !words) return fail(KPZB_EINVAL, "bad replica index or buffer");
+    const RepDesc& r = b->reps[i];
+    cudaError_t e = cudaStreamSynchronize(b->st);
+    if (e != cudaSuccess) return cuda_fail(e, "batch sync");
+    e = cudaMemcpy(r.buf[b->parity], words, (size_t)1 << (2 * r.lx - 2), cudaMemcpyHostToDevice);
+    return e == cudaSuccess ? KPZB_OK : cuda_fail(e, "batch push");
+}
+
+extern "C" kpzb_status kpzb_batch_pop(kpzb_batch* b, int i, uint32_t* words)
+{
+    BCHECK(b);
+    if (i < 0 || i >= b->n || !words) return fail(KPZB_EINVAL, "bad replica index or buffer");
+    const RepDesc& r = b->reps[i];
+    cudaError_t e = cudaStreamSynchronize(b->st);
+    if (e != cudaSuccess) return cuda_fail(e, "batch sync");
+    e = cudaMemcpy(words, r.buf[b->parity], (size_t)1 << (2 * r.lx - 2), cudaMemcpyDeviceToHost);
+    return e == cudaSuccess ? KPZB_OK : cuda_fail(e, "batch pop");
+}
+
+extern "C" kpzb_status kpzb_batch_roughness(kpzb_batch* b, double* w2)
+{
+    BCHECK(b);
+    if (!w2) return fail(KPZB_EINVAL, "null output");
+    for (int i = 0; i < b->n; ++i) {
+        const RepDesc& r = b->reps[i];
+        MomentsOut m;
+        const cudaError_t e = analysis_moments(r.buf[b->parity], nullptr, r.lx, r.ly, &b->an, &m, b->st);
+        if (e != cudaSuccess) return cuda_fail(e, "batch roughness");
+        const long double N = (long double)((uint64_t)1 << (2 * r.lx));
+        const long double h1 = (long double)m.s1 / N, h2 = (long double)m.s2 / N;
+        w2[i] = (double)(h2 - h1 * h1);
+    }
+    return KPZB_OK;
+}
+
+extern "C" kpzb_status kpzb_batch_get_mcs(const kpzb_batch* b, uint64_t* mcs)
+{
+    if (!b || !mcs) return fail(KPZB_EINVAL, "null argument");
+    *mcs = b->t;
+    return KPZB_OK;
 }

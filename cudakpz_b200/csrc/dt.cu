@@ -1,17 +1,217 @@
-// dt.cu -- double-tiling random-sequential dynamics (placeholder until the DT kernel lands).
+// dt.cu -- double-tiling (DT) random-sequential dynamics on ENC_LOCAL lattices (sm_100a).
+//
+// Reference behaviour: SchedulerDT::doMcs (kpz/schedulerDT.cu:38-78) -- per MCS a random
+// origin in [0, 2*block) and a shuffled order of the four domain sets, one launch per set;
+// kpzKernelTemplateDT + copyInDT/copyOutDT (kpz/kpz.cu:126-155, kpz/kpzCopy.cu:144-187) --
+// each block is copied with a one-word halo into shared memory, updated, copied back; the
+// inner single-hit double tiling of KpzCores::BaseDT
+// (kpz/kpzSimulationPrimitivesTemplates.cu:110-141) -- per attempt round the whole block
+// uses one random quadrant (sub-cell) of every thread cell, so the sites updated in a round
+// never share a word and need no atomics; the per-site rule of PQSyncRng
+// (kpz/kpzSimulationPrimitivesTemplates.cu:229-268).
+//
+// Geometry: 32x16 threads, thread cells of 8x8 sites (2x2 words), blocks of 256x128 sites
+// (64x32 words), shared tile 65x33 words, 64 rounds per launch (one attempt per site per
+// MCS).  All random numbers come from the counter stream (see oracle/kpz_oracle.h), so the
+// CPU emulation ko_dt_mcs reproduces every lattice bit for bit.
+#include <cmath>
+#include <cstring>
+
 #include "kpzb_api_internal.h"
 #include "kpzb_common.cuh"
+#include "kpzb_internal.h"
 
 namespace kpzb {
-kpzb_status dt_init(DtState* s, int, int, int)
+
+constexpr uint32_t TAG_DT_SUB = 4u;
+constexpr uint32_t TAG_DT_POS = 5u;
+constexpr int DT_TX = 32, DT_TY = 16;
+constexpr int DT_BXW = 64, DT_BYW = 32;           // block in words
+constexpr int DT_BX = 4 * DT_BXW, DT_BY = 4 * DT_BYW;  // block in sites
+constexpr int DT_TW = DT_BXW + 1, DT_TH = DT_BYW + 1;  // shared tile with halo
+constexpr int DT_ROUNDS = 64;
+
+template <bool COUNT>
+__global__ void __launch_bounds__(DT_TX* DT_TY)
+dt_kernel(uint32_t* __restrict__ sys, int lxw, int lyw, int lnbx, int nblocks, int ox, int oy,
+          int d, uint32_t t, Key key, uint32_t stream, Thresh tp, Thresh tq,
+          unsigned long long* __restrict__ counters)
 {
-    s->ready = false;
-    return fail(KPZB_EUNSUPPORTED, "DT dynamics not built yet");
+    __shared__ uint32_t tile[DT_TH * DT_TW];
+    const int tid = threadIdx.y * DT_TX + threadIdx.x;
+    const uint32_t Wx = 1u << lxw, Wy = 1u << lyw;
+    const bool need_u = !(tp.always || tp.planes == 0) || !(tq.always || tq.planes == 0);
+    unsigned long long ndep = 0, ndes = 0;
+
+    for (int b = blockIdx.x; b < nblocks; b += gridDim.x) {
+        const int bx = b & ((1 << lnbx) - 1), by = b >> lnbx;
+        const uint32_t X0 = (uint32_t)ox + (uint32_t)(2 * bx + (d & 1)) * DT_BX;
+        const uint32_t Y0 = (uint32_t)oy + (uint32_t)(2 * by + (d >> 1)) * DT_BY;
+        const uint32_t wx0 = X0 >> 2, wy0 = Y0 >> 2;
+        for (int i = tid; i < DT_TH * DT_TW; i += DT_TX * DT_TY) {
+            const uint32_t r = i / DT_TW, c = i - r * DT_TW;
+            tile[i] = sys[(size_t)((wy0 + r) & (Wy - 1)) * Wx + ((wx0 + c) & (Wx - 1))];
+        }
+        // block-wide sub-cell sequence: 2 bits per round (every thread derives the same words)
+        const uint4 sub = philox4x32_10(
+            make_uint4((uint32_t)b, t, (TAG_DT_SUB << 24) | ((uint32_t)d << 16), stream), key);
+        const uint32_t cid = (uint32_t)b * (DT_TX * DT_TY) + (uint32_t)tid;
+        const int sx0 = (int)(X0 & 3u) + threadIdx.x * 8;
+        const int sy0 = (int)(Y0 & 3u) + threadIdx.y * 8;
+        __syncthreads();
+        uint4 pos = make_uint4(0, 0, 0, 0), uu = make_uint4(0, 0, 0, 0);
+        for (int r = 0; r < DT_ROUNDS; ++r) {
+            if ((r & 31) == 0)
+                pos = philox4x32_10(
+                    make_uint4(cid, t, (TAG_DT_POS << 24) | ((uint32_t)d << 16) | (uint32_t)(r >> 5), stream),
+                    key);
+            if (need_u && (r & 3) == 0)
+                uu = philox4x32_10(
+                    make_uint4(cid, t, (TAG_DT << 24) | ((uint32_t)d << 16) | (uint32_t)(r >> 2), stream),
+                    key);
+            const uint32_t sw = (r < 16) ? sub.x : (r < 32) ? sub.y : (r < 48) ? sub.z : sub.w;
+            const int s = (int)((sw >> (2 * (r & 15))) & 3u);
+            const int pq = (r & 31) >> 3;
+            const uint32_t pw = pq == 0 ? pos.x : pq == 1 ? pos.y : pq == 2 ? pos.z : pos.w;
+            const int pb = (int)((pw >> (4 * (r & 7))) & 15u);
+            const int x = sx0 + (s & 1) * 4 + (pb & 3);
+            const int y = sy0 + (s >> 1) * 4 + (pb >> 2);
+            // ENC_LOCAL word / bit inside the tile (kpz/systemSize.h:94-100)
+            const int wi = (y >> 2) * DT_TW + (x >> 2);
+            const int sh = ((x & 3) << 1) | ((y & 3) << 3);
+            const int wr = (y >> 2) * DT_TW + ((x + 1) >> 2);
+            const int shr = (((x + 1) & 3) << 1) | ((y & 3) << 3);
+            const int wd = ((y + 1) >> 2) * DT_TW + (x >> 2);
+            const int shd = ((x & 3) << 1) | (((y + 1) & 3) << 3);
+            const uint32_t cw = tile[wi];
+            const int config = (int)((cw >> sh) & 3u) | (int)(((tile[wr] >> shr) & 1u) << 2) |
+                               (int)(((tile[wd] >> (shd | 1)) & 1u) << 3);
+            bool flip = false;
+            if (config == 12 || config == 3) {
+                const Thresh& th = config == 12 ? tp : tq;
+                if (th.always) flip = true;
+                else if (th.planes) {
+                    const uint32_t u = (r & 3) == 0 ? uu.x : (r & 3) == 1 ? uu.y : (r & 3) == 2 ? uu.z : uu.w;
+                    flip = u < th.t;
+                }
+            }
+            if (flip) {
+                tile[wi] ^= 3u << sh;
+                tile[wr] ^= 1u << shr;
+                tile[wd] ^= 1u << (shd | 1);
+                if (COUNT) {
+                    if (config == 12) ++ndep;
+                    else ++ndes;
+                }
+            }
+            __syncthreads();
+        }
+        for (int i = tid; i < DT_TH * DT_TW; i += DT_TX * DT_TY) {
+            const uint32_t r = i / DT_TW, c = i - r * DT_TW;
+            sys[(size_t)((wy0 + r) & (Wy - 1)) * Wx + ((wx0 + c) & (Wx - 1))] = tile[i];
+        }
+        __syncthreads();
+    }
+    if (COUNT) {
+        for (int o = 16; o > 0; o >>= 1) {
+            ndep += __shfl_xor_sync(0xffffffffu, ndep, o);
+            ndes += __shfl_xor_sync(0xffffffffu, ndes, o);
+        }
+        if ((tid & 31) == 0 && (ndep | ndes)) {
+            atomicAdd(&counters[0], ndep);
+            atomicAdd(&counters[1], ndes);
+        }
+    }
 }
+
+// Host copy of the Philox4x32-10 bijection for the per-MCS origin and domain-set order.
+static void philox_host(const uint32_t ctr[4], uint64_t seed, uint32_t out[4])
+{
+    uint32_t c0 = ctr[0], c1 = ctr[1], c2 = ctr[2], c3 = ctr[3];
+    uint32_t k0 = (uint32_t)seed, k1 = (uint32_t)(seed >> 32);
+    for (int r = 0; r < 10; ++r) {
+        if (r) {
+            k0 += 0x9E3779B9u;
+            k1 += 0xBB67AE85u;
+        }
+        const uint64_t p0 = (uint64_t)0xD2511F53u * c0, p1 = (uint64_t)0xCD9E8D57u * c2;
+        const uint32_t n0 = (uint32_t)(p1 >> 32) ^ c1 ^ k0, n2 = (uint32_t)(p0 >> 32) ^ c3 ^ k1;
+        c0 = n0;
+        c1 = (uint32_t)p1;
+        c2 = n2;
+        c3 = (uint32_t)p0;
+    }
+    out[0] = c0;
+    out[1] = c1;
+    out[2] = c2;
+    out[3] = c3;
+}
+
+// Origin in [0, 2*block) sites and the Kmc::Shuffle<4> order (inc/shuffle.h:76-90).
+static void dt_plan(uint64_t seed, uint32_t stream, uint32_t t, int* ox, int* oy, int order[4])
+{
+    const uint32_t ctr[4] = {0u, t, TAG_DT_ORIGIN << 24, stream};
+    uint32_t r[4];
+    philox_host(ctr, seed, r);
+    *ox = (int)(r[0] & (uint32_t)(2 * DT_BX - 1));
+    *oy = (int)(r[1] & (uint32_t)(2 * DT_BY - 1));
+    uint32_t rnd = r[2];
+    for (int a = 0; a < 4; ++a) order[a] = a;
+    for (int a = 0; a < 4; ++a) {
+        const int i = (int)(rnd & 3u);
+        const int v = order[i];
+        order[i] = order[a];
+        order[a] = v;
+        rnd >>= 2;
+    }
+}
+
+kpzb_status dt_init(DtState* s, int lx, int ly, int sm_count)
+{
+    if (lx < 9 || ly < 8) return fail(KPZB_EINVAL, "DT needs lx >= 9 and ly >= 8 (one 512x256 double tile)");
+    const int nblocks = (1 << (lx - 9)) * (1 << (ly - 8));
+    // 2048 threads per SM / 512 per CTA: 4 resident CTAs per SM
+    s->grid = nblocks < sm_count * 4 ? nblocks : sm_count * 4;
+    s->ready = true;
+    return KPZB_OK;
+}
+
 void dt_free(DtState* s) { s->ready = false; }
-kpzb_status dt_enqueue(DtState*, uint32_t*, int, int, uint64_t, int, double, double, uint64_t,
-                       uint32_t, cudaStream_t)
+
+static uint64_t thresh_dt(double p)
 {
-    return fail(KPZB_EUNSUPPORTED, "DT dynamics not built yet");
+    if (!(p > 0.0)) return 0;
+    if (p >= 1.0) return 1ull << 32;
+    const double t = std::ceil(p * 4294967296.0);
+    return t >= 4294967296.0 ? (1ull << 32) : (uint64_t)t;
 }
+
+kpzb_status dt_enqueue(DtState* s, uint32_t* d_local, int lx, int ly, uint64_t t0, int n, double p,
+                       double q, uint64_t seed, uint32_t stream, cudaStream_t st,
+                       unsigned long long* d_counters)
+{
+    if (!s->ready) return fail(KPZB_ESTATE, "DT state not initialised");
+    const Key key = make_key(seed);
+    const Thresh tp = make_thresh(thresh_dt(p)), tq = make_thresh(thresh_dt(q));
+    const int lnbx = lx - 9;
+    const int nblocks = (1 << lnbx) * (1 << (ly - 8));
+    const dim3 block(DT_TX, DT_TY);
+    for (int i = 0; i < n; ++i) {
+        const uint32_t t = (uint32_t)(t0 + (uint64_t)i);
+        int ox, oy, order[4];
+        dt_plan(seed, stream, t, &ox, &oy, order);
+        for (int a = 0; a < 4; ++a) {
+            if (d_counters)
+                dt_kernel<true><<<s->grid, block, 0, st>>>(d_local, lx - 2, ly - 2, lnbx, nblocks, ox, oy,
+                                                           order[a], t, key, stream, tp, tq, d_counters);
+            else
+                dt_kernel<false><<<s->grid, block, 0, st>>>(d_local, lx - 2, ly - 2, lnbx, nblocks, ox, oy,
+                                                            order[a], t, key, stream, tp, tq, nullptr);
+        }
+        const cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return cuda_fail(e, "dt_kernel");
+    }
+    return KPZB_OK;
+}
+
 }  // namespace kpzb

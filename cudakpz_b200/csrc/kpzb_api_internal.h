@@ -36,6 +36,7 @@ struct DtState {
 kpzb_status dt_init(DtState* s, int lx, int ly, int sm_count);
 void dt_free(DtState* s);
 kpzb_status dt_enqueue(DtState* s, uint32_t* d_local, int lx, int ly, uint64_t t0, int n,
-                       double p, double q, uint64_t seed, uint32_t stream, cudaStream_t st);
+                       double p, double q, uint64_t seed, uint32_t stream, cudaStream_t st,
+                       unsigned long long* d_counters);
 
 }  // namespace kpzb

@@ -120,6 +120,43 @@ __device__ __forceinline__ uint4 decide4(uint4 cp, uint4 cq, Thresh tp, Thresh t
     return make_uint4(ltp.x | ltq.x, ltp.y | ltq.y, ltp.z | ltq.z, ltp.w | ltq.w);
 }
 
+// Decision modes, chosen once per launch from the two thresholds:
+//   DEC_NONE   no random plane can matter (every threshold is 0 or 2^32),
+//   DEC_ONE    at most the MSB plane matters (thresholds in {0, 2^31, 2^32}, e.g. p = 1/2),
+//   DEC_GENERAL anything else (bit-serial loop of decide4).
+enum DecMode { DEC_NONE = 0, DEC_ONE = 1, DEC_GENERAL = 2 };
+
+__host__ __device__ inline int dec_mode(Thresh tp, Thresh tq)
+{
+    const int m = tp.planes > tq.planes ? tp.planes : tq.planes;
+    return m == 0 ? DEC_NONE : m == 1 ? DEC_ONE : DEC_GENERAL;
+}
+
+// decide4 with the cheap modes spelled out; identical results in every mode.
+__device__ __forceinline__ uint4 decide4_mode(int mode, uint4 cp, uint4 cq, Thresh tp, Thresh tq,
+                                              Key key, uint32_t qgroup, uint32_t step,
+                                              uint32_t stream)
+{
+    if (mode == DEC_NONE) {
+        const uint32_t ap = tp.always ? 0xFFFFFFFFu : 0u, aq = tq.always ? 0xFFFFFFFFu : 0u;
+        return make_uint4((cp.x & ap) | (cq.x & aq), (cp.y & ap) | (cq.y & aq),
+                          (cp.z & ap) | (cq.z & aq), (cp.w & ap) | (cq.w & aq));
+    }
+    if (mode == DEC_ONE) {
+        // a threshold with one plane is 2^31: sites whose MSB of u is 0 flip
+        const uint32_t any = cp.x | cp.y | cp.z | cp.w | cq.x | cq.y | cq.z | cq.w;
+        uint4 r = make_uint4(0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu);
+        if (any) r = philox4x32_10(make_uint4(qgroup, step, TAG_SCA << 8, stream), key);
+        const uint32_t ap = tp.always ? 0xFFFFFFFFu : 0u, aq = tq.always ? 0xFFFFFFFFu : 0u;
+        const uint32_t hp = tp.planes ? 0xFFFFFFFFu : 0u, hq = tq.planes ? 0xFFFFFFFFu : 0u;
+        return make_uint4((cp.x & (ap | (hp & ~r.x))) | (cq.x & (aq | (hq & ~r.x))),
+                          (cp.y & (ap | (hp & ~r.y))) | (cq.y & (aq | (hq & ~r.y))),
+                          (cp.z & (ap | (hp & ~r.z))) | (cq.z & (aq | (hq & ~r.z))),
+                          (cp.w & (ap | (hp & ~r.w))) | (cq.w & (aq | (hq & ~r.w))));
+    }
+    return decide4(cp, cq, tp, tq, key, qgroup, step, stream);
+}
+
 __device__ __forceinline__ uint4 operator^(uint4 a, uint4 b)
 {
     return make_uint4(a.x ^ b.x, a.y ^ b.y, a.z ^ b.z, a.w ^ b.w);

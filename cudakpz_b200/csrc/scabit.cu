@@ -18,6 +18,7 @@
 #include "kpzb_api_internal.h"
 #include "kpzb_common.cuh"
 #include "kpzb_internal.h"
+#include "scabit_band.cuh"
 
 namespace kpzb {
 
@@ -82,7 +83,8 @@ scabit_half_kernel(uint32_t* __restrict__ sys, int lx, int ly, int sigma, uint32
             cq.y = tX.y & tY.y & ~(xX.y | oY.y);
             cq.z = tX.z & tY.z & ~(xX.z | oY.z);
             cq.w = tX.w & tY.w & ~(xX.w | oY.w);
-            const uint4 m = decide4(cp, cq, tp, tq, key, (uint32_t)((roff + wi) >> 2), step, stream);
+            const uint4 m = decide4_mode(dec_mode(tp, tq), cp, cq, tp, tq, key,
+                                         (uint32_t)((roff + wi) >> 2), step, stream);
             if (COUNT) {
                 ndep += __popc(m.x & cp.x) + __popc(m.y & cp.y) + __popc(m.z & cp.z) + __popc(m.w & cp.w);
                 ndes += __popc(m.x & cq.x) + __popc(m.y & cq.y) + __popc(m.z & cq.z) + __popc(m.w & cq.w);
@@ -171,55 +173,7 @@ cudaError_t scabit_half(uint32_t* d_sys, int lx, int ly, int sigma, uint32_t ste
 // thread boundaries only in the first word of each 4-word group, which is updated
 // with shared-memory atomicXor; all other words have a single writer.
 // ---------------------------------------------------------------------------------
-__device__ __forceinline__ uint32_t smem_u32(const void* p)
-{
-    return (uint32_t)__cvta_generic_to_shared(p);
-}
-
-__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count)
-{
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
-}
-
-__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes)
-{
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
-                 "r"(bytes)
-                 : "memory");
-}
-
-__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity)
-{
-    uint32_t ok;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-        "selp.u32 %0, 1, 0, p;\n\t}"
-        : "=r"(ok)
-        : "r"(smem_u32(bar)), "r"(parity)
-        : "memory");
-    return ok != 0;
-}
-
-__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar)
-{
-    asm volatile(
-        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-            smem_u32(dst)),
-        "l"(src), "r"(bytes), "r"(smem_u32(bar))
-        : "memory");
-}
-
-__device__ __forceinline__ void bulk_s2g(void* dst, const void* src, uint32_t bytes)
-{
-    asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(dst),
-                 "r"(smem_u32(src)), "r"(bytes)
-                 : "memory");
-}
-
 constexpr int FUSED_THREADS = 512;
-// bounded spin on the TMA mbarrier: ~2^26 polls (far above any real copy time)
-constexpr uint32_t MBAR_SPIN_LIMIT = 1u << 26;
 
 template <bool COUNT>
 __global__ void __launch_bounds__(FUSED_THREADS)
@@ -230,132 +184,15 @@ scabit_fused_kernel(const uint32_t* __restrict__ src, uint32_t* __restrict__ dst
     extern __shared__ __align__(128) uint32_t smem[];
     __shared__ __align__(8) uint64_t bar;
     __shared__ int abort_flag;
-
-    const uint64_t Wr = 1ull << (lx - 6);
-    const uint64_t Q = 1ull << (lx + ly - 6);
-    const int64_t rows = 1ll << ly;
-    const int H = 2 * k;
-    const int R = B + 2 * H;
-    const int G = (int)(Wr / 4);  // 4-word groups per row
-    const int lgG = lx - 8;
-    const uint64_t qsz = (uint64_t)R * Wr;  // words per quadrant slab in smem
-    const int64_t y0 = (int64_t)blockIdx.x * B;
-    const int Bc = (int)(rows - y0 < B ? rows - y0 : B);  // rows this CTA writes
-    const int64_t ylo = y0 - H;                       // global row of local row 0
-
     if (threadIdx.x == 0) {
-        abort_flag = 0;
         mbar_init(&bar, 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     __syncthreads();
-    if (threadIdx.x == 0) {
-        const uint32_t total = (uint32_t)(4ull * qsz * 4ull);
-        mbar_expect_tx(&bar, total);
-        // rows [ylo, ylo + R) mod rows: at most two contiguous pieces per quadrant
-        int64_t r0 = ((ylo % rows) + rows) % rows;
-        int done = 0;
-        while (done < R) {
-            const int piece = (int)((int64_t)(R - done) < rows - r0 ? (int64_t)(R - done) : rows - r0);
-            for (int qd = 0; qd < 4; ++qd)
-                bulk_g2s(smem + qd * qsz + (uint64_t)done * Wr, src + qd * Q + (uint64_t)r0 * Wr,
-                         (uint32_t)((uint64_t)piece * Wr * 4), &bar);
-            done += piece;
-            r0 = 0;
-        }
-        uint32_t spins = 0;
-        while (!mbar_try_wait(&bar, 0)) {
-            if (++spins > MBAR_SPIN_LIMIT) {
-                abort_flag = 1;
-                break;
-            }
-        }
-    }
-    __syncthreads();
-    if (abort_flag) {
-        // leave dst untouched for this band and report; the in-flight copy targets this
-        // CTA's shared memory only, so keep waiting (bounded) before the CTA retires
-        if (threadIdx.x == 0) {
-            atomicExch(err, 1u);
-            uint32_t spins = 0;
-            while (!mbar_try_wait(&bar, 0) && ++spins < MBAR_SPIN_LIMIT) {
-            }
-        }
-        return;
-    }
-
+    const BandCtl ctl{&bar, &abort_flag, 0u};
+    const BandGeom g{src, dst, lx, ly, (int64_t)blockIdx.x * B, B, k, false, t0, key, stream, tp, tq};
     unsigned long long ndep = 0, ndes = 0;
-    for (int h = 0; h < 2 * k; ++h) {
-        const int sigma = h & 1;
-        const uint32_t step = 2u * (t0 + (uint32_t)(h >> 1)) + (uint32_t)sigma;
-        uint32_t* StX = smem + (sigma ? 2 : 0) * qsz;
-        uint32_t* StY = StX + qsz;
-        uint32_t* SoX = smem + (sigma ? 0 : 2) * qsz;
-        uint32_t* SoY = SoX + qsz;
-        const int ra = h, rb = R - 1 - h;
-        const int items = (rb - ra) << lgG;
-        for (int it = threadIdx.x; it < items; it += FUSED_THREADS) {
-            const int lr = ra + (it >> lgG);
-            const int g = it & (G - 1);
-            const uint64_t w0 = 4ull * g;
-            const int64_t gy = (ylo + lr) & (rows - 1);  // periodic in y (rows is 2^ly)
-            const bool shifted = sigma != (int)(gy & 1);
-            uint4* ptX = reinterpret_cast<uint4*>(StX + (uint64_t)lr * Wr + w0);
-            uint4* ptY = reinterpret_cast<uint4*>(StY + (uint64_t)lr * Wr + w0);
-            uint4* poX = reinterpret_cast<uint4*>(SoX + (uint64_t)lr * Wr + w0);
-            uint4* poY = reinterpret_cast<uint4*>(SoY + (uint64_t)(lr + 1) * Wr + w0);
-            uint4 tX = *ptX, tY = *ptY, oX = *poX, oY = *poY;
-            uint4 xX = oX;
-            uint32_t* nbp = SoX + (uint64_t)lr * Wr + ((w0 + 4) & (Wr - 1));
-            if (shifted) {
-                const uint32_t nb = *nbp;
-                xX.x = (oX.x >> 1) | (oX.y << 31);
-                xX.y = (oX.y >> 1) | (oX.z << 31);
-                xX.z = (oX.z >> 1) | (oX.w << 31);
-                xX.w = (oX.w >> 1) | (nb << 31);
-            }
-            uint4 cp, cq;
-            cp.x = ~(tX.x | tY.x) & xX.x & oY.x;
-            cp.y = ~(tX.y | tY.y) & xX.y & oY.y;
-            cp.z = ~(tX.z | tY.z) & xX.z & oY.z;
-            cp.w = ~(tX.w | tY.w) & xX.w & oY.w;
-            cq.x = tX.x & tY.x & ~(xX.x | oY.x);
-            cq.y = tX.y & tY.y & ~(xX.y | oY.y);
-            cq.z = tX.z & tY.z & ~(xX.z | oY.z);
-            cq.w = tX.w & tY.w & ~(xX.w | oY.w);
-            const uint4 m = decide4(cp, cq, tp, tq, key, (uint32_t)(((uint64_t)gy * Wr + w0) >> 2),
-                                    step, stream);
-            if (COUNT && lr >= H && lr < H + Bc) {
-                ndep += __popc(m.x & cp.x) + __popc(m.y & cp.y) + __popc(m.z & cp.z) + __popc(m.w & cp.w);
-                ndes += __popc(m.x & cq.x) + __popc(m.y & cq.y) + __popc(m.z & cq.z) + __popc(m.w & cq.w);
-            }
-            *ptX = tX ^ m;
-            *ptY = tY ^ m;
-            *poY = oY ^ m;
-            if (shifted) {
-                uint32_t* ox = SoX + (uint64_t)lr * Wr + w0;
-                atomicXor(ox, m.x << 1);
-                ox[1] = oX.y ^ ((m.y << 1) | (m.x >> 31));
-                ox[2] = oX.z ^ ((m.z << 1) | (m.y >> 31));
-                ox[3] = oX.w ^ ((m.w << 1) | (m.z >> 31));
-                if (m.w >> 31) atomicXor(nbp, 1u);
-            } else {
-                *poX = oX ^ m;
-            }
-        }
-        __syncthreads();
-    }
-
-    // write the band's own rows [H, H + Bc) of each quadrant
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        for (int qd = 0; qd < 4; ++qd)
-            bulk_s2g(dst + qd * Q + (uint64_t)y0 * Wr, smem + qd * qsz + (uint64_t)H * Wr,
-                     (uint32_t)((uint64_t)Bc * Wr * 4));
-        asm volatile("cp.async.bulk.commit_group;" ::: "memory");
-        asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
-    }
+    if (!scabit_band<COUNT, FUSED_THREADS>(smem, ctl, g, ndep, ndes, err)) return;
     if (COUNT) {
         for (int o = 16; o > 0; o >>= 1) {
             ndep += __shfl_xor_sync(0xffffffffu, ndep, o);

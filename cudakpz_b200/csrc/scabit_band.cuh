@@ -1,0 +1,230 @@
+// scabit_band.cuh -- one band of SCABit rows advanced k MCS in shared memory (sm_100a).
+//
+// Shared by the single-lattice temporally blocked kernel (scabit.cu) and the batched
+// replica kernel (batch.cu).  A band is R full-width rows of all four ENC_CBBIT quadrants
+// (kpz/systemSize.h:143-165), loaded with TMA bulk copies (cp.async.bulk, local HBM only)
+// and an mbarrier with a bounded wait.
+//   halo mode:     R = B + 4k rows starting 2k rows above the band; half-step h updates
+//                  local rows [h, R-1-h); rows [2k, 2k+B) are exact afterwards.
+//   resident mode: the whole lattice (R = rows); every half-step updates every row with
+//                  periodic y-neighbours inside shared memory; any k.
+// The update rule is that of kpz/kpzSCABit.cu:179-290 with the masks of
+// kpz/kpzSCABitCores.cu:69-74,139-145.  The one-bit x-carry of shifted rows crosses thread
+// boundaries only in the first word of each 4-word group (shared-memory atomicXor).
+#pragma once
+#include "kpzb_common.cuh"
+
+namespace kpzb {
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p)
+{
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
+                 "r"(bytes)
+                 : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity)
+{
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar)
+{
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+            smem_u32(dst)),
+        "l"(src), "r"(bytes), "r"(smem_u32(bar))
+        : "memory");
+}
+
+__device__ __forceinline__ void bulk_s2g(void* dst, const void* src, uint32_t bytes)
+{
+    asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(dst),
+                 "r"(smem_u32(src)), "r"(bytes)
+                 : "memory");
+}
+
+// bounded spin on the TMA mbarrier: ~2^26 polls (far above any real copy time)
+constexpr uint32_t MBAR_SPIN_LIMIT = 1u << 26;
+
+struct BandCtl {
+    uint64_t* bar;     // shared mbarrier, initialised once per CTA with count 1
+    int* abort_flag;   // shared
+    uint32_t phase;    // parity of the mbarrier phase this band waits on
+};
+
+struct BandGeom {
+    const uint32_t* src;
+    uint32_t* dst;
+    int lx, ly;
+    int64_t y0;      // first output row
+    int B;           // output rows (halo mode) or rows (resident)
+    int k;           // MCS per pass
+    bool resident;
+    uint32_t t0;     // MCS index of the first MCS of the pass
+    Key key;
+    uint32_t stream;
+    Thresh tp, tq;
+};
+
+// Runs one band; returns false (after flagging *err) when the TMA load did not complete in
+// time.  Must be called by all threads of the CTA; NT = blockDim.x.
+template <bool COUNT, int NT>
+__device__ bool scabit_band(uint32_t* smem, const BandCtl& ctl, const BandGeom& g,
+                            unsigned long long& ndep, unsigned long long& ndes,
+                            unsigned int* err)
+{
+    const uint64_t Wr = 1ull << (g.lx - 6);
+    const uint64_t Q = 1ull << (g.lx + g.ly - 6);
+    const int64_t rows = 1ll << g.ly;
+    const int H = g.resident ? 0 : 2 * g.k;
+    const int R = g.resident ? (int)rows : g.B + 2 * H;
+    const int G = (int)(Wr / 4);  // 4-word groups per row
+    const int lgG = g.lx - 8;
+    const uint64_t qsz = (uint64_t)R * Wr;  // words per quadrant slab in shared memory
+    const int64_t y0 = g.resident ? 0 : g.y0;
+    const int Bc = g.resident ? (int)rows : (int)(rows - y0 < g.B ? rows - y0 : g.B);
+    const int64_t ylo = y0 - H;  // global row of local row 0
+
+    if (threadIdx.x == 0) {
+        *ctl.abort_flag = 0;
+        mbar_expect_tx(ctl.bar, (uint32_t)(16ull * qsz));
+        int64_t r0 = ylo & (rows - 1);
+        int done = 0;
+        while (done < R) {
+            const int piece = (int)((int64_t)(R - done) < rows - r0 ? (int64_t)(R - done) : rows - r0);
+            for (int qd = 0; qd < 4; ++qd)
+                bulk_g2s(smem + qd * qsz + (uint64_t)done * Wr, g.src + qd * Q + (uint64_t)r0 * Wr,
+                         (uint32_t)((uint64_t)piece * Wr * 4), ctl.bar);
+            done += piece;
+            r0 = 0;
+        }
+        uint32_t spins = 0;
+        while (!mbar_try_wait(ctl.bar, ctl.phase)) {
+            if (++spins > MBAR_SPIN_LIMIT) {
+                *ctl.abort_flag = 1;
+                break;
+            }
+        }
+    }
+    __syncthreads();
+    if (*ctl.abort_flag) {
+        // leave dst untouched and report; the copy in flight targets this CTA's shared
+        // memory only, so wait for it (bounded) before the caller retires the CTA
+        if (threadIdx.x == 0) {
+            atomicExch(err, 1u);
+            uint32_t spins = 0;
+            while (!mbar_try_wait(ctl.bar, ctl.phase) && ++spins < MBAR_SPIN_LIMIT) {
+            }
+        }
+        return false;
+    }
+
+    // Each thread owns one 4-word column group gi and walks rows with stride NT / G; all
+    // shared-memory offsets are 32-bit (a band is at most 227 KB).
+    const int mode = dec_mode(g.tp, g.tq);
+    const uint32_t wr = (uint32_t)Wr;
+    const int gi = (G >= NT) ? (int)threadIdx.x : (int)(threadIdx.x & (G - 1));
+    const int rstride = (G >= NT) ? 1 : NT >> lgG;
+    const int rofs = (G >= NT) ? 0 : (int)(threadIdx.x >> lgG);
+    const uint32_t rmask = (uint32_t)rows - 1u;
+    const int ylo32 = (int)(ylo & (int64_t)rmask);  // ylo mod rows
+    for (int h = 0; h < 2 * g.k; ++h) {
+        const int sigma = h & 1;
+        const uint32_t step = 2u * (g.t0 + (uint32_t)(h >> 1)) + (uint32_t)sigma;
+        uint32_t* StX = smem + (sigma ? 2 : 0) * qsz;
+        uint32_t* StY = StX + qsz;
+        uint32_t* SoX = smem + (sigma ? 0 : 2) * qsz;
+        uint32_t* SoY = SoX + qsz;
+        const int ra = g.resident ? 0 : h;
+        const int rb = g.resident ? R : R - 1 - h;
+        // wide rows (G > NT): a thread takes several column groups of a row in turn
+        for (int gg = gi; gg < G; gg += NT) {
+            const uint32_t w0 = 4u * (uint32_t)gg;
+            const uint32_t wnext = (w0 + 4u) & (wr - 1u);
+            for (int lr = ra + rofs; lr < rb; lr += rstride) {
+                const uint32_t gy = ((uint32_t)ylo32 + (uint32_t)lr) & rmask;  // periodic in y
+                const bool shifted = sigma != (int)(gy & 1u);
+                const uint32_t lr1 = g.resident ? (((uint32_t)lr + 1u) & rmask) : (uint32_t)lr + 1u;
+                const uint32_t ro = (uint32_t)lr * wr;
+                uint4* ptX = reinterpret_cast<uint4*>(StX + ro + w0);
+                uint4* ptY = reinterpret_cast<uint4*>(StY + ro + w0);
+                uint4* poX = reinterpret_cast<uint4*>(SoX + ro + w0);
+                uint4* poY = reinterpret_cast<uint4*>(SoY + lr1 * wr + w0);
+                const uint4 tX = *ptX, tY = *ptY, oX = *poX, oY = *poY;
+                uint32_t* nbp = SoX + ro + wnext;
+                uint4 xX = oX;
+                if (shifted) {
+                    const uint32_t nb = *nbp;
+                    xX.x = __funnelshift_r(oX.x, oX.y, 1);
+                    xX.y = __funnelshift_r(oX.y, oX.z, 1);
+                    xX.z = __funnelshift_r(oX.z, oX.w, 1);
+                    xX.w = __funnelshift_r(oX.w, nb, 1);
+                }
+                uint4 cp, cq;
+                cp.x = ~(tX.x | tY.x) & xX.x & oY.x;
+                cp.y = ~(tX.y | tY.y) & xX.y & oY.y;
+                cp.z = ~(tX.z | tY.z) & xX.z & oY.z;
+                cp.w = ~(tX.w | tY.w) & xX.w & oY.w;
+                cq.x = tX.x & tY.x & ~(xX.x | oY.x);
+                cq.y = tX.y & tY.y & ~(xX.y | oY.y);
+                cq.z = tX.z & tY.z & ~(xX.z | oY.z);
+                cq.w = tX.w & tY.w & ~(xX.w | oY.w);
+                const uint4 m = decide4_mode(mode, cp, cq, g.tp, g.tq, g.key,
+                                             (gy << (g.lx - 8)) + (uint32_t)gg, step, g.stream);
+                if (COUNT && lr >= H && lr < H + Bc) {
+                    ndep += __popc(m.x & cp.x) + __popc(m.y & cp.y) + __popc(m.z & cp.z) + __popc(m.w & cp.w);
+                    ndes += __popc(m.x & cq.x) + __popc(m.y & cq.y) + __popc(m.z & cq.z) + __popc(m.w & cq.w);
+                }
+                *ptX = tX ^ m;
+                *ptY = tY ^ m;
+                *poY = oY ^ m;
+                if (shifted) {
+                    uint32_t* ox = SoX + ro + w0;
+                    atomicXor(ox, m.x << 1);
+                    ox[1] = oX.y ^ __funnelshift_l(m.x, m.y, 1);
+                    ox[2] = oX.z ^ __funnelshift_l(m.y, m.z, 1);
+                    ox[3] = oX.w ^ __funnelshift_l(m.z, m.w, 1);
+                    if (m.w >> 31) atomicXor(nbp, 1u);
+                } else {
+                    *poX = oX ^ m;
+                }
+            }
+        }
+        __syncthreads();
+    }
+
+    // write the band's own rows [H, H + Bc) of each quadrant, then wait until the bulk
+    // store has read shared memory so the caller may reuse it
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int qd = 0; qd < 4; ++qd)
+            bulk_s2g(g.dst + qd * Q + (uint64_t)y0 * Wr, smem + qd * qsz + (uint64_t)H * Wr,
+                     (uint32_t)((uint64_t)Bc * Wr * 4));
+        asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+        asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
+    }
+    __syncthreads();
+    return true;
+}
+
+}  // namespace kpzb

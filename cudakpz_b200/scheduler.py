@@ -266,6 +266,15 @@ class Batch:
     def mcs(self, n: int):
         check(lib.kpzb_batch_mcs(self._h, int(n)), "kpzb_batch_mcs")
 
+    def setFusion(self, mcs_per_pass: int, passes_per_graph: int = 8):
+        check(lib.kpzb_batch_set_fusion(self._h, mcs_per_pass, passes_per_graph),
+              "kpzb_batch_set_fusion")
+
+    def deviceMcs(self) -> int:
+        v = C.c_uint64()
+        check(lib.kpzb_batch_get_mcs(self._h, C.byref(v)), "kpzb_batch_get_mcs")
+        return int(v.value)
+
     def push(self, i: int, words: np.ndarray):
         w = np.ascontiguousarray(words, dtype=np.uint32)
         check(lib.kpzb_batch_push(self._h, i, w.ctypes.data), "kpzb_batch_push")

@@ -59,8 +59,8 @@ const char* kpzb_version(void);
 /* Create a scheduler for a 2^lx x 2^ly lattice on `device` (-1: current device).
  * Replaces SchedulerSCA/SchedulerSCABit/SchedulerDT constructors + SchedulerBase::initCUDA
  * (kpz/schedulerSCABit.cu:84-88, kpz/schedulerBase.cu:65-74, kpz/schedulerDT.cu:93-118).
- * Limits: 8 <= lx <= 30 (SCA/SCABit), 8 <= lx (DT: lx, ly >= 10), 2 <= ly <= 30,
- * lx + ly <= 38.  The lattice starts flat. */
+ * Limits: 8 <= lx <= 30, 2 <= ly <= 30, 14 <= lx + ly <= 38; DT also needs lx >= 9 and
+ * ly >= 8 (one double tile of 512x256 sites).  The lattice starts flat. */
 kpzb_status kpzb_create(kpzb_handle** h, int lx, int ly, int dynamics, int device);
 kpzb_status kpzb_destroy(kpzb_handle* h);
 
@@ -155,7 +155,12 @@ kpzb_status kpzb_batch_create(kpzb_batch** b, int n, const int* lx, const double
                               int device);
 kpzb_status kpzb_batch_destroy(kpzb_batch* b);
 kpzb_status kpzb_batch_init_homogeneous(kpzb_batch* b);
+/* n MCS for every replica (synchronous).  Square lattices only, 8 <= lx <= 16. */
 kpzb_status kpzb_batch_mcs(kpzb_batch* b, int n);
+/* MCS per pass (1..32; default 8) and passes per captured CUDA graph (1..256; default 8).
+ * Results are identical for every choice. */
+kpzb_status kpzb_batch_set_fusion(kpzb_batch* b, int mcs_per_pass, int passes_per_graph);
+kpzb_status kpzb_batch_get_mcs(const kpzb_batch* b, uint64_t* mcs);
 kpzb_status kpzb_batch_push(kpzb_batch* b, int i, const uint32_t* words);
 kpzb_status kpzb_batch_pop(kpzb_batch* b, int i, uint32_t* words);
 /* W^2 of every replica, out[n]. */

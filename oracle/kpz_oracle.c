@@ -341,6 +341,97 @@ void ko_check_invariants(const uint32_t* w, int lx, int ly, int encoding, int64_
 }
 
 /* ------------------------------------------------------------------------ */
+/* Double tiling: see kpz_oracle.h.  Block 256x128 sites, 32x16 thread cells */
+/* of 8x8 sites, 64 rounds per launch.                                      */
+/* ------------------------------------------------------------------------ */
+static void philox_u32(uint64_t seed, uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3, uint32_t out[4])
+{
+    uint32_t ctr[4] = {c0, c1, c2, c3};
+    uint32_t key[2] = {(uint32_t)seed, (uint32_t)(seed >> 32)};
+    ko_philox4x32_10(ctr, key, out);
+}
+
+void ko_dt_plan(uint64_t seed, uint32_t stream, uint64_t t, int* ox, int* oy, int order[4])
+{
+    uint32_t r[4];
+    philox_u32(seed, 0u, (uint32_t)t, KO_TAG_DT_ORIGIN << 24, stream, r);
+    *ox = (int)(r[0] & 511u); /* [0, 2 * 256) sites */
+    *oy = (int)(r[1] & 255u); /* [0, 2 * 128) sites */
+    /* Kmc::Shuffle<4>::shuffle (inc/shuffle.h:76-90): RC4 key-schedule style swaps */
+    uint32_t rnd = r[2];
+    for (int a = 0; a < 4; ++a) order[a] = a;
+    for (int a = 0; a < 4; ++a) {
+        int i = (int)(rnd & 3u);
+        int v = order[i];
+        order[i] = order[a];
+        order[a] = v;
+        rnd >>= 2;
+    }
+}
+
+void ko_dt_mcs(uint32_t* w, int lx, int ly, uint64_t seed, uint32_t stream, uint64_t t0, int n,
+               double p, double q, int64_t* dep, int64_t* des)
+{
+    const int L = 1 << lx, M = 1 << ly;
+    const int BX = 256, BY = 128;
+    const int nbx = L / (2 * BX), nby = M / (2 * BY);
+    const uint64_t Tp = ko_threshold(p), Tq = ko_threshold(q);
+    int64_t nd = 0, nr = 0;
+    for (int i = 0; i < n; ++i) {
+        const uint64_t t = t0 + (uint64_t)i;
+        int ox, oy, order[4];
+        ko_dt_plan(seed, stream, t, &ox, &oy, order);
+        for (int a = 0; a < 4; ++a) {
+            const int d = order[a];
+            for (int b = 0; b < nbx * nby; ++b) {
+                const int bx = b % nbx, by = b / nbx;
+                const int X0 = ox + (2 * bx + (d & 1)) * BX;
+                const int Y0 = oy + (2 * by + (d >> 1)) * BY;
+                uint32_t sub[4];
+                philox_u32(seed, (uint32_t)b, (uint32_t)t, (KO_TAG_DT_SUB << 24) | ((uint32_t)d << 16),
+                           stream, sub);
+                for (int r = 0; r < 64; ++r) {
+                    const int s = (int)((sub[r >> 4] >> (2 * (r & 15))) & 3u);
+                    for (int cell = 0; cell < 512; ++cell) {
+                        const int tx = cell & 31, ty = cell >> 5;
+                        const uint32_t cid = (uint32_t)b * 512u + (uint32_t)cell;
+                        uint32_t pw[4];
+                        philox_u32(seed, cid, (uint32_t)t,
+                                   (KO_TAG_DT_POS << 24) | ((uint32_t)d << 16) | (uint32_t)(r >> 5),
+                                   stream, pw);
+                        const int pos = (int)((pw[(r & 31) >> 3] >> (4 * (r & 7))) & 15u);
+                        const int x = (X0 + tx * 8 + (s & 1) * 4 + (pos & 3)) & (L - 1);
+                        const int y = (Y0 + ty * 8 + (s >> 1) * 4 + (pos >> 2)) & (M - 1);
+                        const int c = ko_local_get(w, lx, x, y);
+                        const int rr = ko_local_get(w, lx, (x + 1) & (L - 1), y) & 1;
+                        const int ll = (ko_local_get(w, lx, x, (y + 1) & (M - 1)) >> 1) & 1;
+                        const int config = c | (rr << 2) | (ll << 3);
+                        uint64_t T;
+                        if (config == 12) T = Tp;
+                        else if (config == 3) T = Tq;
+                        else continue;
+                        if (T == 0) continue;
+                        if (T < ((uint64_t)1 << 32)) {
+                            uint32_t uw[4];
+                            philox_u32(seed, cid, (uint32_t)t,
+                                       (KO_TAG_DT << 24) | ((uint32_t)d << 16) | (uint32_t)(r >> 2),
+                                       stream, uw);
+                            if ((uint64_t)uw[r & 3] >= T) continue;
+                        }
+                        ko_local_flip(w, lx, x, y, 3);
+                        ko_local_flip(w, lx, (x + 1) & (L - 1), y, 1);
+                        ko_local_flip(w, lx, x, (y + 1) & (M - 1), 2);
+                        if (config == 12) ++nd; else ++nr;
+                    }
+                }
+            }
+        }
+    }
+    if (dep) *dep += nd;
+    if (des) *des += nr;
+}
+
+/* ------------------------------------------------------------------------ */
 /* dSFMT-19937 (vendored BSD third-party code in the reference,             */
 /* inc/dSFMT/dSFMT.{h,cpp}, parameters inc/dSFMT/dSFMT-params19937.h;       */
 /* Saito & Matsumoto, "A PRNG specialized in double precision floating      */
@@ -428,6 +519,13 @@ void ko_dsfmt_reseed(ko_dsfmt* s, uint32_t seed)
 /* SchedulerCPU::mcs / mcsPQ (kpz/schedulerCPU.inl:21-88, kpz/schedulerCPU.cpp:35-46) */
 void ko_rs_mcs(uint32_t* w, int lx, int ly, ko_dsfmt* s, int n, int pq, double p, double q)
 {
+    ko_rs_mcs_count(w, lx, ly, s, n, pq, p, q, 0, 0);
+}
+
+void ko_rs_mcs_count(uint32_t* w, int lx, int ly, ko_dsfmt* s, int n, int pq, double p, double q,
+                     int64_t* dep, int64_t* des)
+{
+    int64_t nd = 0, nr = 0;
     int L = 1 << lx, M = 1 << ly;
     uint64_t N = (uint64_t)1 << (lx + ly);
     int oneone = pq && p == 1.0 && q == 1.0;
@@ -453,6 +551,9 @@ void ko_rs_mcs(uint32_t* w, int lx, int ly, ko_dsfmt* s, int n, int pq, double p
             ko_local_flip(w, lx, x, y, 3);
             ko_local_flip(w, lx, (x + 1) & (L - 1), y, 1);
             ko_local_flip(w, lx, x, (y + 1) & (M - 1), 2);
+            if (config == 12) ++nd; else ++nr;
         }
     }
+    if (dep) *dep += nd;
+    if (des) *des += nr;
 }

@@ -84,6 +84,27 @@ void ko_correlate(const uint32_t* sys, const uint32_t* snap, int lx, int ly, int
  * y-sum, rep[2] = plaquettes with nonzero loop. All zero for a valid lattice. */
 void ko_check_invariants(const uint32_t* w, int lx, int ly, int encoding, int64_t rep[3]);
 
+/* ---- double-tiling (DT) random-sequential dynamics, CPU emulation of the GPU scheme ----
+ * Restates SchedulerDT::doMcs (kpz/schedulerDT.cu:65-78: random origin in [0, 2*block) and a
+ * shuffled order of the 4 domain sets per MCS, kpz/kpzCopy.cu:144-187: block + halo tiles)
+ * with the inner single-hit double tiling of KpzCores::BaseDT
+ * (kpz/kpzSimulationPrimitivesTemplates.cu:110-141: per round one block-wide sub-cell, each
+ * thread one attempt inside that quadrant of its thread cell), driven by the counter stream:
+ *   origin/order : Philox(ctr=(0, t, TAG_DT_ORIGIN<<24, stream)) words 0,1,2
+ *   sub-cells    : Philox(ctr=(block, t, TAG_DT_SUB<<24 | d<<16, stream)), 2 bits per round
+ *   positions    : Philox(ctr=(cell, t, TAG_DT_POS<<24 | d<<16 | r>>5, stream)), 4 bits/round
+ *   acceptance u : Philox(ctr=(cell, t, TAG_DT<<24 | d<<16 | r>>2, stream)), word r&3
+ * Geometry: 32x16 threads, 8x8-site thread cells, blocks of 256x128 sites, 64 rounds per
+ * launch (one attempt per site per MCS).  ENC_LOCAL lattice, lx >= 9, ly >= 8. */
+#define KO_TAG_DT 2u
+#define KO_TAG_DT_ORIGIN 3u
+#define KO_TAG_DT_SUB 4u
+#define KO_TAG_DT_POS 5u
+void ko_dt_mcs(uint32_t* w, int lx, int ly, uint64_t seed, uint32_t stream, uint64_t t0, int n,
+               double p, double q, int64_t* dep, int64_t* des);
+/* the per-MCS origin (sites) and domain-set order used by ko_dt_mcs */
+void ko_dt_plan(uint64_t seed, uint32_t stream, uint64_t t, int* ox, int* oy, int order[4]);
+
 /* ---- random-sequential CPU scheduler with dSFMT-19937 ---- */
 typedef struct ko_dsfmt ko_dsfmt;
 size_t ko_dsfmt_size(void);
@@ -94,6 +115,9 @@ void ko_dsfmt_reseed(ko_dsfmt* s, uint32_t seed);
 /* SchedulerCPU::mcs (p=1,q=0, 2 draws/attempt) if pq==0, mcsPQ (third draw only when
  * the site is active) if pq==1. ENC_LOCAL lattice. */
 void ko_rs_mcs(uint32_t* w, int lx, int ly, ko_dsfmt* s, int n, int pq, double p, double q);
+/* the same, also counting depositions and desorptions */
+void ko_rs_mcs_count(uint32_t* w, int lx, int ly, ko_dsfmt* s, int n, int pq, double p, double q,
+                     int64_t* dep, int64_t* des);
 
 #ifdef __cplusplus
 }

@@ -48,12 +48,18 @@ def _load():
         "ko_roughness": (None, [u32p, C.c_int, C.c_int, C.c_int, dblp]),
         "ko_correlate": (None, [u32p, u32p, C.c_int, C.c_int, C.c_int, C.c_double, dblp]),
         "ko_check_invariants": (None, [u32p, C.c_int, C.c_int, C.c_int, i64p]),
+        "ko_dt_mcs": (None, [u32p, C.c_int, C.c_int, C.c_uint64, C.c_uint32, C.c_uint64, C.c_int,
+                             C.c_double, C.c_double, i64p, i64p]),
+        "ko_dt_plan": (None, [C.c_uint64, C.c_uint32, C.c_uint64, C.POINTER(C.c_int),
+                              C.POINTER(C.c_int), C.POINTER(C.c_int)]),
         "ko_dsfmt_size": (C.c_size_t, []),
         "ko_dsfmt_init": (None, [C.c_void_p, C.c_uint32]),
         "ko_dsfmt_reseed": (None, [C.c_void_p, C.c_uint32]),
         "ko_dsfmt_close_open": (C.c_double, [C.c_void_p]),
         "ko_rs_mcs": (None, [u32p, C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_int, C.c_double,
                              C.c_double]),
+        "ko_rs_mcs_count": (None, [u32p, C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_int,
+                                   C.c_double, C.c_double, i64p, i64p]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
@@ -111,6 +117,21 @@ def sca_mcs(w: np.ndarray, lx: int, ly: int, encoding: int, seed: int, stream: i
     dep, des = C.c_int64(0), C.c_int64(0)
     lib.ko_sca_mcs(_u32(w), lx, ly, encoding, seed, stream, t0, n, p, q, C.byref(dep), C.byref(des))
     return dep.value, des.value
+
+
+def dt_mcs(w: np.ndarray, lx: int, ly: int, seed: int, stream: int, t0: int, n: int,
+           p: float, q: float):
+    """Double-tiling RS emulation (ENC_LOCAL, in place); returns (#deposits, #desorptions)."""
+    dep, des = C.c_int64(0), C.c_int64(0)
+    lib.ko_dt_mcs(_u32(w), lx, ly, seed, stream, t0, n, p, q, C.byref(dep), C.byref(des))
+    return dep.value, des.value
+
+
+def dt_plan(seed: int, stream: int, t: int):
+    ox, oy = C.c_int(), C.c_int()
+    order = (C.c_int * 4)()
+    lib.ko_dt_plan(seed, stream, t, C.byref(ox), C.byref(oy), order)
+    return ox.value, oy.value, list(order)
 
 
 def heights(w: np.ndarray, lx: int, ly: int, encoding: int) -> np.ndarray:
@@ -173,8 +194,11 @@ class DSFMT:
 
 
 def rs_mcs(w: np.ndarray, lx: int, ly: int, rng: DSFMT, n: int, pq: bool = False,
-           p: float = 1.0, q: float = 0.0) -> None:
-    lib.ko_rs_mcs(_u32(w), lx, ly, rng.ptr, n, int(pq), p, q)
+           p: float = 1.0, q: float = 0.0):
+    """SchedulerCPU::mcs (pq False) / mcsPQ (pq True) in place; returns (#dep, #des)."""
+    dep, des = C.c_int64(0), C.c_int64(0)
+    lib.ko_rs_mcs_count(_u32(w), lx, ly, rng.ptr, n, int(pq), p, q, C.byref(dep), C.byref(des))
+    return dep.value, des.value
 
 
 def random_lattice(lx: int, ly: int, encoding: int, seed: int, mcs: int = 4,

@@ -1,0 +1,109 @@
+"""GPU double-tiling (DT) random-sequential dynamics, through the C ABI.
+
+Two kinds of parity:
+  * bit-exact against the CPU emulation of the same DT scheme (oracle ko_dt_mcs): same
+    counter stream, same origins / domain-set order / sub-cells / positions, so any race or
+    halo error in the kernel shows up as a differing word;
+  * statistical against the exact random-sequential scheduler SchedulerCPU
+    (kpz/schedulerCPU.inl:50-88), restated in the oracle and pinned bit-exactly to the
+    reference by tests/test_oracle_golden.py: W^2(t) and the interface velocity over
+    independent seeds agree within 4 combined standard errors.
+Reference DT behaviour: kpz/schedulerDT.cu:38-78, kpz/kpz.cu:126-155,
+kpz/kpzSimulationPrimitivesTemplates.cu:110-141.
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def run_dt(kpzb, lx, ly, p, q, seed, n, init=None, stream=0, counters=False):
+    s = kpzb.Scheduler(lx, ly, scheduler="dt")
+    s.setPQ(p, q)
+    s.supplySeed(seed, stream)
+    if init is not None:
+        s.pushSystem(init)
+    if counters:
+        s.enableCounters(True)
+    s.mcsPQSyncRng(n)
+    out = s.popSystem()
+    cnt = s.counters() if counters else None
+    s.close()
+    return out, cnt
+
+
+@pytest.mark.parametrize("p,q", [(1.0, 0.0), (0.95, 0.05), (0.5, 0.5), (1.0, 1.0), (0.3, 0.6)])
+@pytest.mark.parametrize("lx,ly", [(9, 8), (10, 9), (11, 10)])
+def test_dt_bit_exact_vs_emulation(kpzb, oracle, lx, ly, p, q):
+    n = 3
+    ref = oracle.homogeneous(lx, ly, oracle.ENC_LOCAL)
+    rdep, rdes = oracle.dt_mcs(ref, lx, ly, 42, 0, 0, n, p, q)
+    got, cnt = run_dt(kpzb, lx, ly, p, q, 42, n, counters=True)
+    d = np.nonzero(got != ref)[0]
+    assert d.size == 0, (d.size, int(d[0]))
+    assert cnt == (rdep, rdes)
+
+
+def test_dt_random_start_and_stream(kpzb, oracle):
+    lx, ly = 10, 10
+    init = oracle.cbbit_to_local(oracle.random_lattice(lx, ly, oracle.ENC_CBBIT, seed=4, mcs=6), lx, ly)
+    ref = init.copy()
+    oracle.dt_mcs(ref, lx, ly, 7, 5, 0, 4, 0.9, 0.2)
+    got, _ = run_dt(kpzb, lx, ly, 0.9, 0.2, 7, 4, init=init, stream=5)
+    assert np.array_equal(got, ref)
+
+
+def test_dt_invariants_large(kpzb):
+    s = kpzb.Scheduler(12, 12, scheduler="dt")
+    s.setPQ(0.95, 0.05)
+    s.supplySeed(3)
+    s.mcsPQSyncRng(20)
+    ok, rep = s.consitencyCheck()
+    assert ok, rep
+    s.close()
+
+
+def _mean_err(a):
+    a = np.asarray(a, dtype=float)
+    return a.mean(axis=0), a.std(axis=0, ddof=1) / np.sqrt(len(a))
+
+
+def test_dt_statistics_match_random_sequential(kpzb, oracle):
+    """W^2(t) and velocity of GPU DT vs the exact RS scheduler, p=0.95 q=0.05, 512^2."""
+    lx = ly = 9
+    N = 1 << (lx + ly)
+    p, q = 0.95, 0.05
+    ts = [1, 2, 4, 8, 16, 32]
+    seeds = range(1, 13)
+    w_dt, w_rs, v_dt, v_rs = [], [], [], []
+    for sd in seeds:
+        s = kpzb.Scheduler(lx, ly, scheduler="dt")
+        s.setPQ(p, q)
+        s.supplySeed(sd)
+        s.enableCounters(True)
+        row, t = [], 0
+        for T in ts:
+            s.mcsPQSyncRng(T - t)
+            t = T
+            row.append(s.roughness().w2)
+        dep, des = s.counters()
+        v_dt.append(2.0 * (dep - des) / N / ts[-1])
+        w_dt.append(row)
+        s.close()
+        w = oracle.homogeneous(lx, ly, oracle.ENC_LOCAL)
+        rng = oracle.DSFMT(sd)
+        row, t, dep, des = [], 0, 0, 0
+        for T in ts:
+            a, b = oracle.rs_mcs(w, lx, ly, rng, T - t, pq=True, p=p, q=q)
+            dep, des = dep + a, des + b
+            t = T
+            row.append(oracle.roughness(w, lx, ly, oracle.ENC_LOCAL)[0])
+        v_rs.append(2.0 * (dep - des) / N / ts[-1])
+        w_rs.append(row)
+    m1, e1 = _mean_err(w_dt)
+    m2, e2 = _mean_err(w_rs)
+    z = np.abs(m1 - m2) / np.sqrt(e1 ** 2 + e2 ** 2)
+    assert np.all(z < 4.0), (m1, m2, z)
+    mv1, ev1 = _mean_err(v_dt)
+    mv2, ev2 = _mean_err(v_rs)
+    assert abs(mv1 - mv2) < 4.0 * np.sqrt(ev1 ** 2 + ev2 ** 2) + 1e-4, (mv1, mv2)

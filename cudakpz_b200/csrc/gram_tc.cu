@@ -1,0 +1,282 @@
+// gram_tc.cu -- exact int8 limb Gram A A^T (A: 192 x N, K-major) on tcgen05 tensor cores.
+//
+// One persistent CTA per SM takes a contiguous K range.  Warp 0 streams 192-row x 128-byte
+// K tiles of A into a ring of shared-memory stages with 2D TMA (SWIZZLE_128B, local HBM
+// only, no multicast); warp 1 allocates 256 TMEM columns and issues, per 32-byte K step,
+//   D1[0:128, 0:192]   += A[0:128]   . A[0:192]^T   (M=128, N=192)
+//   D2[0:128, 0:64]    += A[64:192]  . A[128:192]^T (M=128, N=64)
+// (kind::i8, signed, int32 accumulators in TMEM); together they cover every (row <= col)
+// entry of the symmetric 192 x 192 limb Gram.  Every 2^18 K elements (|l l'| <= 2^12, so
+// the int32 sums stay below 2^30) warps 2-5 read the accumulators with tcgen05.ld and add
+// them to the CTA's int64 partial in global memory; a final kernel sums the partials.
+// Every mbarrier wait is bounded: on expiry the kernel raises a flag, stops issuing work,
+// drains what it issued, frees its TMEM and returns.
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
+#include <algorithm>
+#include <cstring>
+
+#include "kpzb_api_internal.h"
+#include "kpzb_gram.h"
+#include "scabit_band.cuh"
+
+namespace kpzb {
+
+constexpr int TC_ROWS = 192;
+constexpr int TC_KT = 128;                        // K bytes per tile (one 128B swizzle row)
+constexpr int TC_STAGE = TC_ROWS * TC_KT;         // 24 KB
+constexpr int TC_STAGES = 6;
+constexpr int TC_WINDOW = (1 << 18) / TC_KT;      // K tiles per int32 accumulation window
+constexpr int TC_THREADS = 192;
+constexpr int TC_COLS = 256;                      // TMEM columns: D1 0..191, D2 192..255
+constexpr uint32_t TC_SPIN = 1u << 26;
+
+// UMMA instruction descriptor, kind::i8: S32 accumulate (bits 4-5 = 2), signed A and B
+// (bits 7-9, 10-12 = 1), both K-major, N>>3 at bit 17, M>>4 at bit 24.
+__host__ __device__ constexpr uint32_t idesc_i8(int M, int N)
+{
+    return (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
+
+// Shared-memory descriptor of a K-major SWIZZLE_128B operand: rows of 128 bytes, 8-row
+// groups 1024 bytes apart (SBO), LBO 16 bytes, descriptor version 1, layout type 2.
+__device__ __forceinline__ uint64_t sdesc_sw128(uint32_t saddr)
+{
+    return (uint64_t)((saddr >> 4) & 0x3FFFu) | (1ull << 16) | ((uint64_t)(1024 >> 4) << 32) | (1ull << 46) |
+           (2ull << 61);
+}
+
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity)
+{
+    uint32_t spins = 0;
+    while (!mbar_try_wait(bar, parity))
+        if (++spins > TC_SPIN) return false;
+    return true;
+}
+
+__device__ __forceinline__ void tma_load_2d(void* dst, const void* tmap, int x, int y, uint64_t* bar)
+{
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(
+            smem_u32(dst)),
+        "l"(tmap), "r"(x), "r"(y), "r"(smem_u32(bar))
+        : "memory");
+}
+
+__device__ __forceinline__ void umma_i8(uint32_t dtmem, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                        uint32_t accumulate)
+{
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}" ::"r"(dtmem),
+        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
+}
+
+__device__ __forceinline__ void umma_commit(uint64_t* bar)
+{
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                     smem_u32(bar))
+                 : "memory");
+}
+
+__global__ void __launch_bounds__(TC_THREADS, 1)
+gram_tc_kernel(const __grid_constant__ CUtensorMap tmap, uint64_t nkt, long long* __restrict__ part,
+               unsigned int* __restrict__ err)
+{
+    extern __shared__ __align__(1024) uint8_t smem_raw[];
+    __shared__ __align__(8) uint64_t full[TC_STAGES], empty[TC_STAGES], accf, acce;
+    __shared__ uint32_t tmem_base;
+    __shared__ volatile int abort_flag;
+    uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+
+    // contiguous K-tile range of this CTA
+    const uint64_t per = nkt / gridDim.x, rem = nkt % gridDim.x;
+    const uint64_t kt0 = blockIdx.x * per + ((uint64_t)blockIdx.x < rem ? (uint64_t)blockIdx.x : rem);
+    const uint64_t nloc = per + (blockIdx.x < rem ? 1 : 0);
+    const uint64_t nwin = (nloc + TC_WINDOW - 1) / TC_WINDOW;
+
+    if (threadIdx.x == 0) {
+        abort_flag = 0;
+        for (int s = 0; s < TC_STAGES; ++s) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], 1);
+        }
+        mbar_init(&accf, 1);
+        mbar_init(&acce, 128);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 1) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_base)),
+                     "r"(TC_COLS));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tbase = tmem_base;
+
+    if (warp == 0) {
+        if (lane == 0) {
+            uint64_t issued = 0;
+            for (uint64_t i = 0; i < nloc; ++i) {
+                const int s = (int)(i % TC_STAGES);
+                const uint32_t ph = (uint32_t)((i / TC_STAGES) & 1);
+                if (abort_flag || !mbar_wait_bounded(&empty[s], ph ^ 1u)) {
+                    abort_flag = 1;
+                    break;
+                }
+                mbar_expect_tx(&full[s], TC_STAGE);
+                tma_load_2d(smem + s * TC_STAGE, &tmap, (int)((kt0 + i) * TC_KT), 0, &full[s]);
+                issued = i + 1;
+            }
+            // copies still in flight land before the CTA retires (bounded)
+            for (uint64_t j = issued > TC_STAGES ? issued - TC_STAGES : 0; j < issued; ++j)
+                mbar_wait_bounded(&full[j % TC_STAGES], (uint32_t)((j / TC_STAGES) & 1));
+        }
+    } else if (warp == 1) {
+        if (lane == 0) {
+            const uint32_t id1 = idesc_i8(128, 192), id2 = idesc_i8(128, 64);
+            for (uint64_t i = 0; i < nloc && !abort_flag; ++i) {
+                const int s = (int)(i % TC_STAGES);
+                const uint32_t ph = (uint32_t)((i / TC_STAGES) & 1);
+                const uint64_t w = i / TC_WINDOW;
+                const bool first = (i % TC_WINDOW) == 0;
+                if (first && w > 0 && !mbar_wait_bounded(&acce, (uint32_t)((w - 1) & 1))) {
+                    abort_flag = 1;
+                    break;
+                }
+                if (!mbar_wait_bounded(&full[s], ph)) {
+                    abort_flag = 1;
+                    break;
+                }
+                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                const uint32_t sa = smem_u32(smem + s * TC_STAGE);
+                for (int kk = 0; kk < TC_KT / 32; ++kk) {
+                    const uint32_t acc = (first && kk == 0) ? 0u : 1u;
+                    umma_i8(tbase, sdesc_sw128(sa + 32 * kk), sdesc_sw128(sa + 32 * kk), id1, acc);
+                    umma_i8(tbase + 192, sdesc_sw128(sa + 64 * TC_KT + 32 * kk),
+                            sdesc_sw128(sa + 128 * TC_KT + 32 * kk), id2, acc);
+                }
+                umma_commit(&empty[s]);
+                if ((i % TC_WINDOW) == TC_WINDOW - 1 || i + 1 == nloc) umma_commit(&accf);
+            }
+        }
+    } else {
+        // epilogue: warps 2..5 own TMEM lane quarters (warp % 4)
+        const int q = warp & 3;
+        const int r = 32 * q + lane;  // accumulator row (TMEM lane)
+        long long* prow1 = part + (uint64_t)blockIdx.x * TC_ROWS * TC_ROWS + (uint64_t)r * TC_ROWS;
+        long long* prow2 = part + (uint64_t)blockIdx.x * TC_ROWS * TC_ROWS + (uint64_t)(64 + r) * TC_ROWS + 128;
+        for (uint64_t w = 0; w < nwin; ++w) {
+            if (!mbar_wait_bounded(&accf, (uint32_t)(w & 1))) {
+                abort_flag = 1;
+                break;
+            }
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            for (int c0 = 0; c0 < TC_COLS; c0 += 32) {
+                uint32_t v[32];
+                const uint32_t taddr = tbase + ((uint32_t)(32 * q) << 16) + (uint32_t)c0;
+                asm volatile(
+                    "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+                    "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+                    : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
+                      "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]),
+                      "=r"(v[14]), "=r"(v[15]), "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]),
+                      "=r"(v[21]), "=r"(v[22]), "=r"(v[23]), "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]),
+                      "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
+                    : "r"(taddr));
+                asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+                if (c0 < 192) {
+                    for (int j = 0; j < 32; ++j) prow1[c0 + j] += (long long)(int32_t)v[j];
+                } else if (r >= 64) {
+                    // D2 rows 64..127 are limb rows 128..191; rows below 128 repeat D1
+                    for (int j = 0; j < 32; ++j) prow2[c0 - 192 + j] += (long long)(int32_t)v[j];
+                }
+            }
+            asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+            asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(&acce)) : "memory");
+        }
+    }
+    // drain: all issued MMAs complete before the accumulator columns are released
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    if (abort_flag && threadIdx.x == 0) atomicExch(err, 1u);
+    if (warp == 1) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tbase), "r"(TC_COLS));
+}
+
+__global__ void gram_reduce_kernel(const long long* __restrict__ part, int grid, long long* __restrict__ out)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < TC_ROWS * TC_ROWS; i += gridDim.x * blockDim.x) {
+        long long s = 0;
+        for (int c = 0; c < grid; ++c) s += part[(uint64_t)c * TC_ROWS * TC_ROWS + i];
+        out[i] = s;
+    }
+}
+
+kpzb_status gram_tc_setup(GramTC* tc, const int8_t* d_limbs, uint64_t N, int sm_count)
+{
+    if (N % TC_KT || N > (1ull << 30)) return fail(KPZB_EINVAL, "gram: N must be a multiple of 128, <= 2^30");
+    PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    cudaError_t e = cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", reinterpret_cast<void**>(&encode),
+                                            cudaEnableDefault, &q);
+    if (e != cudaSuccess || !encode || q != cudaDriverEntryPointSuccess)
+        return fail(KPZB_ECUDA, "cuTensorMapEncodeTiled unavailable");
+    const cuuint64_t dims[2] = {(cuuint64_t)N, (cuuint64_t)TC_ROWS};
+    const cuuint64_t strides[1] = {(cuuint64_t)N};  // bytes between limb rows
+    const cuuint32_t box[2] = {(cuuint32_t)TC_KT, (cuuint32_t)TC_ROWS};
+    const cuuint32_t estr[2] = {1, 1};
+    CUtensorMap* map = reinterpret_cast<CUtensorMap*>(tc->tmap);
+    const CUresult r = encode(map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, const_cast<int8_t*>(d_limbs), dims, strides,
+                              box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                              CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return fail(KPZB_ECUDA, "cuTensorMapEncodeTiled failed");
+    tc->grid = sm_count;
+    if ((e = cudaMalloc(&tc->d_part, (size_t)tc->grid * TC_ROWS * TC_ROWS * 8)) != cudaSuccess)
+        return cuda_fail(e, "cudaMalloc(gram partials)");
+    if ((e = cudaMalloc(&tc->d_out, TC_ROWS * TC_ROWS * 8 + 64)) != cudaSuccess) return cuda_fail(e, "cudaMalloc(gram)");
+    tc->d_err = reinterpret_cast<unsigned int*>(tc->d_out + TC_ROWS * TC_ROWS);
+    if ((e = cudaFuncSetAttribute(gram_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  TC_STAGES * TC_STAGE + 1024)) != cudaSuccess)
+        return cuda_fail(e, "gram smem attribute");
+    tc->ready = true;
+    return KPZB_OK;
+}
+
+void gram_tc_free(GramTC* tc)
+{
+    cudaFree(tc->d_part);
+    cudaFree(tc->d_out);
+    tc->d_part = nullptr;
+    tc->d_out = nullptr;
+    tc->ready = false;
+}
+
+kpzb_status gram_tc_run(GramTC* tc, uint64_t N, int64_t* out, cudaStream_t st)
+{
+    if (!tc->ready) return fail(KPZB_ESTATE, "gram tensor path not set up");
+    cudaError_t e;
+    if ((e = cudaMemsetAsync(tc->d_part, 0, (size_t)tc->grid * TC_ROWS * TC_ROWS * 8, st)) != cudaSuccess)
+        return cuda_fail(e, "memset partials");
+    if ((e = cudaMemsetAsync(tc->d_err, 0, 4, st)) != cudaSuccess) return cuda_fail(e, "memset flag");
+    const CUtensorMap* map = reinterpret_cast<const CUtensorMap*>(tc->tmap);
+    gram_tc_kernel<<<tc->grid, TC_THREADS, TC_STAGES * TC_STAGE + 1024, st>>>(
+        *map, N / TC_KT, reinterpret_cast<long long*>(tc->d_part), tc->d_err);
+    if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, "gram_tc_kernel");
+    gram_reduce_kernel<<<64, 256, 0, st>>>(reinterpret_cast<const long long*>(tc->d_part), tc->grid,
+                                          reinterpret_cast<long long*>(tc->d_out));
+    unsigned int flag = 0;
+    if ((e = cudaMemcpyAsync(out, tc->d_out, TC_ROWS * TC_ROWS * 8, cudaMemcpyDeviceToHost, st)) != cudaSuccess)
+        return cuda_fail(e, "gram copy");
+    if ((e = cudaMemcpyAsync(&flag, tc->d_err, 4, cudaMemcpyDeviceToHost, st)) != cudaSuccess)
+        return cuda_fail(e, "gram flag");
+    if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return cuda_fail(e, "gram sync");
+    if (flag) return fail(KPZB_ETIMEOUT, "a bounded device wait in the tensor-core Gram expired");
+    return KPZB_OK;
+}
+
+}  // namespace kpzb

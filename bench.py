@@ -50,6 +50,12 @@ def parse():
     ap.add_argument("--fusion", type=int, default=0, help="MCS per HBM pass (0 = library default)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--only-pq", type=int, default=-1,
+                    help="run only lattice i of the headline pair (profiling a single rate)")
+    ap.add_argument("--lx", type=int, default=0,
+                    help="override the workload's log2 lattice side (small cases for ncu)")
+    ap.add_argument("--workload", choices=["scabit", "dt", "batch", "gram"], default="scabit",
+                    help="scabit: the headline 16384^2 SCA runs; dt / batch / gram: the other configs")
     return ap.parse_args()
 
 
@@ -143,7 +149,9 @@ def run_ours(args, world, rank, local):
 
     dev_stream = torch.cuda.Stream()
     scheds = []
-    for (p, q) in PQS:
+    pqs = PQS if args.only_pq < 0 else [PQS[args.only_pq]]
+    LX = LY = args.lx or globals()["LX"]
+    for (p, q) in pqs:
         s = kpzb.Scheduler(LX, LY, scheduler="scaBit", device=local)
         s.setPQ(p, q)
         s.supplySeed(SEED, rank)
@@ -166,38 +174,37 @@ def run_ours(args, world, rank, local):
     clocks.start()
     torch.cuda.synchronize()
     barrier(world)
-    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ev = [[torch.cuda.Event(enable_timing=True) for _ in range(len(scheds) + 1)] for _ in range(args.steps)]
     t_wall0 = time.perf_counter()
     for i in range(args.steps):
         with torch.cuda.stream(dev_stream):
             flush_l2(torch, flush)
-            starts[i].record(dev_stream)
-        step()
-        with torch.cuda.stream(dev_stream):
-            ends[i].record(dev_stream)
+        ev[i][0].record(dev_stream)
+        for j, s in enumerate(scheds):
+            s.mcsPQSyncRngAsync(M)
+            ev[i][j + 1].record(dev_stream)
     torch.cuda.synchronize()
     barrier(world)
     wall = time.perf_counter() - t_wall0
     clk = clocks.stop()
-    ms = sum(a.elapsed_time(b) for a, b in zip(starts, ends))
-    ms = max_over_ranks(ms, world)
+    per_lat = [sum(ev[i][j].elapsed_time(ev[i][j + 1]) for i in range(args.steps)) for j in range(len(scheds))]
+    ms = max_over_ranks(sum(per_lat), world)
     updates = float(N) * M * len(scheds) * args.steps * world
     value = updates / (ms * 1e6)
 
-    # launches: the library runs k-MCS fused passes (k = its resolved choice) plus a
-    # one-launch-per-half-step remainder
-    k = scheds[0].fusion()
-    fused_launches = (M // k) if k > 1 else 0
-    half_launches = 2 * (M - fused_launches * k)
-    launches_per_step = (fused_launches + half_launches) * len(scheds)
-    dominant = "scabit_fused_kernel" if k > 1 else "scabit_half_kernel"
-    if k > 1:
-        per_launch_ms = ms / (args.steps * launches_per_step)
-        bytes_per_launch = float(N) * k  # 1 B per attempted update, N*k attempts per pass
-    else:
-        per_launch_ms = ms / (args.steps * launches_per_step)
-        bytes_per_launch = float(N) / 2  # one half-step: N/2 attempts
+    # launches: each lattice runs k-MCS fused passes (k = the tuner's choice for its rates)
+    # plus a one-launch-per-half-step remainder
+    ks = [s.fusion() for s in scheds]
+    launches_per_step = 0
+    for k in ks:
+        fused = (M // k) if k > 1 else 0
+        launches_per_step += fused + 2 * (M - fused * k)
+    k = ks[0]
+    dominant = "scabit_fused_kernel" if max(ks) > 1 else "scabit_half_kernel"
+    # algorithmic bytes: 1 B per attempted update over the whole timed region, divided by the
+    # device time of the launches (fused passes carry more than 95 % of it)
+    per_launch_ms = sum(per_lat) / (args.steps * launches_per_step)
+    bytes_per_launch = float(N) * M * len(scheds) / launches_per_step
     peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (
         ROOT / "MEASURED_PEAKS.json").exists() else {}
     peak = peaks.get("hbm_gbs", 6650.0)
@@ -206,7 +213,7 @@ def run_ours(args, world, rank, local):
                 "peak": peak, "peak_source": "measured" if "hbm_gbs" in peaks else "fallback",
                 "unit": "GB/s", "frac": round(achieved / peak, 4),
                 "traffic": NCU_TRAFFIC_PER_LAUNCH, "algorithmic_bytes_per_launch": bytes_per_launch,
-                "launch_ms": round(per_launch_ms, 4), "mcs_per_launch": k if k > 1 else 0.5}
+                "launch_ms": round(per_launch_ms, 4), "mcs_per_pass": ks}
 
     e2e = None
     if not args.no_e2e:
@@ -214,7 +221,9 @@ def run_ours(args, world, rank, local):
     for s in scheds:
         s.setStream(0)
         s.close()
-    return value, ms, wall, clk, roofline, e2e, launches_per_step * args.steps, k
+    per_lattice = [{"p": p, "q": q, "mcs_per_pass": kk, "upd_per_ns": round(float(N) * M * args.steps / (t * 1e6), 1)}
+                   for (p, q), kk, t in zip(pqs, ks, per_lat)]
+    return value, ms, wall, clk, roofline, e2e, launches_per_step * args.steps, ks, per_lattice
 
 
 def run_e2e(args, torch, kpzb, scheds, N, M, world):
@@ -248,58 +257,265 @@ def run_e2e(args, torch, kpzb, scheds, N, M, world):
             "d2h_bytes_per_step": (nw * 4 + 64) * len(scheds), "steps": steps}
 
 
-def cpu_sample(nthreads=1):
-    """Oracle SCABit per-site restatement on a 2048^2 sample, (1,0) and (0.5,0.5), 1 MCS each."""
+REF_BIN = ROOT / "oracle" / "_ref" / "kpz_ref"
+REF_LX = 14  # CPU sample on the benchmark lattice itself (16384^2)
+REF_MCS = 2  # MCS per (p,q) per sample: a few seconds of CPU work on 8 cores
+
+
+def ref_sample(threads):
+    """The reference's own SchedulerCPUCBBit (kpz/schedulerCPUCBBit_nested.inl), compiled from
+    its sources into oracle/_ref/kpz_ref: REF_MCS MCS at (1,0) and at (0.5,0.5) on the 16384^2
+    lattice with `threads` threads; returns (updates/ns, seconds of timed work)."""
+    upd, secs = 0.0, 0.0
+    for (p, q) in PQS:
+        r = subprocess.run([str(REF_BIN), "bench-cbbit", str(REF_LX), str(p), str(q), str(REF_MCS), str(threads)],
+                           capture_output=True, text=True, check=True)
+        line = [ln for ln in r.stdout.splitlines() if ln and not ln.startswith("#")][0].split()
+        secs += float(line[1])
+        upd += float(1 << (2 * REF_LX)) * REF_MCS
+    return upd / (secs * 1e9), secs
+
+
+def port_sample():
+    """Fallback when the reference binary was not built: the oracle's per-site SCABit."""
     from oracle import oracle as o
-    lx = ly = 11
+    lx = 11
     t0 = time.perf_counter()
     upd = 0
     for (p, q) in PQS:
-        w = o.homogeneous(lx, ly, o.ENC_CBBIT)
-        o.sca_mcs(w, lx, ly, o.ENC_CBBIT, SEED, 0, 0, 1, p, q)
-        upd += 1 << (lx + ly)
+        w = o.homogeneous(lx, lx, o.ENC_CBBIT)
+        o.sca_mcs(w, lx, lx, o.ENC_CBBIT, SEED, 0, 0, 1, p, q)
+        upd += 1 << (2 * lx)
     dt = time.perf_counter() - t0
     return upd / (dt * 1e9), dt
 
 
+def cpu_baseline_sample(threads):
+    if REF_BIN.exists():
+        v, secs = ref_sample(threads)
+        return {"value": round(v, 6), "unit": UNIT, "cores": threads, "kind": "reference",
+                "sample": f"reference SchedulerCPUCBBit (oracle/_ref), 16384^2, {REF_MCS} MCS at (1,0) + "
+                          f"{REF_MCS} MCS at (0.5,0.5), {threads} threads, {secs:.2f} s timed"}
+    v, secs = port_sample()
+    return {"value": round(v, 6), "unit": UNIT, "cores": 1, "kind": "port",
+            "sample": f"oracle per-site SCABit, 2048^2, 1 MCS at (1,0) + 1 MCS at (0.5,0.5), {secs:.1f} s"}
+
+
 def run_reference(args, world, rank):
-    """Reference arm: the CPU implementation of the path on the host cores (rank 0 only)."""
+    """Reference arm: the reference's CPU implementation of the path on all host cores
+    (rank 0 only); each step a bounded sample of the workload (see cpu_baseline_sample)."""
     if rank != 0:
         return None
-    import multiprocessing as mp
     cores = os.cpu_count() or 1
-    ctx = mp.get_context("spawn")
-    vals = []
     for _ in range(args.warmup):
-        pass
+        cpu_baseline_sample(cores)
+    vals = []
     t0 = time.perf_counter()
-    with ctx.Pool(cores) as pool:
-        for _ in range(args.steps):
-            res = pool.map(_ref_worker, range(cores))
-            vals.append(sum(r[0] for r in res))
+    last = None
+    for _ in range(args.steps):
+        last = cpu_baseline_sample(cores)
+        vals.append(last["value"])
     wall = time.perf_counter() - t0
     value = statistics.median(vals)
-    line = {"metric": METRIC, "value": round(value, 6), "unit": UNIT, "impl": "reference",
+    last["value"] = round(value, 6)
+    return {"metric": METRIC, "value": round(value, 6), "unit": UNIT, "impl": "reference",
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": round(wall * 1e3 / args.steps, 3), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
-            "config": {"workload": "SCABit 16384^2 (p,q)=(1,0),(0.5,0.5); CPU sample 2048^2, 1 MCS "
-                                   "per (p,q) per core"},
-            "cpu_baseline": {"value": round(value, 6), "unit": UNIT, "cores": cores, "kind": "port",
-                             "sample": "2048^2 lattice, 1 MCS at (1,0) and 1 MCS at (0.5,0.5), per core"},
-            "e2e": {"value": round(value, 6), "unit": UNIT, "h2d_bytes_per_step": 0,
-                    "d2h_bytes_per_step": 0}}
-    return line
+            "config": {"workload": "SCABit 16384^2 periodic, flat start, (p,q)=(1,0) and (0.5,0.5); "
+                                   "each CPU step 2 MCS per (p,q) on the 16384^2 lattice"},
+            "cpu_baseline": last,
+            "e2e": {"value": round(value, 6), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
 
-def _ref_worker(i):
-    sys.path.insert(0, str(ROOT))
-    return cpu_sample()
+def _line(metric_value, ms_step, args, world, config, **extra):
+    d = {"metric": METRIC, "value": round(metric_value, 4), "unit": extra.pop("unit", UNIT),
+         "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_step, 4),
+         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+         "dtype": extra.pop("dtype", "u32"), "data": "synthetic", "config": config}
+    d.update(extra)
+    return d
+
+
+def _timed(torch, stream, fn, steps):
+    """Device time of `steps` calls of fn on `stream` (CUDA events), ms total."""
+    a = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+    b = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+    for i in range(steps):
+        a[i].record(stream)
+        fn()
+        b[i].record(stream)
+    torch.cuda.synchronize()
+    return sum(x.elapsed_time(y) for x, y in zip(a, b))
+
+
+def run_dt(args, world, rank, local):
+    """Config C3: DT random-sequential, 65536^2 (1 GiB ENC_LOCAL), p=0.95 q=0.05."""
+    import torch
+    torch.cuda.set_device(local)
+    import cudakpz_b200 as kpzb
+    lx = args.lx or 16
+    st = torch.cuda.Stream()
+    s = kpzb.Scheduler(lx, lx, scheduler="dt", device=local)
+    s.setPQ(0.95, 0.05)
+    s.supplySeed(1 + rank)
+    s.setStream(st.cuda_stream)
+    m = max(1, args.mcs_per_step // 100)
+    for _ in range(args.warmup):
+        s.mcsPQSyncRngAsync(m)
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local)
+    clocks.start()
+    ms = _timed(torch, st, lambda: s.mcsPQSyncRngAsync(m), args.steps)
+    clk = clocks.stop()
+    ms = max_over_ranks(ms, world)
+    N = 1 << (2 * lx)
+    value = float(N) * m * args.steps * world / (ms * 1e6)
+    launches = 4 * m * args.steps
+    per_launch = ms / launches
+    alg_launch = 0.52 * N / 4  # one domain set per launch: N/4 attempts at ~0.52 B each
+    peak = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()).get("hbm_gbs", 6650.0) if (
+        ROOT / "MEASURED_PEAKS.json").exists() else 6650.0
+    ach = alg_launch / (per_launch * 1e-3) / 1e9
+    s.setStream(0)
+    ok, rep = s.consitencyCheck()
+    s.close()
+    return _line(value, ms / args.steps, args, world,
+                 {"workload": "DT random-sequential 65536^2 periodic (1 GiB ENC_LOCAL), flat start, "
+                              "p=0.95 q=0.05, random origin + shuffled domain sets per MCS",
+                  "mcs_per_step": m, "lattice": "65536x65536", "parallelism": f"replicas x{world}"},
+                 roofline={"bound": "hbm", "kernel": "dt_kernel", "achieved": round(ach, 1), "peak": peak,
+                           "unit": "GB/s", "frac": round(ach / peak, 4), "traffic": None,
+                           "note": "integer/barrier bound; 0.52 B/attempt algorithmic"},
+                 clocks=clk, gpu_launches=launches, invariants_ok=ok)
+
+
+def run_batch(args, world, rank, local):
+    """Config C4: 512 replicas (256x256^2, 128x1024^2, 64x2048^2, 64x4096^2), rates from
+    {(1,0),(0.9,0.1),(0.75,0.25)} drawn with seed 0, replica seeds 1000+i; one batched pass
+    kernel per k MCS vs the plain per-lattice launch loop (one launch per half-step)."""
+    import numpy as np
+    import torch
+    torch.cuda.set_device(local)
+    import cudakpz_b200 as kpzb
+    lxs = [8] * 256 + [10] * 128 + [11] * 64 + [12] * 64
+    rng = np.random.default_rng(0)
+    rates = [(1.0, 0.0), (0.9, 0.1), (0.75, 0.25)]
+    pq = [rates[i] for i in rng.integers(0, 3, size=len(lxs))]
+    seeds = [1000 + i for i in range(len(lxs))]
+    sites = float(sum(1 << (2 * lx) for lx in lxs))
+    b = kpzb.Batch(lxs, [a for a, _ in pq], [c for _, c in pq], seeds, device=local)
+    m = 64
+    b.mcs(m * args.warmup)
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local)
+    clocks.start()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        b.mcs(m)
+    dt_b = time.perf_counter() - t0
+    clk = clocks.stop()
+    dt_b = max_over_ranks(dt_b, world)
+    value = sites * m * args.steps * world / (dt_b * 1e9)
+    # plain per-lattice launch loop on the same replicas (one step, same MCS)
+    hs = []
+    for i, lx in enumerate(lxs):
+        s = kpzb.Scheduler(lx, lx, device=local)
+        s.setPQ(*pq[i])
+        s.supplySeed(seeds[i])
+        s.setFusion(1)
+        hs.append(s)
+    for s in hs:
+        s.mcsPQSyncRngAsync(2)
+    for s in hs:
+        s.join()
+    t0 = time.perf_counter()
+    for s in hs:
+        s.mcsPQSyncRngAsync(m)
+    for s in hs:
+        s.join()
+    dt_plain = time.perf_counter() - t0
+    plain = sites * m / (dt_plain * 1e9)
+    # identical per-replica lattices: compare a sample of replicas after equal MCS
+    same = True
+    for i in (0, 300, 400, 500):
+        ref = kpzb.Scheduler(lxs[i], lxs[i], device=local)
+        ref.setPQ(*pq[i])
+        ref.supplySeed(seeds[i])
+        ref.mcsPQSyncRng(m * (args.warmup + args.steps))
+        same &= bool(np.array_equal(ref.popSystem(), b.pop(i)))
+        ref.close()
+    for s in hs:
+        s.close()
+    b.close()
+    return _line(value, dt_b * 1e3 / args.steps, args, world,
+                 {"workload": "512 SCABit replicas (256x256^2,128x1024^2,64x2048^2,64x4096^2), mixed (p,q)",
+                  "mcs_per_step": m, "parallelism": f"replicas x{world}"},
+                 plain_loop_value=round(plain, 3), speedup_vs_plain_loop=round(value / plain, 2),
+                 replicas_bit_identical_to_single_runs=same, clocks=clk,
+                 timing="host wall clock around synchronous batch calls")
+
+
+def run_gram(args, world, rank, local):
+    """Config C5: exact height autocorrelator, 64 snapshots of a 16384^2 SCA run at p=1 q=0
+    (snapshots after MCS 1..64), full 64x64 Gram over 2^28 sites on tcgen05 INT8 vs int64."""
+    import numpy as np
+    import torch
+    torch.cuda.set_device(local)
+    import cudakpz_b200 as kpzb
+    lx = args.lx or 14
+    N = 1 << (2 * lx)
+    s = kpzb.Scheduler(lx, lx, device=local)
+    s.setPQ(1.0, 0.0)
+    s.supplySeed(42)
+    g = kpzb.Gram(lx, lx, 64, device=local)
+    for _ in range(64):
+        s.mcsPQSyncRng(1)
+        g.add_device(s.devicePtr())
+    for _ in range(args.warmup):
+        g.compute(0)
+    clocks = ClockSampler(local)
+    clocks.start()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        G0, S0 = g.compute(0)
+    dt0 = (time.perf_counter() - t0) / args.steps
+    clk = clocks.stop()
+    t0 = time.perf_counter()
+    G1, S1 = g.compute(1)
+    dt1 = time.perf_counter() - t0
+    exact = bool(np.array_equal(G0, G1) and np.array_equal(S0, S1))
+    tops = 2.0 * 64 * 64 * N / dt0 / 1e12
+    limb_tops = 2.0 * (128 * 192 + 128 * 64) * N / dt0 / 1e12
+    hbm_bytes = 192.0 * N
+    peak = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()).get("hbm_gbs", 6650.0) if (
+        ROOT / "MEASURED_PEAKS.json").exists() else 6650.0
+    g.close()
+    s.close()
+    return _line(tops, dt0 * 1e3, args, world,
+                 {"workload": "64x64 exact height Gram, 16384^2 lattice, 3 int8 limbs, tcgen05 kind::i8",
+                  "snapshots": 64, "sites": N},
+                 unit="TOPS (2*64*64*N height-product ops / s)", dtype="int8->int32->int64",
+                 limb_tensor_tops=round(limb_tops, 1), int64_cuda_core_s=round(dt1, 4),
+                 speedup_vs_int64=round(dt1 / dt0, 2), exact_match_int64=exact,
+                 roofline={"bound": "hbm", "kernel": "gram_tc_kernel",
+                           "achieved": round(hbm_bytes / dt0 / 1e9, 1), "peak": peak, "unit": "GB/s",
+                           "frac": round(hbm_bytes / dt0 / 1e9 / peak, 4), "traffic": None},
+                 clocks=clk, timing="host wall clock around synchronous compute calls")
 
 
 def main():
     args = parse()
     world, rank, local = dist_setup(args.gpus)
+    if args.workload != "scabit" and args.impl == "ours":
+        fn = {"dt": run_dt, "batch": run_batch, "gram": run_gram}[args.workload]
+        line = fn(args, world, rank, local)
+        if rank == 0:
+            print(json.dumps(line), flush=True)
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+        return
     if args.impl == "reference":
         line = run_reference(args, world, rank)
         if line is not None:
@@ -308,12 +524,10 @@ def main():
             import torch.distributed as dist
             dist.destroy_process_group()
         return
-    value, ms, wall, clk, roofline, e2e, launches, k = run_ours(args, world, rank, local)
+    value, ms, wall, clk, roofline, e2e, launches, ks, per_lattice = run_ours(args, world, rank, local)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
-        v, dt = cpu_sample()
-        cpu = {"value": round(v, 6), "unit": UNIT, "cores": 1, "kind": "port",
-               "sample": f"oracle per-site SCABit, 2048^2, 1 MCS at (1,0) + 1 MCS at (0.5,0.5), {dt:.1f} s"}
+        cpu = cpu_baseline_sample(os.cpu_count() or 1)
     if rank == 0:
         line = {"metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 4),
@@ -322,10 +536,11 @@ def main():
                 "config": {"workload": "SCABit 16384^2 periodic, flat start, (p,q)=(1,0) and (0.5,0.5), "
                                        "seed 42, counter-based random bits",
                            "lattice": "16384x16384", "mcs_per_step": args.mcs_per_step,
-                           "lattices_per_gpu": len(PQS), "mcs_per_pass": k,
+                           "lattices_per_gpu": len(PQS), "mcs_per_pass": ks,
                            "l2": "flushed between steps (256 MiB write, untimed)",
                            "parallelism": f"replicas x{world}"},
-                "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk,
+                "per_lattice": per_lattice, "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
+                "clocks": clk,
                 "gpu_launches": launches, "wall_s": round(wall, 3)}
         print(json.dumps(line), flush=True)
     if world > 1:

@@ -12,6 +12,7 @@
 // Three passes: (1) per-row x=0 slopes and x-slope sums, (2) one-CTA scan over rows to
 // get row-start heights, (3) per-site walk with a CTA-wide scan of 64-site chunk sums.
 // Per-CTA partials are reduced in a fixed order so the FP64 sums are deterministic.
+#include "kpzb_api_internal.h"
 #include "kpzb_common.cuh"
 #include "kpzb_internal.h"
 
@@ -441,3 +442,78 @@ cudaError_t analysis_invariants(const uint32_t* d_sys, int lx, int ly, AnalysisS
 }
 
 }  // namespace kpzb
+
+// ---------------------------------------------------------------------------------------
+// Roughness without any allocation (kpzb_roughness_noalloc).
+//
+// Some callers cannot allocate device memory at the point where they want a measurement:
+// an application whose memory manager owns the whole device (a caching allocator that must
+// see every allocation, or a budget already spent on lattices), or a timing loop that must
+// not stall other streams -- cudaMalloc and cudaFree can synchronize the device.  For them
+// this entry point reads a caller's device lattice and writes the caller's host output, and
+// keeps its scratch (row tables and per-CTA partial sums) in one file-scope device array of
+// fixed size.  Every GPU that loads the library holds the array until the process exits.
+//
+// Limit: ly <= NOALLOC_MAX_LY (at most 65536 rows); any lx the other entry points accept.
+// The array is shared by every call: concurrent calls that overlap on the GPU (on different
+// streams or host threads) race on it and must be serialized by the caller.  Every kernel
+// writes each scratch word before reading it, so nothing has to be cleared between calls.
+// On each device the first call looks up the array's device address with
+// cudaGetSymbolAddress while that device is current; that first call should therefore come
+// before any stream capture the caller starts.
+// ---------------------------------------------------------------------------------------
+namespace kpzb {
+
+constexpr int NOALLOC_MAX_LY = 16;
+constexpr size_t NOALLOC_ROWINFO = 2ull * (1ull << NOALLOC_MAX_LY) * sizeof(int32_t);
+constexpr size_t NOALLOC_ROWSTART = (1ull << NOALLOC_MAX_LY) * sizeof(int64_t);
+constexpr size_t NOALLOC_PARTIALS = (AN_MAX_GRID + 1) * sizeof(Partial);
+constexpr size_t NOALLOC_BYTES = NOALLOC_ROWINFO + NOALLOC_ROWSTART + NOALLOC_PARTIALS;
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[NOALLOC_BYTES];
+
+namespace {
+constexpr int NOALLOC_MAX_DEVICES = 64;
+void* g_noalloc_addr[NOALLOC_MAX_DEVICES] = {};
+}  // namespace
+
+}  // namespace kpzb
+
+extern "C" kpzb_status kpzb_roughness_noalloc(const uint32_t* d_cbbit, int lx, int ly, double out[8],
+                                              void* stream)
+{
+    using namespace kpzb;
+    if (!d_cbbit || !out) return fail(KPZB_EINVAL, "null lattice or output");
+    if (lx < 8 || lx > 30 || ly < 2 || lx + ly < 14 || lx + ly > 38)
+        return fail(KPZB_EINVAL, "lattice size out of range (8<=lx<=30, 14<=lx+ly<=38)");
+    if (ly > NOALLOC_MAX_LY)
+        return fail(KPZB_EINVAL, "ly > 16: the fixed no-allocation scratch holds at most 65536 rows");
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
+    if (dev < 0 || dev >= NOALLOC_MAX_DEVICES) return fail(KPZB_EINVAL, "device index beyond 63");
+    if (!g_noalloc_addr[dev]) {
+        void* p = nullptr;
+        e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess || !p) return cuda_fail(e, "cudaGetSymbolAddress(no-alloc scratch)");
+        g_noalloc_addr[dev] = p;
+    }
+    unsigned char* base = static_cast<unsigned char*>(g_noalloc_addr[dev]);
+    AnalysisScratch view;
+    view.rowinfo = reinterpret_cast<int32_t*>(base);
+    view.rowstart = reinterpret_cast<int64_t*>(base + NOALLOC_ROWINFO);
+    view.acc = reinterpret_cast<unsigned long long*>(base + NOALLOC_ROWINFO + NOALLOC_ROWSTART);
+    view.rows_cap = 1ull << NOALLOC_MAX_LY;
+    MomentsOut m;
+    e = analysis_moments(d_cbbit, nullptr, lx, ly, &view, &m, static_cast<cudaStream_t>(stream));
+    if (e != cudaSuccess) return cuda_fail(e, "roughness (no-alloc)");
+    const long double N = (long double)((uint64_t)1 << (lx + ly));
+    long double h[7];
+    h[0] = (long double)m.s1 / N;
+    h[1] = (long double)m.s2 / N;
+    for (int k = 0; k < 5; ++k) h[2 + k] = (long double)m.s3to7[k] / N;
+    out[0] = (double)(h[1] - h[0] * h[0]);
+    for (int k = 0; k < 7; ++k) out[1 + k] = (double)h[k];
+    return KPZB_OK;
+}
+

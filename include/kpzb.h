@@ -108,6 +108,15 @@ int kpzb_encoding(const kpzb_handle* h);
 /* SchedulerService::roughness (kpz/schedulerService.cpp:292-297, kpz/correlator.cpp:607-697):
  * out[0] = W^2, out[1..7] = <h^k> of the path-relative heights (kpz/correlator.cpp:47-96). */
 kpzb_status kpzb_roughness(kpzb_handle* h, double out[8]);
+/* Roughness (as kpzb_roughness) of a caller's device ENC_CBBIT lattice, without allocating:
+ * no cudaMalloc/cudaFree or allocating library call; scratch lives in a fixed device array
+ * of about 1.2 MB held by every GPU that loads the library.  For callers that cannot
+ * allocate device memory at measurement time (their allocator owns the device, or an
+ * allocation would synchronize the device inside a timing loop).  No counterpart in the
+ * reference.  Limit: ly <= 16.  Calls overlapping on the GPU race on the shared scratch; the
+ * first call on each device looks up the scratch address and should precede any stream
+ * capture.  `stream` is a cudaStream_t (NULL: default stream); synchronous. */
+kpzb_status kpzb_roughness_noalloc(const uint32_t* d_cbbit, int lx, int ly, double out[8], void* stream);
 /* Exact power sums of the relative heights: s12[0] = sum h, s12[1] = sum h^2,
  * hminmax[0..1] = min/max height. */
 kpzb_status kpzb_height_sums(kpzb_handle* h, int64_t s12[2], int64_t hminmax[2]);

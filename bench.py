@@ -227,7 +227,8 @@ def run_ours(args, world, rank, local):
 
 
 def run_e2e(args, torch, kpzb, scheds, N, M, world):
-    """Public API with host buffers: push (pinned H2D) -> mcs -> pop (D2H) -> roughness."""
+    """Public API with host buffers: push (pinned H2D) -> mcs -> pop (D2H) -> roughness, every
+    step, both lattices, through the asynchronous push/pop entry points."""
     import numpy as np
     nw = scheds[0].size_words()
     host = [torch.empty(nw, dtype=torch.int32).pin_memory() for _ in scheds]
@@ -243,10 +244,13 @@ def run_e2e(args, torch, kpzb, scheds, N, M, world):
     barrier(world)
     t0 = time.perf_counter()
     for _ in range(steps):
+        # each lattice on its own stream: one lattice's copies overlap the other's MCS
         for h, o, s in zip(host, outs, scheds):
-            s.pushSystem(h.numpy().view(np.uint32))
-            s.mcsPQSyncRng(M)
-            s.popSystem(o.numpy().view(np.uint32))
+            s.pushSystemAsync(h.numpy().view(np.uint32))
+            s.mcsPQSyncRngAsync(M)
+            s.popSystemAsync(o.numpy().view(np.uint32))
+        for s in scheds:
+            s.join()
             s.roughness()
     torch.cuda.synchronize()
     dt = time.perf_counter() - t0

@@ -52,6 +52,8 @@ SIGNATURES = {
     "kpzb_autotune": (C.c_int, [_vp, _intp, _intp, C.POINTER(C.c_float)]),
     "kpzb_push": (C.c_int, [_vp, _vp]),
     "kpzb_pop": (C.c_int, [_vp, _vp]),
+    "kpzb_push_async": (C.c_int, [_vp, _vp]),
+    "kpzb_pop_async": (C.c_int, [_vp, _vp]),
     "kpzb_push_device": (C.c_int, [_vp, _vp]),
     "kpzb_pop_device": (C.c_int, [_vp, _vp]),
     "kpzb_size_words": (C.c_size_t, [_vp]),

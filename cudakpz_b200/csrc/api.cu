@@ -326,7 +326,7 @@ extern "C" kpzb_status kpzb_mcs(kpzb_handle* h, int n)
 extern "C" size_t kpzb_size_words(const kpzb_handle* h) { return h ? h->words() : 0; }
 extern "C" int kpzb_encoding(const kpzb_handle* h) { return h ? h->encoding() : -1; }
 
-static kpzb_status push_from(kpzb_handle* h, const uint32_t* src, cudaMemcpyKind kind)
+static kpzb_status push_from(kpzb_handle* h, const uint32_t* src, cudaMemcpyKind kind, bool sync = true)
 {
     if (h->dyn == KPZB_DYN_SCA) {
         kpzb_status s = ensure_tmp(h);
@@ -336,11 +336,11 @@ static kpzb_status push_from(kpzb_handle* h, const uint32_t* src, cudaMemcpyKind
     } else {
         KPZB_CU(cudaMemcpyAsync(h->d_sys, src, h->words() * 4, kind, h->st), "push copy");
     }
-    KPZB_CU(cudaStreamSynchronize(h->st), "push sync");
+    if (sync) KPZB_CU(cudaStreamSynchronize(h->st), "push sync");
     return KPZB_OK;
 }
 
-static kpzb_status pop_to(kpzb_handle* h, uint32_t* dst, cudaMemcpyKind kind)
+static kpzb_status pop_to(kpzb_handle* h, uint32_t* dst, cudaMemcpyKind kind, bool sync = true)
 {
     if (h->dyn == KPZB_DYN_SCA) {
         kpzb_status s = ensure_tmp(h);
@@ -350,7 +350,7 @@ static kpzb_status pop_to(kpzb_handle* h, uint32_t* dst, cudaMemcpyKind kind)
     } else {
         KPZB_CU(cudaMemcpyAsync(dst, h->d_sys, h->words() * 4, kind, h->st), "pop copy");
     }
-    KPZB_CU(cudaStreamSynchronize(h->st), "pop sync");
+    if (sync) KPZB_CU(cudaStreamSynchronize(h->st), "pop sync");
     return KPZB_OK;
 }
 
@@ -365,6 +365,18 @@ extern "C" kpzb_status kpzb_pop(kpzb_handle* h, uint32_t* words)
     KPZB_CHECK_H(h);
     if (!words) return fail(KPZB_EINVAL, "null buffer");
     return pop_to(h, words, cudaMemcpyDeviceToHost);
+}
+extern "C" kpzb_status kpzb_push_async(kpzb_handle* h, const uint32_t* words)
+{
+    KPZB_CHECK_H(h);
+    if (!words) return fail(KPZB_EINVAL, "null buffer");
+    return push_from(h, words, cudaMemcpyHostToDevice, false);
+}
+extern "C" kpzb_status kpzb_pop_async(kpzb_handle* h, uint32_t* words)
+{
+    KPZB_CHECK_H(h);
+    if (!words) return fail(KPZB_EINVAL, "null buffer");
+    return pop_to(h, words, cudaMemcpyDeviceToHost, false);
 }
 extern "C" kpzb_status kpzb_push_device(kpzb_handle* h, const uint32_t* d_words)
 {

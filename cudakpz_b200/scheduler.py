@@ -181,6 +181,19 @@ class Scheduler:
             raise ValueError(f"expected {self.size_words()} words, got {w.size}")
         check(lib.kpzb_push(self._h, w.ctypes.data), "kpzb_push")
 
+    def pushSystemAsync(self, words: np.ndarray) -> None:
+        """Enqueue the host->device copy; `words` must stay alive (and should be page-locked)
+        until join()."""
+        if words.dtype != np.uint32 or not words.flags.c_contiguous or words.size != self.size_words():
+            raise ValueError("expected a contiguous uint32 array of size_words() words")
+        check(lib.kpzb_push_async(self._h, words.ctypes.data), "kpzb_push_async")
+
+    def popSystemAsync(self, out: np.ndarray) -> np.ndarray:
+        if out.dtype != np.uint32 or not out.flags.c_contiguous or out.size != self.size_words():
+            raise ValueError("expected a contiguous uint32 array of size_words() words")
+        check(lib.kpzb_pop_async(self._h, out.ctypes.data), "kpzb_pop_async")
+        return out
+
     def popSystem(self, out: Optional[np.ndarray] = None) -> np.ndarray:
         if out is None:
             out = np.empty(self.size_words(), dtype=np.uint32)

@@ -99,6 +99,12 @@ kpzb_status kpzb_autotune(kpzb_handle* h, int* mcs_per_pass, int* ctas_per_sm, f
  * in the handle's encoding (kpzb_size_words words) to / from the device. */
 kpzb_status kpzb_push(kpzb_handle* h, const uint32_t* words);
 kpzb_status kpzb_pop(kpzb_handle* h, uint32_t* words);
+/* Asynchronous push/pop: enqueued on the handle's stream behind earlier work, returning at
+ * once; the host buffer must stay valid until kpzb_join.  With page-locked host buffers the
+ * copies overlap other handles' MCS.  (The reference copies synchronously after join():
+ * kpz/schedulerBase.cu:35-52.) */
+kpzb_status kpzb_push_async(kpzb_handle* h, const uint32_t* words);
+kpzb_status kpzb_pop_async(kpzb_handle* h, uint32_t* words);
 /* Same, with device buffers of the caller (cudaMemcpyDeviceToDevice on the handle's stream). */
 kpzb_status kpzb_push_device(kpzb_handle* h, const uint32_t* d_words);
 kpzb_status kpzb_pop_device(kpzb_handle* h, uint32_t* d_words);

@@ -165,3 +165,25 @@ def test_full_size_first_mcs_vs_oracle(kpzb, oracle):
     oracle.sca_mcs(ref, lx, ly, oracle.ENC_CBBIT, 42, 0, 0, 2, 1.0, 0.0)
     got = run_gpu(kpzb, lx, ly, "scaBit", 1.0, 0.0, 42, 2, fusion=0)
     assert first_diff(got, ref) is None, first_diff(got, ref)
+
+
+@pytest.mark.parametrize("sched", ["scaBit", "sca"])
+def test_async_push_pop_equals_sync(kpzb, oracle, sched):
+    """kpzb_push_async -> kpzb_mcs_async -> kpzb_pop_async -> kpzb_join == the synchronous path."""
+    lx = ly = 10
+    enc = oracle.ENC_CBBIT if sched == "scaBit" else oracle.ENC_LOCAL
+    init = oracle.random_lattice(lx, ly, oracle.ENC_CBBIT, seed=21, mcs=3)
+    if enc == oracle.ENC_LOCAL:
+        init = oracle.cbbit_to_local(init, lx, ly)
+    ref = init.copy()
+    oracle.sca_mcs(ref, lx, ly, enc, 8, 0, 0, 9, 0.5, 0.5)
+    s = kpzb.Scheduler(lx, ly, scheduler=sched)
+    s.setPQ(0.5, 0.5)
+    s.supplySeed(8)
+    out = np.empty_like(init)
+    s.pushSystemAsync(init)
+    s.mcsPQSyncRngAsync(9)
+    s.popSystemAsync(out)
+    s.join()
+    assert np.array_equal(out, ref)
+    s.close()

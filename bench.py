@@ -4,7 +4,7 @@
 Workload (one GPU): two resident 16384x16384 periodic lattices (2^28 sites, 64 MiB packed
 each, ENC_CBBIT), flat start, one at (p,q) = (1,0) and one at (0.5,0.5), counter-based
 random bits from seed 42.  A step advances each lattice by --mcs-per-step Monte-Carlo
-steps (default 200, so 50 steps cover the 10^4 MCS of the configuration).  Inputs are
+steps (default 200; the default 50 steps are the 10^4 MCS of the configuration).  Inputs are
 resident in HBM when the timed region starts; L2 is flushed between steps (untimed).
 
 value  = whole-job attempted updates / ns, device time (CUDA events on the lattices' stream),
@@ -35,15 +35,16 @@ PQS = [(1.0, 0.0), (0.5, 0.5)]
 METRIC = "site updates/ns (SCA, DT, batched) vs plain loop; exact correlator TOPS"
 UNIT = "attempted site updates/ns"
 
-# Per-launch DRAM traffic of scabit_fused_kernel measured by ncu (dram__bytes_read.sum +
-# dram__bytes_write.sum), summarised in profiles/scabit_fused_16384.md; None until captured.
-NCU_TRAFFIC_PER_LAUNCH = None
+# Per-launch DRAM traffic (dram__bytes_read.sum + dram__bytes_write.sum) of the fused pass
+# kernel at 16384^2, from one ncu capture per (p, q, MCS per pass); the commands and the
+# full figures are in profiles/scabit_fused_16384.md.
+NCU_TRAFFIC_PER_LAUNCH = {(1.0, 0.0, 7): 67.326e6 + 23.604e6, (0.5, 0.5, 4): 67.237e6 + 18.461e6}
 
 
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--mcs-per-step", type=int, default=200)
@@ -88,29 +89,71 @@ def max_over_ranks(x, world):
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+    """SM clocks and throttle reasons sampled every 10 ms during the timed region (NVML via
+    nvidia-ml-py, read only; nvidia-smi at its 100 ms minimum when NVML is unavailable)."""
 
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    NAMES = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
 
     def __init__(self, gpu_index):
         self.gpu = gpu_index
         self.proc = None
         self.path = None
+        self.thread = None
+        self.samples = []
+        self.reasons = set()
+        self.smax = None
+
+    def _nvml_loop(self, nv, h):
+        bits = {"hw_slowdown": nv.nvmlClocksEventReasonHwSlowdown,
+                "hw_thermal_slowdown": nv.nvmlClocksEventReasonHwThermalSlowdown,
+                "sw_thermal_slowdown": nv.nvmlClocksEventReasonSwThermalSlowdown,
+                "sw_power_cap": nv.nvmlClocksEventReasonSwPowerCap}
+        while not self.stop_flag:
+            try:
+                self.samples.append(float(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)))
+                r = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+                for nm, b in bits.items():
+                    if r & b:
+                        self.reasons.add(nm)
+            except Exception:  # pragma: no cover - depends on the driver
+                pass
+            time.sleep(0.01)
 
     def start(self):
+        import threading
+        self.stop_flag = False
+        try:
+            import pynvml as nv
+            nv.nvmlInit()
+            vis = os.environ.get("CUDA_VISIBLE_DEVICES")
+            idx = int(vis.split(",")[self.gpu]) if vis and vis.split(",")[0].isdigit() else self.gpu
+            h = nv.nvmlDeviceGetHandleByIndex(idx)
+            self.smax = float(nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM))
+            self.thread = threading.Thread(target=self._nvml_loop, args=(nv, h), daemon=True)
+            self.thread.start()
+            return
+        except Exception:
+            self.thread = None
         fd, self.path = tempfile.mkstemp(suffix=".csv")
         os.close(fd)
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.Q}",
-                 "--format=csv,noheader,nounits", "-lms", "200"],
+                 "--format=csv,noheader,nounits", "-lms", "100"],
                 stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
         except OSError:
             self.proc = None
 
     def stop(self):
+        if self.thread is not None:
+            self.stop_flag = True
+            self.thread.join(timeout=5)
+            sm = self.samples
+            return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": self.smax,
+                    "reasons": sorted(self.reasons), "samples": len(sm), "source": "nvml 10 ms"}
         if self.proc is None:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
         self.proc.terminate()
@@ -119,7 +162,6 @@ class ClockSampler:
         except subprocess.TimeoutExpired:
             self.proc.kill()
         sm, smax, reasons = [], [], set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         for line in Path(self.path).read_text().splitlines():
             f = [x.strip() for x in line.split(",")]
             if len(f) < 9:
@@ -129,13 +171,13 @@ class ClockSampler:
                 smax.append(float(f[2]))
             except ValueError:
                 continue
-            for nm, v in zip(names, f[5:9]):
+            for nm, v in zip(self.NAMES, f[5:9]):
                 if v.lower() == "active":
                     reasons.add(nm)
         os.unlink(self.path)
         return {"sm_mhz": statistics.median(sm) if sm else None,
                 "sm_max_mhz": max(smax) if smax else None,
-                "reasons": sorted(reasons), "samples": len(sm)}
+                "reasons": sorted(reasons), "samples": len(sm), "source": "nvidia-smi 100 ms"}
 
 
 def flush_l2(torch, buf):
@@ -212,8 +254,28 @@ def run_ours(args, world, rank, local):
     roofline = {"bound": "hbm", "kernel": dominant, "achieved": round(achieved, 1),
                 "peak": peak, "peak_source": "measured" if "hbm_gbs" in peaks else "fallback",
                 "unit": "GB/s", "frac": round(achieved / peak, 4),
-                "traffic": NCU_TRAFFIC_PER_LAUNCH, "algorithmic_bytes_per_launch": bytes_per_launch,
+                "traffic": fused_traffic(pqs, ks, M, LX), "algorithmic_bytes_per_launch": bytes_per_launch,
                 "launch_ms": round(per_launch_ms, 4), "mcs_per_pass": ks}
+
+    # INT roofline: the bitwise update's algorithmic ALU operations against the measured
+    # LOP3 throughput of this GPU (probe kernel, a few ms, after the timed region)
+    lop3, iadd3 = kpzb.probe_alu_peak(local)
+    opw = [alu_ops_per_word(p, q) for (p, q) in pqs]
+    int_roofline = None
+    if None not in opw:
+        ops_step = sum(float(N) * M * o / 32.0 for o in opw)
+        int_ach = ops_step * args.steps / (sum(per_lat) * 1e-3)
+        upd_per_op = float(N) * M * len(scheds) / ops_step  # attempts per algorithmic ALU op
+        int_roof_upd = lop3 * upd_per_op / 1e9
+        hbm_roof_upd = peak  # 1 B per attempt: GB/s == attempts/ns
+        int_roofline = {"bound": "int-alu", "achieved": round(int_ach / 1e12, 3),
+                        "peak": round(lop3 / 1e12, 3), "unit": "Tops/s", "frac": round(int_ach / lop3, 4),
+                        "peak_source": "measured live (kpzb_probe_alu_peak, 3-input LOP3 chains)",
+                        "iadd3_peak": round(iadd3 / 1e12, 3),
+                        "alu_ops_per_word": {f"{p},{q}": o for (p, q), o in zip(pqs, opw)},
+                        "roofline_upd_per_ns": round(int_roof_upd, 1)}
+        roofline["slower_roofline"] = "hbm" if hbm_roof_upd <= int_roof_upd else "int-alu"
+        roofline["frac_of_slower_roofline"] = round(value / min(hbm_roof_upd, int_roof_upd), 4)
 
     e2e = None
     if not args.no_e2e:
@@ -223,7 +285,42 @@ def run_ours(args, world, rank, local):
         s.close()
     per_lattice = [{"p": p, "q": q, "mcs_per_pass": kk, "upd_per_ns": round(float(N) * M * args.steps / (t * 1e6), 1)}
                    for (p, q), kk, t in zip(pqs, ks, per_lat)]
+    roofline["int_roofline"] = int_roofline
     return value, ms, wall, clk, roofline, e2e, launches_per_step * args.steps, ks, per_lattice
+
+
+def fused_traffic(pqs, ks, M, lx):
+    """Launch-weighted mean DRAM bytes per fused pass from the ncu captures, when every
+    lattice ran a captured (p, q, k) at 16384^2; None otherwise."""
+    if lx != 14:
+        return None
+    tot, n = 0.0, 0
+    for (p, q), k in zip(pqs, ks):
+        t = NCU_TRAFFIC_PER_LAUNCH.get((p, q, k))
+        if t is None or k < 2:
+            return None
+        tot += t * (M // k)
+        n += M // k
+    return round(tot / n) if n else None
+
+
+def alu_ops_per_word(p, q):
+    """Algorithmic integer-ALU operations per 32-site word per half-step of the SCABit rule
+    (kpz/kpzSCABitCores.cu:69-74,139-145), counted as 3-input LOP3 / funnel-shift steps:
+    minimum candidates 2 (when p > 0), maximum candidates 2 (when q > 0), their union 1 (when
+    both), XOR of the flip mask into the four words 4, the one-bit x-shift of every other row 1
+    (2 shifts on half the rows), and per random plane 1 to apply it plus the ALU part of
+    Philox4x32-10 per word (10 rounds x 2 three-way XORs / 4 words = 5; its multiplies run on
+    the FMA pipe).  p, q in {0, 1} need no plane, 1/2 one; other rates are not counted here."""
+    ops = 4 + 1
+    ops += 2 if p > 0 else 0
+    ops += 2 if q > 0 else 0
+    ops += 1 if (p > 0 and q > 0) else 0
+    planes = sum(1 for r in (p, q) if 0 < r < 1) and 1
+    if any(0 < r < 1 and r != 0.5 for r in (p, q)):
+        return None
+    ops += planes * (1 + 5)
+    return ops
 
 
 def run_e2e(args, torch, kpzb, scheds, N, M, world):
@@ -385,9 +482,9 @@ def run_dt(args, world, rank, local):
     ok, rep = s.consitencyCheck()
     s.close()
     return _line(value, ms / args.steps, args, world,
-                 {"workload": "DT random-sequential 65536^2 periodic (1 GiB ENC_LOCAL), flat start, "
-                              "p=0.95 q=0.05, random origin + shuffled domain sets per MCS",
-                  "mcs_per_step": m, "lattice": "65536x65536", "parallelism": f"replicas x{world}"},
+                 {"workload": f"DT random-sequential {1 << lx}^2 periodic ({N // 4 >> 20} MiB ENC_LOCAL), "
+                              "flat start, p=0.95 q=0.05, random origin + shuffled domain sets per MCS",
+                  "mcs_per_step": m, "lattice": f"{1 << lx}x{1 << lx}", "parallelism": f"replicas x{world}"},
                  roofline={"bound": "hbm", "kernel": "dt_kernel", "achieved": round(ach, 1), "peak": peak,
                            "unit": "GB/s", "frac": round(ach / peak, 4), "traffic": None,
                            "note": "integer/barrier bound; 0.52 B/attempt algorithmic"},

@@ -39,6 +39,7 @@ _vp = C.c_void_p
 SIGNATURES = {
     "kpzb_last_error": (C.c_char_p, []),
     "kpzb_version": (C.c_char_p, []),
+    "kpzb_probe_alu_peak": (C.c_int, [C.c_int, _dblp, _dblp]),
     "kpzb_create": (C.c_int, [C.POINTER(_vp), C.c_int, C.c_int, C.c_int, C.c_int]),
     "kpzb_destroy": (C.c_int, [_vp]),
     "kpzb_init_homogeneous": (C.c_int, [_vp]),

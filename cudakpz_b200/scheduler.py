@@ -343,3 +343,11 @@ class Gram:
         check(lib.kpzb_gram_compute(self._h, method, G.ctypes.data_as(C.POINTER(C.c_int64)),
                                     S1.ctypes.data_as(C.POINTER(C.c_int64))), "kpzb_gram_compute")
         return G, S1
+
+
+def probe_alu_peak(device: int = -1):
+    """Measured integer-ALU throughput (LOP3 chain ops/s, 3-input add chain ops/s) of a GPU:
+    the denominator of the INT roofline of the bitwise SCA update (kpzb_probe_alu_peak)."""
+    a, b = C.c_double(0.0), C.c_double(0.0)
+    check(lib.kpzb_probe_alu_peak(device, C.byref(a), C.byref(b)), "kpzb_probe_alu_peak")
+    return a.value, b.value

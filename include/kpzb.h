@@ -55,6 +55,11 @@ typedef struct kpzb_handle kpzb_handle;
 const char* kpzb_last_error(void);
 /* Library version string. */
 const char* kpzb_version(void);
+/* Measured integer-ALU throughput of `device` (-1: current), in thread-level operations per
+ * second: a 3-input LOP3 chain and a 3-input IADD3 chain over 8 CTAs of 256 threads per SM,
+ * CUDA-event timed (a few ms).  The denominator of the INT roofline of the bitwise SCA
+ * update.  No counterpart in the reference (a measurement helper). */
+kpzb_status kpzb_probe_alu_peak(int device, double* lop3_per_s, double* iadd3_per_s);
 
 /* Create a scheduler for a 2^lx x 2^ly lattice on `device` (-1: current device).
  * Replaces SchedulerSCA/SchedulerSCABit/SchedulerDT constructors + SchedulerBase::initCUDA

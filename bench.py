@@ -38,7 +38,8 @@ UNIT = "attempted site updates/ns"
 # Per-launch DRAM traffic (dram__bytes_read.sum + dram__bytes_write.sum) of the fused pass
 # kernel at 16384^2, from one ncu capture per (p, q, MCS per pass); the commands and the
 # full figures are in profiles/scabit_fused_16384.md.
-NCU_TRAFFIC_PER_LAUNCH = {(1.0, 0.0, 7): 67.326e6 + 23.604e6, (0.5, 0.5, 4): 67.237e6 + 18.461e6}
+NCU_TRAFFIC_PER_LAUNCH = {(1.0, 0.0, "band", 7): 67.326e6 + 23.604e6,
+                          (0.5, 0.5, "band", 4): 67.237e6 + 18.461e6}
 
 
 def parse():
@@ -55,6 +56,9 @@ def parse():
                     help="run only lattice i of the headline pair (profiling a single rate)")
     ap.add_argument("--lx", type=int, default=0,
                     help="override the workload's log2 lattice side (small cases for ncu)")
+    ap.add_argument("--reference-gpu", action="store_true",
+                    help="with --impl reference: time the reference's own CUDA scheduler on this GPU "
+                         "(oracle/_ref/kpz_ref_gpu) instead of its CPU scheduler")
     ap.add_argument("--workload", choices=["scabit", "dt", "batch", "gram"], default="scabit",
                     help="scabit: the headline 16384^2 SCA runs; dt / batch / gram: the other configs")
     return ap.parse_args()
@@ -234,15 +238,17 @@ def run_ours(args, world, rank, local):
     updates = float(N) * M * len(scheds) * args.steps * world
     value = updates / (ms * 1e6)
 
-    # launches: each lattice runs k-MCS fused passes (k = the tuner's choice for its rates)
-    # plus a one-launch-per-half-step remainder
-    ks = [s.fusion() for s in scheds]
+    # launches: each lattice runs k-MCS passes of its pass kernel (the tuner's choice for its
+    # rates) plus a one-launch-per-half-step remainder
+    plans = [s.plan() for s in scheds]
+    ks = [pl[0] for pl in plans]
     launches_per_step = 0
     for k in ks:
         fused = (M // k) if k > 1 else 0
         launches_per_step += fused + 2 * (M - fused * k)
-    k = ks[0]
-    dominant = "scabit_fused_kernel" if max(ks) > 1 else "scabit_half_kernel"
+    kinds = sorted({pl[2] for pl in plans if pl[0] > 1})
+    dominant = {"stream": "scabit_stream_kernel", "band": "scabit_fused_kernel"}[kinds[0]] if len(
+        kinds) == 1 else ("+".join(kinds) if kinds else "scabit_half_kernel")
     # algorithmic bytes: 1 B per attempted update over the whole timed region, divided by the
     # device time of the launches (fused passes carry more than 95 % of it)
     per_launch_ms = sum(per_lat) / (args.steps * launches_per_step)
@@ -254,8 +260,9 @@ def run_ours(args, world, rank, local):
     roofline = {"bound": "hbm", "kernel": dominant, "achieved": round(achieved, 1),
                 "peak": peak, "peak_source": "measured" if "hbm_gbs" in peaks else "fallback",
                 "unit": "GB/s", "frac": round(achieved / peak, 4),
-                "traffic": fused_traffic(pqs, ks, M, LX), "algorithmic_bytes_per_launch": bytes_per_launch,
-                "launch_ms": round(per_launch_ms, 4), "mcs_per_pass": ks}
+                "traffic": fused_traffic(pqs, plans, M, LX), "algorithmic_bytes_per_launch": bytes_per_launch,
+                "launch_ms": round(per_launch_ms, 4), "mcs_per_pass": ks,
+                "plans": [{"mcs_per_pass": a, "ctas_per_sm": b, "kernel": c} for a, b, c in plans]}
 
     # INT roofline: the bitwise update's algorithmic ALU operations against the measured
     # LOP3 throughput of this GPU (probe kernel, a few ms, after the timed region)
@@ -283,20 +290,21 @@ def run_ours(args, world, rank, local):
     for s in scheds:
         s.setStream(0)
         s.close()
-    per_lattice = [{"p": p, "q": q, "mcs_per_pass": kk, "upd_per_ns": round(float(N) * M * args.steps / (t * 1e6), 1)}
-                   for (p, q), kk, t in zip(pqs, ks, per_lat)]
+    per_lattice = [{"p": p, "q": q, "mcs_per_pass": kk, "kernel": pl[2],
+                    "upd_per_ns": round(float(N) * M * args.steps / (t * 1e6), 1)}
+                   for (p, q), kk, pl, t in zip(pqs, ks, plans, per_lat)]
     roofline["int_roofline"] = int_roofline
     return value, ms, wall, clk, roofline, e2e, launches_per_step * args.steps, ks, per_lattice
 
 
-def fused_traffic(pqs, ks, M, lx):
-    """Launch-weighted mean DRAM bytes per fused pass from the ncu captures, when every
-    lattice ran a captured (p, q, k) at 16384^2; None otherwise."""
+def fused_traffic(pqs, plans, M, lx):
+    """Launch-weighted mean DRAM bytes per pass from the ncu captures, when every lattice ran a
+    captured (p, q, pass kernel, k) at 16384^2; None otherwise."""
     if lx != 14:
         return None
     tot, n = 0.0, 0
-    for (p, q), k in zip(pqs, ks):
-        t = NCU_TRAFFIC_PER_LAUNCH.get((p, q, k))
+    for (p, q), (k, _, kind) in zip(pqs, plans):
+        t = NCU_TRAFFIC_PER_LAUNCH.get((p, q, kind, k))
         if t is None or k < 2:
             return None
         tot += t * (M // k)
@@ -427,6 +435,57 @@ def run_reference(args, world, rank):
                                    "each CPU step 2 MCS per (p,q) on the 16384^2 lattice"},
             "cpu_baseline": last,
             "e2e": {"value": round(value, 6), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+REF_GPU_BIN = ROOT / "oracle" / "_ref" / "kpz_ref_gpu"
+
+
+def run_reference_gpu(args, world, rank, local):
+    """The reference's own CUDA schedulers on this GPU (rank 0 only): SchedulerSCABit<SLCG64>
+    (kpz/schedulerSCABit.cu, kpz/kpzSCABit.cu) for the headline workload, SchedulerDT<SLCG64,
+    dis> with its default DBSH inner decomposition (kpz/schedulerDT.cu, kpz/kpz.cu) for
+    --workload dt, built from the CudaKpz sources into oracle/_ref/kpz_ref_gpu and driven
+    through their public mcsPQSyncRng (host wall time around the synchronous call)."""
+    if rank != 0:
+        return None
+    if not REF_GPU_BIN.exists():
+        return {"impl": "reference", "device": "gpu",
+                "unavailable": "oracle/_ref/kpz_ref_gpu not built (needs the CudaKpz sources and nvcc)"}
+    env = dict(os.environ, CUDA_VISIBLE_DEVICES=os.environ.get("CUDA_VISIBLE_DEVICES", str(local)))
+    clocks = ClockSampler(local)
+    runs = []
+    if args.workload == "dt":
+        lx = args.lx or 16
+        m = args.steps * max(1, args.mcs_per_step // 100)
+        jobs = [("dt", lx, 0.95, 0.05, max(1, args.warmup // 3), m)]
+        config = {"workload": f"reference SchedulerDT<SLCG64, dis> (DBSH), {1 << lx}^2, p=0.95 q=0.05",
+                  "mcs_timed": m}
+    else:
+        lx = args.lx or LX
+        m = args.steps * args.mcs_per_step
+        jobs = [("scabit", lx, p, q, max(2, args.warmup), m) for (p, q) in PQS]
+        config = {"workload": f"reference SchedulerSCABit<SLCG64>, {1 << lx}^2, flat start, (p,q)=(1,0) and "
+                              "(0.5,0.5)", "mcs_timed_per_lattice": m}
+    clocks.start()
+    for (cmd, lxx, p, q, warm, n) in jobs:
+        r = subprocess.run([str(REF_GPU_BIN), cmd, str(lxx), str(p), str(q), str(warm), str(n)],
+                           capture_output=True, text=True, env=env, timeout=1200)
+        if r.returncode != 0:
+            clocks.stop()
+            return {"impl": "reference", "device": "gpu",
+                    "unavailable": f"kpz_ref_gpu {cmd} exited {r.returncode}: {r.stderr.strip()[-200:]}"}
+        f = [ln for ln in r.stdout.splitlines() if ln and not ln.startswith("#")][-1].split()
+        runs.append({"p": p, "q": q, "upd_per_ns": round(float(f[0]), 1), "seconds": round(float(f[1]), 4),
+                     "w2": float(f[2]), "mcs": n, "lattice": f"{1 << lxx}x{1 << lxx}", "sites": 1 << (2 * lxx)})
+    clk = clocks.stop()
+    upd = sum(float(x["sites"]) * x["mcs"] for x in runs)
+    secs = sum(x["seconds"] for x in runs)
+    value = upd / (secs * 1e9)
+    return {"metric": METRIC, "value": round(value, 3), "unit": UNIT, "impl": "reference", "device": "gpu",
+            "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": round(secs * 1e3 / args.steps, 4), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "u32", "data": "synthetic", "config": config, "per_lattice": runs,
+            "timing": "host wall clock around the reference's synchronous mcsPQSyncRng", "clocks": clk}
 
 
 def _line(metric_value, ms_step, args, world, config, **extra):
@@ -612,6 +671,14 @@ def main():
         fn = {"dt": run_dt, "batch": run_batch, "gram": run_gram}[args.workload]
         line = fn(args, world, rank, local)
         if rank == 0:
+            print(json.dumps(line), flush=True)
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+        return
+    if args.impl == "reference" and args.reference_gpu:
+        line = run_reference_gpu(args, world, rank, local)
+        if line is not None:
             print(json.dumps(line), flush=True)
         if world > 1:
             import torch.distributed as dist

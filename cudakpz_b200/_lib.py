@@ -35,6 +35,14 @@ _dblp = C.POINTER(C.c_double)
 _intp = C.POINTER(C.c_int)
 _vp = C.c_void_p
 
+class Sampling(C.Structure):
+    """kpzb_sampling (include/kpzb.h)."""
+    _fields_ = [("mode", C.c_int), ("density", C.c_double), ("interval", C.c_uint32),
+                ("random_mean", C.c_double), ("seed", C.c_uint64)]
+
+
+SAMPLE_EXP, SAMPLE_LINEAR, SAMPLE_RANDOM = 0, 1, 2
+
 # name -> (restype, argtypes); every symbol declared in include/kpzb.h
 SIGNATURES = {
     "kpzb_last_error": (C.c_char_p, []),
@@ -50,6 +58,12 @@ SIGNATURES = {
     "kpzb_join": (C.c_int, [_vp]),
     "kpzb_set_fusion": (C.c_int, [_vp, C.c_int]),
     "kpzb_get_fusion": (C.c_int, [_vp, _intp]),
+    "kpzb_get_plan": (C.c_int, [_vp, _intp, _intp, _intp]),
+    "kpzb_save": (C.c_int, [_vp, C.c_char_p, C.c_char_p]),
+    "kpzb_load": (C.c_int, [_vp, C.c_char_p]),
+    "kpzb_sample_times": (C.c_int, [C.POINTER(Sampling), C.c_uint64, C.c_uint64, _u64p, C.c_int, _intp]),
+    "kpzb_measure_run": (C.c_int, [_vp, C.POINTER(Sampling), C.c_uint64, C.c_int64, C.c_uint64, _dblp,
+                                   C.c_int, _intp]),
     "kpzb_autotune": (C.c_int, [_vp, _intp, _intp, C.POINTER(C.c_float)]),
     "kpzb_push": (C.c_int, [_vp, _vp]),
     "kpzb_pop": (C.c_int, [_vp, _vp]),

@@ -12,6 +12,7 @@
 // Three passes: (1) per-row x=0 slopes and x-slope sums, (2) one-CTA scan over rows to
 // get row-start heights, (3) per-site walk with a CTA-wide scan of 64-site chunk sums.
 // Per-CTA partials are reduced in a fixed order so the FP64 sums are deterministic.
+#include <cstring>
 #include "kpzb_api_internal.h"
 #include "kpzb_common.cuh"
 #include "kpzb_internal.h"
@@ -291,6 +292,46 @@ static cudaError_t row_tables(const uint32_t* d, int lx, int ly, int32_t* ri, in
     const int grid = (int)((rows * 32 + 255) / 256 < 4096 ? (rows * 32 + 255) / 256 : 4096);
     rowinfo_kernel<<<grid, 256, 0, st>>>(d, lx, ly, ri);
     rowstart_kernel<<<1, 1024, 0, st>>>(ri, ly, rs);
+    return cudaGetLastError();
+}
+
+size_t analysis_record_bytes() { return sizeof(Partial); }
+
+void analysis_decode_record(const void* rec, MomentsOut* out)
+{
+    Partial h;
+    memcpy(&h, rec, sizeof h);
+    out->s1 = h.s1;
+    out->s2 = h.s2;
+    for (int k = 0; k < 5; ++k) out->s3to7[k] = h.s[k];
+    out->hmin = h.hmin;
+    out->hmax = h.hmax;
+    out->cross = h.cross;
+    out->agree = h.agree;
+    out->snap_s1 = h.snap_s1;
+}
+
+cudaError_t analysis_moments_record(const uint32_t* d_sys, const uint32_t* d_snap, int lx, int ly,
+                                    AnalysisScratch* s, void* d_rec, cudaStream_t st)
+{
+    const uint64_t rows = 1ull << ly;
+    int32_t* ri = s->rowinfo;
+    int32_t* ri_s = s->rowinfo + 2 * rows;
+    int64_t* rs = s->rowstart;
+    int64_t* rs_s = s->rowstart + rows;
+    Partial* parts = reinterpret_cast<Partial*>(s->acc);
+    cudaError_t e = row_tables(d_sys, lx, ly, ri, rs, st);
+    if (e != cudaSuccess) return e;
+    const int grid = walk_grid(lx, ly);
+    if (d_snap) {
+        if ((e = row_tables(d_snap, lx, ly, ri_s, rs_s, st)) != cudaSuccess) return e;
+        walk_kernel<1><<<grid, AN_THREADS, 0, st>>>(d_sys, d_snap, lx, ly, ri, rs, ri_s, rs_s,
+                                                    nullptr, parts);
+    } else {
+        walk_kernel<0><<<grid, AN_THREADS, 0, st>>>(d_sys, nullptr, lx, ly, ri, rs, nullptr,
+                                                    nullptr, nullptr, parts);
+    }
+    final_reduce_kernel<<<1, 32, 0, st>>>(parts, grid, reinterpret_cast<Partial*>(d_rec));
     return cudaGetLastError();
 }
 

@@ -4,7 +4,9 @@
 // (kpz/schedulerBase.cu:35-99).  Differences by design: one CUDA stream per handle, no
 // busy-wait event loop, integer status codes instead of exceptions/exit, counter-based RNG
 // keyed by (seed, stream) instead of per-thread TinyMT/SLCG state.
+#include <algorithm>
 #include <cmath>
+#include <vector>
 #include <cstdlib>
 #include <cstdio>
 #include <cstring>
@@ -198,9 +200,25 @@ extern "C" kpzb_status kpzb_get_fusion(kpzb_handle* h, int* mcs_per_pass)
     Plan p;
     kpzb_status s = resolve_plan(h, &p);
     if (s != KPZB_OK) return s;
-    int k = p.k;
-    if (k > 1 && !scabit_fused_shape_cps(h->lx, h->ly, k, p.cps, 0).ok) k = 1;
-    *mcs_per_pass = k;
+    *mcs_per_pass = plan_shape_ok(p, h->lx, h->ly, h->sm_count) ? p.k : 1;
+    return KPZB_OK;
+}
+
+extern "C" kpzb_status kpzb_get_plan(kpzb_handle* h, int* mcs_per_pass, int* ctas_per_sm, int* pass_kernel)
+{
+    if (!h || !mcs_per_pass || !ctas_per_sm || !pass_kernel) return fail(KPZB_EINVAL, "null argument");
+    *mcs_per_pass = 1;
+    *ctas_per_sm = 0;
+    *pass_kernel = KPZB_PASS_HALF_STEPS;
+    if (h->dyn == KPZB_DYN_DT) return KPZB_OK;
+    Plan p;
+    kpzb_status s = resolve_plan(h, &p);
+    if (s != KPZB_OK) return s;
+    if (p.k > 1 && plan_shape_ok(p, h->lx, h->ly, h->sm_count)) {
+        *mcs_per_pass = p.k;
+        *ctas_per_sm = p.kind == PASS_STREAM && p.cps == 0 ? 1 : p.cps;
+        *pass_kernel = p.kind == PASS_STREAM ? KPZB_PASS_STREAM : KPZB_PASS_BAND;
+    }
     return KPZB_OK;
 }
 
@@ -218,7 +236,7 @@ static uint64_t thresh_of(double p)
 static kpzb_status resolve_plan(kpzb_handle* h, Plan* plan)
 {
     if (h->fusion > 0) {
-        *plan = Plan{h->fusion, 0, 0.f, false};
+        *plan = explicit_plan(h->lx, h->ly, h->fusion, h->sm_count);
         return KPZB_OK;
     }
     const uint64_t Tp = thresh_of(h->p), Tq = thresh_of(h->q);
@@ -258,7 +276,21 @@ static kpzb_status enqueue_sca(kpzb_handle* h, int n)
     kpzb_status ps = resolve_plan(h, &plan);
     if (ps != KPZB_OK) return ps;
     const int k = plan.k;
-    if (k > 1) {
+    if (k > 1 && plan.kind == PASS_STREAM) {
+        const StreamShape ss = scabit_stream_shape(h->lx, h->ly, k, h->sm_count, plan.cps ? plan.cps : 1);
+        if (ss.ok) {
+            kpzb_status s = ensure_tmp(h);
+            if (s != KPZB_OK) return s;
+            while (n - done >= k) {
+                KPZB_CU(scabit_stream(h->d_sys, h->d_tmp, h->lx, h->ly, (uint32_t)(h->tdev + done),
+                                      h->seed, h->stream_id, Tp, Tq, ss, cnt,
+                                      reinterpret_cast<unsigned int*>(h->d_counters + 2), h->st),
+                        "scabit_stream");
+                std::swap(h->d_sys, h->d_tmp);
+                done += k;
+            }
+        }
+    } else if (k > 1) {
         FusedShape fs = scabit_fused_shape_cps(h->lx, h->ly, k, plan.cps, 0);
         if (fs.ok) {
             kpzb_status s = ensure_tmp(h);
@@ -480,6 +512,256 @@ extern "C" kpzb_status kpzb_correlate(kpzb_handle* h, double out[10])
     const long double N = (long double)((uint64_t)1 << (h->lx + h->ly));
     out[8] = (double)((long double)(double)m.cross / N - h0 * (long double)h->snap_mean);
     out[9] = (double)((long double)m.agree / N / 2.0L);
+    return KPZB_OK;
+}
+
+// ---------------------------------------------------------------------------------
+// Checkpoint / resume (saveBit layout, kpz/schedulerService.cpp:389-401, plus a trailer)
+// ---------------------------------------------------------------------------------
+namespace {
+const char CKPT_MAGIC[8] = {'K', 'P', 'Z', 'B', 'C', 'K', 'P', 'T'};
+struct CkptTrailer {  // little-endian, written field by field
+    uint32_t version, dyn, lx, ly;
+    uint64_t tdev, seed;
+    uint32_t stream_id, fusion;
+    double p, q;
+    uint32_t has_snap, reserved;
+    double snap_mean;
+};
+}  // namespace
+
+extern "C" kpzb_status kpzb_save(kpzb_handle* h, const char* path, const char* meta)
+{
+    KPZB_CHECK_H(h);
+    if (!path) return fail(KPZB_EINVAL, "null path");
+    std::vector<uint32_t> words(h->words());
+    kpzb_status st = kpzb_pop(h, words.data());
+    if (st != KPZB_OK) return st;
+    std::vector<uint32_t> snap;
+    if (h->has_snap) {
+        snap.resize(h->words());
+        KPZB_CU(cudaMemcpyAsync(snap.data(), h->d_snap, snap.size() * 4, cudaMemcpyDeviceToHost, h->st), "snapshot");
+        KPZB_CU(cudaStreamSynchronize(h->st), "snapshot");
+    }
+    FILE* f = fopen(path, "wb");
+    if (!f) return fail(KPZB_EINVAL, "cannot open the checkpoint file for writing");
+    bool ok = fprintf(f, "%d\n%d\n", h->lx, h->ly) > 0;
+    if (meta) ok = ok && fputs(meta, f) >= 0;
+    ok = ok && fputc('\0', f) != EOF;
+    ok = ok && fwrite(words.data(), 4, words.size(), f) == words.size();
+    CkptTrailer t{};
+    t.version = 1;
+    t.dyn = (uint32_t)h->dyn;
+    t.lx = (uint32_t)h->lx;
+    t.ly = (uint32_t)h->ly;
+    t.tdev = h->tdev;
+    t.seed = h->seed;
+    t.stream_id = h->stream_id;
+    t.fusion = (uint32_t)h->fusion;
+    t.p = h->p;
+    t.q = h->q;
+    t.has_snap = h->has_snap ? 1u : 0u;
+    t.snap_mean = h->snap_mean;
+    ok = ok && fwrite(CKPT_MAGIC, 1, 8, f) == 8 && fwrite(&t, sizeof t, 1, f) == 1;
+    if (h->has_snap) ok = ok && fwrite(snap.data(), 4, snap.size(), f) == snap.size();
+    ok = (fclose(f) == 0) && ok;
+    return ok ? KPZB_OK : fail(KPZB_EINVAL, "checkpoint write failed");
+}
+
+extern "C" kpzb_status kpzb_load(kpzb_handle* h, const char* path)
+{
+    KPZB_CHECK_H(h);
+    if (!path) return fail(KPZB_EINVAL, "null path");
+    FILE* f = fopen(path, "rb");
+    if (!f) return fail(KPZB_EINVAL, "cannot open the checkpoint file");
+    int lx = -1, ly = -1;
+    bool ok = fscanf(f, "%d\n%d", &lx, &ly) == 2;
+    if (ok) {  // rest of the second line, then the meta text up to its '\0'
+        int c;
+        while ((c = fgetc(f)) != EOF && c != '\n') {
+        }
+        while ((c = fgetc(f)) != EOF && c != '\0') {
+        }
+        ok = c == '\0';
+    }
+    if (!ok || lx != h->lx || ly != h->ly) {
+        fclose(f);
+        return fail(KPZB_EINVAL, "not a lattice file of this handle's size");
+    }
+    std::vector<uint32_t> words(h->words());
+    if (fread(words.data(), 4, words.size(), f) != words.size()) {
+        fclose(f);
+        return fail(KPZB_EINVAL, "truncated lattice words");
+    }
+    char magic[8];
+    CkptTrailer t{};
+    std::vector<uint32_t> snap;
+    const bool has_trailer = fread(magic, 1, 8, f) == 8 && memcmp(magic, CKPT_MAGIC, 8) == 0;
+    if (has_trailer) {
+        ok = fread(&t, sizeof t, 1, f) == 1 && t.version == 1 && t.lx == (uint32_t)h->lx &&
+             t.ly == (uint32_t)h->ly && t.dyn == (uint32_t)h->dyn;
+        if (ok && t.has_snap) {
+            snap.resize(h->words());
+            ok = fread(snap.data(), 4, snap.size(), f) == snap.size();
+        }
+    }
+    fclose(f);
+    if (!ok) return fail(KPZB_EINVAL, "bad checkpoint trailer (other dynamics, size or version)");
+    kpzb_status st = kpzb_push(h, words.data());
+    if (st != KPZB_OK) return st;
+    if (has_trailer) {
+        h->tdev = t.tdev;
+        h->seed = t.seed;
+        h->stream_id = t.stream_id;
+        h->fusion = (int)t.fusion;
+        h->p = t.p;
+        h->q = t.q;
+        h->has_snap = t.has_snap != 0;
+        h->snap_mean = t.snap_mean;
+        if (h->has_snap) {
+            if (!h->d_snap) KPZB_CU(cudaMalloc(&h->d_snap, h->words() * 4), "cudaMalloc(snapshot)");
+            KPZB_CU(cudaMemcpyAsync(h->d_snap, snap.data(), snap.size() * 4, cudaMemcpyHostToDevice, h->st), "snapshot");
+            KPZB_CU(cudaStreamSynchronize(h->st), "snapshot");
+        }
+    }
+    return KPZB_OK;
+}
+
+// ---------------------------------------------------------------------------------
+// Measurement scheduling (kpz/sampling.h:84-100, kpz/kpzScaling.cpp:194-215)
+// ---------------------------------------------------------------------------------
+constexpr uint32_t TAG_SAMPLE = 6u;
+
+static bool next_sample(const kpzb_sampling* s, uint64_t t, uint64_t index, uint64_t* next)
+{
+    double v;
+    if (s->mode == KPZB_SAMPLE_LINEAR) {
+        *next = t + s->interval;
+        return true;
+    }
+    if (s->mode == KPZB_SAMPLE_EXP) {
+        v = std::ceil(std::exp(std::log((double)t + 10.0) + s->density));
+    } else {
+        const uint32_t ctr[4] = {(uint32_t)index, (uint32_t)(index >> 32), TAG_SAMPLE << 24, 0u};
+        uint32_t r[4];
+        philox_host(ctr, s->seed, r);
+        const double u = (double)r[0] * (1.0 / 4294967296.0);
+        v = (double)t + std::floor(u * s->random_mean + s->random_mean);
+    }
+    if (!(v < 1.8e19)) return false;
+    uint64_t n = (uint64_t)v;
+    *next = n > t ? n : t + 1;
+    return true;
+}
+
+static kpzb_status check_sampling(const kpzb_sampling* s)
+{
+    if (!s) return fail(KPZB_EINVAL, "null sampling");
+    if (s->mode == KPZB_SAMPLE_LINEAR && s->interval == 0) return fail(KPZB_EINVAL, "linear interval 0");
+    if (s->mode == KPZB_SAMPLE_EXP && !(s->density > 0.0)) return fail(KPZB_EINVAL, "exp density <= 0");
+    if (s->mode == KPZB_SAMPLE_RANDOM && !(s->random_mean > 0.0)) return fail(KPZB_EINVAL, "random mean <= 0");
+    if (s->mode < KPZB_SAMPLE_EXP || s->mode > KPZB_SAMPLE_RANDOM) return fail(KPZB_EINVAL, "unknown mode");
+    return KPZB_OK;
+}
+
+static kpzb_status sample_times(const kpzb_sampling* s, uint64_t start, uint64_t end, std::vector<uint64_t>* out)
+{
+    kpzb_status st = check_sampling(s);
+    if (st != KPZB_OK) return st;
+    out->clear();
+    uint64_t t = start, idx = 0;
+    while (t < end) {
+        uint64_t n;
+        if (!next_sample(s, t, idx++, &n)) return fail(KPZB_EINVAL, "sample time overflow");
+        t = n < end ? n : end;
+        out->push_back(t);
+        if (out->size() > (1u << 26)) return fail(KPZB_EINVAL, "more than 2^26 sample times");
+    }
+    return KPZB_OK;
+}
+
+extern "C" kpzb_status kpzb_sample_times(const kpzb_sampling* s, uint64_t start, uint64_t end, uint64_t* times,
+                                         int max, int* n)
+{
+    if (!n || (max > 0 && !times)) return fail(KPZB_EINVAL, "null argument");
+    std::vector<uint64_t> v;
+    kpzb_status st = sample_times(s, start, end, &v);
+    if (st != KPZB_OK) return st;
+    for (size_t i = 0; i < v.size() && (int)i < max; ++i) times[i] = v[i];
+    *n = (int)v.size();
+    return KPZB_OK;
+}
+
+extern "C" kpzb_status kpzb_measure_run(kpzb_handle* h, const kpzb_sampling* s, uint64_t end, int64_t corr_start,
+                                        uint64_t corr_stop, double* rows, int max_rows, int* n_rows)
+{
+    KPZB_CHECK_H(h);
+    if (!n_rows || (max_rows > 0 && !rows)) return fail(KPZB_EINVAL, "null argument");
+    if (end >= (1ull << 31)) return fail(KPZB_EINVAL, "device MCS counter limit 2^31");
+    const uint64_t t_now = h->tdev;
+    std::vector<uint64_t> times;
+    kpzb_status st = sample_times(s, t_now, end, &times);
+    if (st != KPZB_OK) return st;
+    const bool tag = corr_start >= 0 && (uint64_t)corr_start >= t_now && (uint64_t)corr_start <= end;
+    if (tag && (uint64_t)corr_start > t_now &&
+        !std::binary_search(times.begin(), times.end(), (uint64_t)corr_start)) {
+        times.insert(std::upper_bound(times.begin(), times.end(), (uint64_t)corr_start), (uint64_t)corr_start);
+    }
+    const bool tag_now = tag && (uint64_t)corr_start == t_now;  // snapshot before any MCS
+    *n_rows = (int)times.size() + (tag_now ? 1 : 0);
+    if (*n_rows > max_rows) return fail(KPZB_EINVAL, "rows buffer too small (see *n_rows)");
+    if (tag_now) times.insert(times.begin(), t_now);
+    if (times.empty()) return KPZB_OK;
+
+    const size_t rb = analysis_record_bytes();
+    unsigned char* d_rec = nullptr;
+    KPZB_CU(cudaMallocAsync(&d_rec, rb * times.size(), h->st), "cudaMallocAsync(records)");
+    if (tag && !h->d_snap) KPZB_CU(cudaMalloc(&h->d_snap, h->words() * 4), "cudaMalloc(snapshot)");
+    kpzb_status rs = KPZB_OK;
+    int snap_row = -1;
+    for (size_t i = 0; i < times.size() && rs == KPZB_OK; ++i) {
+        const uint64_t t = times[i];
+        if (t > h->tdev) {
+            rs = kpzb_mcs_async(h, (int)(t - h->tdev));
+            if (rs != KPZB_OK) break;
+        }
+        const uint32_t* v;
+        rs = cbbit_view(h, &v);
+        if (rs != KPZB_OK) break;
+        const bool corr = tag && snap_row >= 0 && t > (uint64_t)corr_start && t <= corr_stop;
+        cudaError_t e = analysis_moments_record(v, corr ? h->d_snap : nullptr, h->lx, h->ly, &h->an, d_rec + i * rb, h->st);
+        if (e == cudaSuccess && tag && t == (uint64_t)corr_start) {
+            e = cudaMemcpyAsync(h->d_snap, v, h->words() * 4, cudaMemcpyDeviceToDevice, h->st);
+            snap_row = (int)i;
+        }
+        if (e != cudaSuccess) rs = cuda_fail(e, "measurement");
+    }
+    std::vector<unsigned char> host(rb * times.size());
+    cudaError_t e = cudaMemcpyAsync(host.data(), d_rec, host.size(), cudaMemcpyDeviceToHost, h->st);
+    cudaFreeAsync(d_rec, h->st);
+    kpzb_status js = kpzb_join(h);  // also reports a bounded device wait that expired
+    if (rs != KPZB_OK) return rs;
+    if (e != cudaSuccess) return cuda_fail(e, "measurement records");
+    if (js != KPZB_OK) return js;
+    const long double N = (long double)((uint64_t)1 << (h->lx + h->ly));
+    long double snap_mean = 0.0L;
+    for (size_t i = 0; i < times.size(); ++i) {
+        MomentsOut m;
+        analysis_decode_record(host.data() + i * rb, &m);
+        double* row = rows + 11 * i;
+        long double h0;
+        row[0] = (double)times[i];
+        fill_roughness(m, h->lx, h->ly, row + 1, &h0);
+        row[9] = row[10] = std::nan("");
+        if ((int)i == snap_row) {
+            snap_mean = h0;
+            h->snap_mean = (double)h0;
+            h->has_snap = true;
+        } else if (snap_row >= 0 && (int)i > snap_row && times[i] <= corr_stop) {
+            row[9] = (double)((long double)(double)m.cross / N - h0 * (long double)(double)snap_mean);
+            row[10] = (double)((long double)m.agree / N / 2.0L);
+        }
+    }
     return KPZB_OK;
 }
 

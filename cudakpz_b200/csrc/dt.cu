@@ -124,8 +124,9 @@ dt_kernel(uint32_t* __restrict__ sys, int lxw, int lyw, int lnbx, int nblocks, i
     }
 }
 
-// Host copy of the Philox4x32-10 bijection for the per-MCS origin and domain-set order.
-static void philox_host(const uint32_t ctr[4], uint64_t seed, uint32_t out[4])
+// Host copy of the Philox4x32-10 bijection for the per-MCS origin and domain-set order (and
+// the random measurement spacing of kpzb_sample_times).
+void philox_host(const uint32_t ctr[4], uint64_t seed, uint32_t out[4])
 {
     uint32_t c0 = ctr[0], c1 = ctr[1], c2 = ctr[2], c3 = ctr[3];
     uint32_t k0 = (uint32_t)seed, k1 = (uint32_t)(seed >> 32);

@@ -15,18 +15,29 @@ int sm_count_of(int device);
 int auto_fusion(int lx, int ly);
 
 // SCABit pass shape: k MCS per HBM pass (1 = one launch per half-step), cps CTAs per SM
-// (0 = shape heuristic), and the measured cost when it came from the tuner.
+// (0 = shape heuristic), the measured cost when it came from the tuner, and the pass kernel
+// (band: scabit_fused_kernel, stream: scabit_stream_kernel).
+enum PassKernel { PASS_BAND = 0, PASS_STREAM = 1 };
 struct Plan {
     int k;
     int cps;
     float ms_per_mcs;
     bool tuned;
+    int kind;
 };
+// Pass kernel and CTAs per SM for an explicitly set fusion depth: the streaming kernel with one
+// chunk per SM, unless the environment variable KPZB_PASS_KERNEL says "band" or "stream2" (two
+// chunks per SM), or the streaming shape does not fit.
+Plan explicit_plan(int lx, int ly, int k, int sm_count);
+bool plan_shape_ok(const Plan& p, int lx, int ly, int sm_count);
 bool lookup_plan(int lx, int ly, uint64_t Tp, uint64_t Tq, int sm_count, Plan* out);
 Plan default_plan(int lx, int ly);
 cudaError_t tune_plan(uint32_t* d_src, int lx, int ly, uint64_t seed, uint32_t stream_id,
                       uint64_t Tp, uint64_t Tq, int sm_count, unsigned int* d_err,
                       cudaStream_t st, Plan* out);
+
+// Philox4x32-10 on the host (the same bijection as the device stream).
+void philox_host(const uint32_t ctr[4], uint64_t seed, uint32_t out[4]);
 
 // Double-tiling random-sequential scheduler state (dt.cu).
 struct DtState {

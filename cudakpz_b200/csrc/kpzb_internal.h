@@ -32,6 +32,22 @@ cudaError_t scabit_fused(const uint32_t* d_src, uint32_t* d_dst, int lx, int ly,
                          const FusedShape& sh, unsigned long long* d_counters, unsigned int* d_err,
                          cudaStream_t st);
 
+// Streaming (wavefront) temporal blocking: k MCS per HBM pass, a chunk of rows per CTA.
+struct StreamShape {
+    int mcs;       // MCS per pass
+    int slots;     // ring slots (rows of all four quadrants) in shared memory
+    int prefetch;  // rows loaded ahead of first use (beyond the one-tick minimum)
+    int threads;   // threads per CTA
+    size_t smem;   // dynamic shared memory bytes
+    int grid;      // chunks (CTAs)
+    bool ok;
+};
+StreamShape scabit_stream_shape(int lx, int ly, int mcs_per_pass, int sm_count, int ctas_per_sm);
+cudaError_t scabit_stream(const uint32_t* d_src, uint32_t* d_dst, int lx, int ly, uint32_t t0,
+                          uint64_t seed, uint32_t stream_id, uint64_t Tp, uint64_t Tq,
+                          const StreamShape& sh, unsigned long long* d_counters, unsigned int* d_err,
+                          cudaStream_t st);
+
 // codec / init
 cudaError_t init_homogeneous_dev(uint32_t* d, int lx, int ly, int encoding, cudaStream_t st);
 cudaError_t local_to_cbbit_dev(const uint32_t* local, uint32_t* cbbit, int lx, int ly, cudaStream_t st);
@@ -57,6 +73,13 @@ struct MomentsOut {
 };
 cudaError_t analysis_moments(const uint32_t* d_sys, const uint32_t* d_snap, int lx, int ly,
                              AnalysisScratch* s, MomentsOut* out, cudaStream_t st);
+// The same moments left on the device: the final reduction record is written to d_rec
+// (analysis_record_bytes() bytes) on stream st, with no host synchronisation; decode a host
+// copy with analysis_decode_record.
+size_t analysis_record_bytes();
+cudaError_t analysis_moments_record(const uint32_t* d_sys, const uint32_t* d_snap, int lx, int ly,
+                                    AnalysisScratch* s, void* d_rec, cudaStream_t st);
+void analysis_decode_record(const void* rec, MomentsOut* out);
 cudaError_t analysis_heights(const uint32_t* d_sys, int lx, int ly, AnalysisScratch* s,
                              int32_t* d_heights, cudaStream_t st);
 // invariants: rep[0] bad rows, rep[1] bad columns, rep[2] bad plaquettes

@@ -174,9 +174,10 @@ cudaError_t scabit_half(uint32_t* d_sys, int lx, int ly, int sigma, uint32_t ste
 // with shared-memory atomicXor; all other words have a single writer.
 // ---------------------------------------------------------------------------------
 constexpr int FUSED_THREADS = 512;
+constexpr int FUSED_THREADS_WIDE = 1024;  // mode-specialised variants fit 64 registers
 
-template <bool COUNT>
-__global__ void __launch_bounds__(FUSED_THREADS)
+template <int MODE, bool USEQ, bool COUNT, int NT>
+__global__ void __launch_bounds__(NT, 1)
 scabit_fused_kernel(const uint32_t* __restrict__ src, uint32_t* __restrict__ dst, int lx, int ly,
                     uint32_t t0, Key key, uint32_t stream, Thresh tp, Thresh tq, int B, int k,
                     unsigned long long* __restrict__ counters, unsigned int* __restrict__ err)
@@ -192,7 +193,7 @@ scabit_fused_kernel(const uint32_t* __restrict__ src, uint32_t* __restrict__ dst
     const BandCtl ctl{&bar, &abort_flag, 0u};
     const BandGeom g{src, dst, lx, ly, (int64_t)blockIdx.x * B, B, k, false, t0, key, stream, tp, tq};
     unsigned long long ndep = 0, ndes = 0;
-    if (!scabit_band<COUNT, FUSED_THREADS>(smem, ctl, g, ndep, ndes, err)) return;
+    if (!scabit_band<MODE, USEQ, COUNT, NT>(smem, ctl, g, ndep, ndes, err)) return;
     if (COUNT) {
         for (int o = 16; o > 0; o >>= 1) {
             ndep += __shfl_xor_sync(0xffffffffu, ndep, o);
@@ -223,10 +224,13 @@ FusedShape scabit_fused_shape(int lx, int ly, int mcs_per_pass, int sm_count, si
 }
 
 // ctas_per_sm: 1 or 2 CTAs resident per SM (2 lets one CTA's TMA load overlap the other's
-// compute); 0 picks 2 when the band stays at least as tall as the halo, else 1.
+// compute); 0 picks 2 when the band stays at least as tall as the halo, else 1; 3 = one CTA
+// per SM of 1024 threads (the rate-specialised kernels; the general decision keeps 512).
 FusedShape scabit_fused_shape_cps(int lx, int ly, int mcs_per_pass, int ctas_per_sm,
                                   size_t smem_optin)
 {
+    const bool wide = ctas_per_sm == 3;
+    if (wide) ctas_per_sm = 1;
     FusedShape f{};
     f.ok = false;
     if (smem_optin == 0) smem_optin = 227 * 1024;
@@ -252,11 +256,44 @@ FusedShape scabit_fused_shape_cps(int lx, int ly, int mcs_per_pass, int ctas_per
     f.band = B;
     f.halo = 2 * k;
     f.mcs = k;
-    f.threads = FUSED_THREADS;
+    f.threads = wide ? FUSED_THREADS_WIDE : FUSED_THREADS;
     f.smem = (size_t)R * row_bytes;
     f.grid = (int)((rows + B - 1) / B);
     f.ok = true;  // the load loop handles halos that wrap the lattice more than once
     return f;
+}
+
+template <int MODE, bool USEQ, bool COUNT>
+static cudaError_t launch_fused(const uint32_t* d_src, uint32_t* d_dst, int lx, int ly, uint32_t t0, Key key,
+                                uint32_t stream_id, Thresh tp, Thresh tq, const FusedShape& sh,
+                                unsigned long long* d_counters, unsigned int* d_err, cudaStream_t st)
+{
+    // the general bit-serial decision keeps 512 threads (its registers do not fit 64)
+    auto kern = scabit_fused_kernel<MODE, USEQ, COUNT, FUSED_THREADS>;
+    int nt = FUSED_THREADS;
+    if constexpr (MODE != DEC_GENERAL) {
+        if (sh.threads == FUSED_THREADS_WIDE) {
+            kern = scabit_fused_kernel<MODE, USEQ, COUNT, FUSED_THREADS_WIDE>;
+            nt = FUSED_THREADS_WIDE;
+        }
+    }
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh.smem);
+    if (e != cudaSuccess) return e;
+    kern<<<sh.grid, nt, sh.smem, st>>>(d_src, d_dst, lx, ly, t0, key, stream_id, tp, tq, sh.band, sh.mcs,
+                                       d_counters, d_err);
+    return cudaGetLastError();
+}
+
+template <int MODE, bool USEQ>
+static cudaError_t launch_fused_c(const uint32_t* d_src, uint32_t* d_dst, int lx, int ly, uint32_t t0, Key key,
+                                  uint32_t stream_id, Thresh tp, Thresh tq, const FusedShape& sh,
+                                  unsigned long long* d_counters, unsigned int* d_err, cudaStream_t st)
+{
+    if (d_counters)
+        return launch_fused<MODE, USEQ, true>(d_src, d_dst, lx, ly, t0, key, stream_id, tp, tq, sh, d_counters,
+                                              d_err, st);
+    return launch_fused<MODE, USEQ, false>(d_src, d_dst, lx, ly, t0, key, stream_id, tp, tq, sh, nullptr, d_err,
+                                           st);
 }
 
 cudaError_t scabit_fused(const uint32_t* d_src, uint32_t* d_dst, int lx, int ly, uint32_t t0,
@@ -266,21 +303,17 @@ cudaError_t scabit_fused(const uint32_t* d_src, uint32_t* d_dst, int lx, int ly,
 {
     const Key key = make_key(seed);
     const Thresh tp = make_thresh(Tp), tq = make_thresh(Tq);
-    cudaError_t e;
-    if (d_counters) {
-        e = cudaFuncSetAttribute(scabit_fused_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)sh.smem);
-        if (e != cudaSuccess) return e;
-        scabit_fused_kernel<true><<<sh.grid, sh.threads, sh.smem, st>>>(
-            d_src, d_dst, lx, ly, t0, key, stream_id, tp, tq, sh.band, sh.mcs, d_counters, d_err);
-    } else {
-        e = cudaFuncSetAttribute(scabit_fused_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)sh.smem);
-        if (e != cudaSuccess) return e;
-        scabit_fused_kernel<false><<<sh.grid, sh.threads, sh.smem, st>>>(
-            d_src, d_dst, lx, ly, t0, key, stream_id, tp, tq, sh.band, sh.mcs, d_counters, d_err);
-    }
-    return cudaGetLastError();
+    const int mode = dec_mode(tp, tq);
+    const bool useq = tq.always || tq.planes > 0;
+#define KPZB_FUSED_CASE(M)                                                                                    \
+    return useq ? launch_fused_c<M, true>(d_src, d_dst, lx, ly, t0, key, stream_id, tp, tq, sh, d_counters,   \
+                                          d_err, st)                                                          \
+                : launch_fused_c<M, false>(d_src, d_dst, lx, ly, t0, key, stream_id, tp, tq, sh, d_counters,  \
+                                           d_err, st)
+    if (mode == DEC_NONE) KPZB_FUSED_CASE(DEC_NONE);
+    if (mode == DEC_ONE) KPZB_FUSED_CASE(DEC_ONE);
+    KPZB_FUSED_CASE(DEC_GENERAL);
+#undef KPZB_FUSED_CASE
 }
 
 }  // namespace kpzb

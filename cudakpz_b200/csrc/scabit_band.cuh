@@ -85,9 +85,82 @@ struct BandGeom {
     Thresh tp, tq;
 };
 
+// One 4-word group (128 sites, one Philox group) of one half-step: the rule of
+// kpz/kpzSCABit.cu:179-290 with the masks of kpz/kpzSCABitCores.cu:69-74,139-145.
+// pTX/pTY: this sublattice's X/Y words of the row; pOX: the other sublattice's X words of the
+// row; pOY: the other sublattice's Y words of the next row; nbp: the first word of the next
+// group of the other X row (the one-bit carry of shifted rows).  MODE is a DecMode, or -1 to
+// decide with the runtime mode `mode_rt`; USEQ false when maxima never flip (q = 0), which
+// drops the maximum-candidate mask.  The carry crosses groups with shared-memory atomicXor on
+// disjoint bits (bit 0 of the next group's first word; bits 1..31 of this group's), so
+// neighbouring groups of a row may be updated concurrently.
+template <int MODE, bool USEQ, bool COUNT>
+__device__ __forceinline__ void sca_update_group(uint32_t* pTX, uint32_t* pTY, uint32_t* pOX,
+                                                 uint32_t* pOY, uint32_t* nbp, bool shifted,
+                                                 int mode_rt, const Thresh& tp, const Thresh& tq,
+                                                 Key key, uint32_t qgroup, uint32_t step,
+                                                 uint32_t stream, bool count_row,
+                                                 unsigned long long& ndep, unsigned long long& ndes)
+{
+    uint4* ptX = reinterpret_cast<uint4*>(pTX);
+    uint4* ptY = reinterpret_cast<uint4*>(pTY);
+    uint4* poX = reinterpret_cast<uint4*>(pOX);
+    uint4* poY = reinterpret_cast<uint4*>(pOY);
+    const uint4 tX = *ptX, tY = *ptY, oX = *poX, oY = *poY;
+    uint4 xX = oX;
+    if (shifted) {
+        const uint32_t nb = *nbp;
+        xX.x = __funnelshift_r(oX.x, oX.y, 1);
+        xX.y = __funnelshift_r(oX.y, oX.z, 1);
+        xX.z = __funnelshift_r(oX.z, oX.w, 1);
+        xX.w = __funnelshift_r(oX.w, nb, 1);
+    }
+    uint4 cp, cq = make_uint4(0, 0, 0, 0);
+    cp.x = ~(tX.x | tY.x) & xX.x & oY.x;
+    cp.y = ~(tX.y | tY.y) & xX.y & oY.y;
+    cp.z = ~(tX.z | tY.z) & xX.z & oY.z;
+    cp.w = ~(tX.w | tY.w) & xX.w & oY.w;
+    if (USEQ) {
+        cq.x = tX.x & tY.x & ~(xX.x | oY.x);
+        cq.y = tX.y & tY.y & ~(xX.y | oY.y);
+        cq.z = tX.z & tY.z & ~(xX.z | oY.z);
+        cq.w = tX.w & tY.w & ~(xX.w | oY.w);
+    }
+    uint4 m;
+    if (MODE == DEC_NONE) {
+        const uint32_t ap = tp.always ? 0xFFFFFFFFu : 0u;
+        if (USEQ) {
+            const uint32_t aq = tq.always ? 0xFFFFFFFFu : 0u;
+            m = make_uint4((cp.x & ap) | (cq.x & aq), (cp.y & ap) | (cq.y & aq), (cp.z & ap) | (cq.z & aq),
+                           (cp.w & ap) | (cq.w & aq));
+        } else {
+            m = make_uint4(cp.x & ap, cp.y & ap, cp.z & ap, cp.w & ap);
+        }
+    } else {
+        m = decide4_mode(MODE < 0 ? mode_rt : MODE, cp, cq, tp, tq, key, qgroup, step, stream);
+    }
+    if (COUNT && count_row) {
+        ndep += __popc(m.x & cp.x) + __popc(m.y & cp.y) + __popc(m.z & cp.z) + __popc(m.w & cp.w);
+        if (USEQ) ndes += __popc(m.x & cq.x) + __popc(m.y & cq.y) + __popc(m.z & cq.z) + __popc(m.w & cq.w);
+    }
+    *ptX = tX ^ m;
+    *ptY = tY ^ m;
+    *poY = oY ^ m;
+    if (shifted) {
+        atomicXor(pOX, m.x << 1);
+        pOX[1] = oX.y ^ __funnelshift_l(m.x, m.y, 1);
+        pOX[2] = oX.z ^ __funnelshift_l(m.y, m.z, 1);
+        pOX[3] = oX.w ^ __funnelshift_l(m.z, m.w, 1);
+        if (m.w >> 31) atomicXor(nbp, 1u);
+    } else {
+        *poX = oX ^ m;
+    }
+}
+
 // Runs one band; returns false (after flagging *err) when the TMA load did not complete in
-// time.  Must be called by all threads of the CTA; NT = blockDim.x.
-template <bool COUNT, int NT>
+// time.  Must be called by all threads of the CTA; NT = blockDim.x.  MODE / USEQ as for
+// sca_update_group (MODE -1 with USEQ true: rates known only at run time, as in a batch).
+template <int MODE, bool USEQ, bool COUNT, int NT>
 __device__ bool scabit_band(uint32_t* smem, const BandCtl& ctl, const BandGeom& g,
                             unsigned long long& ndep, unsigned long long& ndes,
                             unsigned int* err)
@@ -140,20 +213,21 @@ __device__ bool scabit_band(uint32_t* smem, const BandCtl& ctl, const BandGeom& 
 
     // Each thread owns one 4-word column group gi and walks rows with stride NT / G; all
     // shared-memory offsets are 32-bit (a band is at most 227 KB).
-    const int mode = dec_mode(g.tp, g.tq);
+    const int mode_rt = MODE < 0 ? dec_mode(g.tp, g.tq) : MODE;
     const uint32_t wr = (uint32_t)Wr;
     const int gi = (G >= NT) ? (int)threadIdx.x : (int)(threadIdx.x & (G - 1));
     const int rstride = (G >= NT) ? 1 : NT >> lgG;
     const int rofs = (G >= NT) ? 0 : (int)(threadIdx.x >> lgG);
     const uint32_t rmask = (uint32_t)rows - 1u;
     const int ylo32 = (int)(ylo & (int64_t)rmask);  // ylo mod rows
+    const uint32_t q32 = (uint32_t)qsz;
     for (int h = 0; h < 2 * g.k; ++h) {
         const int sigma = h & 1;
         const uint32_t step = 2u * (g.t0 + (uint32_t)(h >> 1)) + (uint32_t)sigma;
-        uint32_t* StX = smem + (sigma ? 2 : 0) * qsz;
-        uint32_t* StY = StX + qsz;
-        uint32_t* SoX = smem + (sigma ? 0 : 2) * qsz;
-        uint32_t* SoY = SoX + qsz;
+        uint32_t* StX = smem + (sigma ? 2u * q32 : 0u);
+        uint32_t* StY = StX + q32;
+        uint32_t* SoX = smem + (sigma ? 0u : 2u * q32);
+        uint32_t* SoY = SoX + q32;
         const int ra = g.resident ? 0 : h;
         const int rb = g.resident ? R : R - 1 - h;
         // wide rows (G > NT): a thread takes several column groups of a row in turn
@@ -162,51 +236,12 @@ __device__ bool scabit_band(uint32_t* smem, const BandCtl& ctl, const BandGeom& 
             const uint32_t wnext = (w0 + 4u) & (wr - 1u);
             for (int lr = ra + rofs; lr < rb; lr += rstride) {
                 const uint32_t gy = ((uint32_t)ylo32 + (uint32_t)lr) & rmask;  // periodic in y
-                const bool shifted = sigma != (int)(gy & 1u);
-                const uint32_t lr1 = g.resident ? (((uint32_t)lr + 1u) & rmask) : (uint32_t)lr + 1u;
                 const uint32_t ro = (uint32_t)lr * wr;
-                uint4* ptX = reinterpret_cast<uint4*>(StX + ro + w0);
-                uint4* ptY = reinterpret_cast<uint4*>(StY + ro + w0);
-                uint4* poX = reinterpret_cast<uint4*>(SoX + ro + w0);
-                uint4* poY = reinterpret_cast<uint4*>(SoY + lr1 * wr + w0);
-                const uint4 tX = *ptX, tY = *ptY, oX = *poX, oY = *poY;
-                uint32_t* nbp = SoX + ro + wnext;
-                uint4 xX = oX;
-                if (shifted) {
-                    const uint32_t nb = *nbp;
-                    xX.x = __funnelshift_r(oX.x, oX.y, 1);
-                    xX.y = __funnelshift_r(oX.y, oX.z, 1);
-                    xX.z = __funnelshift_r(oX.z, oX.w, 1);
-                    xX.w = __funnelshift_r(oX.w, nb, 1);
-                }
-                uint4 cp, cq;
-                cp.x = ~(tX.x | tY.x) & xX.x & oY.x;
-                cp.y = ~(tX.y | tY.y) & xX.y & oY.y;
-                cp.z = ~(tX.z | tY.z) & xX.z & oY.z;
-                cp.w = ~(tX.w | tY.w) & xX.w & oY.w;
-                cq.x = tX.x & tY.x & ~(xX.x | oY.x);
-                cq.y = tX.y & tY.y & ~(xX.y | oY.y);
-                cq.z = tX.z & tY.z & ~(xX.z | oY.z);
-                cq.w = tX.w & tY.w & ~(xX.w | oY.w);
-                const uint4 m = decide4_mode(mode, cp, cq, g.tp, g.tq, g.key,
-                                             (gy << (g.lx - 8)) + (uint32_t)gg, step, g.stream);
-                if (COUNT && lr >= H && lr < H + Bc) {
-                    ndep += __popc(m.x & cp.x) + __popc(m.y & cp.y) + __popc(m.z & cp.z) + __popc(m.w & cp.w);
-                    ndes += __popc(m.x & cq.x) + __popc(m.y & cq.y) + __popc(m.z & cq.z) + __popc(m.w & cq.w);
-                }
-                *ptX = tX ^ m;
-                *ptY = tY ^ m;
-                *poY = oY ^ m;
-                if (shifted) {
-                    uint32_t* ox = SoX + ro + w0;
-                    atomicXor(ox, m.x << 1);
-                    ox[1] = oX.y ^ __funnelshift_l(m.x, m.y, 1);
-                    ox[2] = oX.z ^ __funnelshift_l(m.y, m.z, 1);
-                    ox[3] = oX.w ^ __funnelshift_l(m.z, m.w, 1);
-                    if (m.w >> 31) atomicXor(nbp, 1u);
-                } else {
-                    *poX = oX ^ m;
-                }
+                const uint32_t ro1 = g.resident ? (((uint32_t)lr + 1u) & rmask) * wr : ro + wr;
+                sca_update_group<MODE, USEQ, COUNT>(StX + ro + w0, StY + ro + w0, SoX + ro + w0, SoY + ro1 + w0,
+                                                    SoX + ro + wnext, sigma != (int)(gy & 1u), mode_rt, g.tp,
+                                                    g.tq, g.key, (gy << lgG) + (uint32_t)gg, step, g.stream,
+                                                    lr >= H && lr < H + Bc, ndep, ndes);
             }
         }
         __syncthreads();

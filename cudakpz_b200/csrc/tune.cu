@@ -31,7 +31,7 @@ std::string plan_key(int lx, int ly, uint64_t Tp, uint64_t Tq, int sm_count)
     const int planes = a.planes > b.planes ? a.planes : b.planes;
     const int pclass = planes == 0 ? 0 : planes == 1 ? 1 : planes <= 4 ? 2 : 3;
     char buf[96];
-    snprintf(buf, sizeof buf, "scabit:%d:%d:rng%d:sm%d", lx, ly, pclass, sm_count);
+    snprintf(buf, sizeof buf, "scabit3:%d:%d:rng%d:sm%d", lx, ly, pclass, sm_count);
     return buf;
 }
 
@@ -44,9 +44,10 @@ void load_file()
     FILE* f = fopen(path, "r");
     if (!f) return;
     char key[96];
-    int k, cps;
+    int kind, k, cps;
     float ms;
-    while (fscanf(f, "%95s %d %d %f", key, &k, &cps, &ms) == 4) g_plans[key] = Plan{k, cps, ms, true};
+    while (fscanf(f, "%95s %d %d %d %f", key, &kind, &k, &cps, &ms) == 5)
+        g_plans[key] = Plan{k, cps, ms, true, kind};
     fclose(f);
 }
 
@@ -57,7 +58,8 @@ void save_file()
     FILE* f = fopen(path, "w");
     if (!f) return;
     for (const auto& kv : g_plans)
-        fprintf(f, "%s %d %d %.6f\n", kv.first.c_str(), kv.second.k, kv.second.cps, kv.second.ms_per_mcs);
+        fprintf(f, "%s %d %d %d %.6f\n", kv.first.c_str(), kv.second.kind, kv.second.k, kv.second.cps,
+                kv.second.ms_per_mcs);
     fclose(f);
 }
 }  // namespace
@@ -74,8 +76,27 @@ bool lookup_plan(int lx, int ly, uint64_t Tp, uint64_t Tq, int sm_count, Plan* o
 
 Plan default_plan(int lx, int ly)
 {
+    // the streaming kernel at 4 MCS per pass where it fits, else the band heuristic
+    if (scabit_stream_shape(lx, ly, 4, 148, 1).ok) return Plan{4, 1, 0.f, false, PASS_STREAM};
     const int k = auto_fusion(lx, ly);
-    return Plan{k, 0, 0.f, false};
+    return Plan{k, 0, 0.f, false, PASS_BAND};
+}
+
+Plan explicit_plan(int lx, int ly, int k, int sm_count)
+{
+    const char* env = getenv("KPZB_PASS_KERNEL");
+    const std::string v = env ? env : "";
+    if (k <= 1 || v == "band") return Plan{k, 0, 0.f, false, PASS_BAND};
+    const int cps = v == "stream2" ? 2 : 1;
+    if (scabit_stream_shape(lx, ly, k, sm_count, cps).ok) return Plan{k, cps, 0.f, false, PASS_STREAM};
+    return Plan{k, 0, 0.f, false, PASS_BAND};
+}
+
+bool plan_shape_ok(const Plan& p, int lx, int ly, int sm_count)
+{
+    if (p.k <= 1) return true;
+    if (p.kind == PASS_STREAM) return scabit_stream_shape(lx, ly, p.k, sm_count, p.cps ? p.cps : 1).ok;
+    return scabit_fused_shape_cps(lx, ly, p.k, p.cps, 0).ok;
 }
 
 cudaError_t tune_plan(uint32_t* d_src, int lx, int ly, uint64_t seed, uint32_t stream_id,
@@ -96,15 +117,16 @@ cudaError_t tune_plan(uint32_t* d_src, int lx, int ly, uint64_t seed, uint32_t s
     cudaEventCreate(&e1);
 
     struct Cand {
-        int k, cps;
+        int k, cps, kind;
     };
-    std::vector<Cand> cands{{1, 0}};
+    std::vector<Cand> cands{{1, 0, PASS_BAND}};
     for (int k = 2; k <= 8; ++k)
-        for (int cps = 1; cps <= 2; ++cps) {
+        for (int cps = 1; cps <= 3; ++cps) {
             FusedShape f = scabit_fused_shape_cps(lx, ly, k, cps, 0);
-            if (f.ok && f.band >= 2) cands.push_back({k, cps});
+            if (f.ok && f.band >= 2) cands.push_back({k, cps, PASS_BAND});
+            if (cps <= 2 && scabit_stream_shape(lx, ly, k, sm_count, cps).ok) cands.push_back({k, cps, PASS_STREAM});
         }
-    Plan best{1, 0, 1e30f, true};
+    Plan best{1, 0, 1e30f, true, PASS_BAND};
     const ScabitShape hs = scabit_shape(lx, ly, sm_count);
     for (const Cand& c : cands) {
         // enough MCS per measurement to dwarf launch overhead, capped by lattice size
@@ -120,10 +142,14 @@ cudaError_t tune_plan(uint32_t* d_src, int lx, int ly, uint64_t seed, uint32_t s
                 return cudaSuccess;
             }
             const FusedShape f = scabit_fused_shape_cps(lx, ly, c.k, c.cps, 0);
+            const StreamShape ss = scabit_stream_shape(lx, ly, c.k, sm_count, c.cps);
             uint32_t *s = a, *d = b;
             for (int m = 0; m + c.k <= mcs; m += c.k) {
-                cudaError_t r = scabit_fused(s, d, lx, ly, (uint32_t)m, seed, stream_id, Tp, Tq, f,
-                                             nullptr, d_err, st);
+                cudaError_t r = c.kind == PASS_STREAM
+                                    ? scabit_stream(s, d, lx, ly, (uint32_t)m, seed, stream_id, Tp, Tq, ss,
+                                                    nullptr, d_err, st)
+                                    : scabit_fused(s, d, lx, ly, (uint32_t)m, seed, stream_id, Tp, Tq, f,
+                                                   nullptr, d_err, st);
                 if (r != cudaSuccess) return r;
                 std::swap(s, d);
             }
@@ -139,9 +165,10 @@ cudaError_t tune_plan(uint32_t* d_src, int lx, int ly, uint64_t seed, uint32_t s
         cudaEventElapsedTime(&ms, e0, e1);
         const float per = ms / (float)mcs;
         if (getenv("KPZB_TUNE_VERBOSE"))
-            fprintf(stderr, "kpzb tune lx=%d ly=%d k=%d cps=%d: %.4f ms/MCS, %.1f upd/ns\n", lx, ly,
-                    c.k, c.cps, per, (double)(1ull << (lx + ly)) / (per * 1e6));
-        if (per < best.ms_per_mcs) best = Plan{c.k, c.cps, per, true};
+            fprintf(stderr, "kpzb tune lx=%d ly=%d %s k=%d cps=%d: %.4f ms/MCS, %.1f upd/ns\n", lx, ly,
+                    c.kind == PASS_STREAM ? "stream" : "band", c.k, c.cps, per,
+                    (double)(1ull << (lx + ly)) / (per * 1e6));
+        if (per < best.ms_per_mcs) best = Plan{c.k, c.cps, per, true, c.kind};
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);

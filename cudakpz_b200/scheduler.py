@@ -119,6 +119,42 @@ class Scheduler:
         check(lib.kpzb_get_fusion(self._h, C.byref(v)), "kpzb_get_fusion")
         return int(v.value)
 
+    def plan(self):
+        """(mcs_per_pass, ctas_per_sm, pass_kernel) used for the current rates; pass_kernel is
+        "half-steps", "band" or "stream" (kpzb_get_plan)."""
+        k, c, kind = C.c_int(), C.c_int(), C.c_int()
+        check(lib.kpzb_get_plan(self._h, C.byref(k), C.byref(c), C.byref(kind)), "kpzb_get_plan")
+        return int(k.value), int(c.value), ("half-steps", "band", "stream")[kind.value]
+
+    def saveBit(self, path: str, meta: Optional[str] = None) -> None:
+        """SchedulerService::saveBit's file (kpz/schedulerService.cpp:389-401) plus the resume
+        trailer (kpzb_save)."""
+        check(lib.kpzb_save(self._h, str(path).encode(), None if meta is None else meta.encode()), "kpzb_save")
+
+    def loadBit(self, path: str) -> None:
+        """Restore a kpzb_save checkpoint (lattice, MCS, seed, rates, correlator tag) or the
+        lattice of a plain saveBit file (kpzb_load)."""
+        check(lib.kpzb_load(self._h, str(path).encode()), "kpzb_load")
+        v = C.c_uint64()
+        check(lib.kpzb_get_mcs(self._h, C.byref(v)), "kpzb_get_mcs")
+        self._mcs = int(v.value)
+
+    def measureRun(self, end: int, sampling=None, corr_start: int = -1, corr_stop: int = 0):
+        """The frontend's measurement loop (kpz/kpzScaling.cpp:194-215) with the analysis on the
+        device: advance to `end`, measuring at every sample time of `sampling` (default: the
+        reference's exp sampling with density 0.1).  Returns an (n, 11) array of rows
+        {t, W^2, <h^1..7>, ch, cs} (kpzb_measure_run)."""
+        smp = sampling if sampling is not None else make_sampling()
+        n = C.c_int()
+        st = lib.kpzb_measure_run(self._h, C.byref(smp), end, corr_start, corr_stop, None, 0, C.byref(n))
+        if st != _lib.KPZB_OK and n.value == 0:
+            check(st, "kpzb_measure_run")
+        rows = np.zeros((max(n.value, 1), 11), dtype=np.float64)
+        check(lib.kpzb_measure_run(self._h, C.byref(smp), end, corr_start, corr_stop,
+                                   rows.ctypes.data_as(C.POINTER(C.c_double)), rows.shape[0], C.byref(n)),
+              "kpzb_measure_run")
+        return rows[: n.value]
+
     def autotune(self):
         """Measure the pass shapes for the current rates; returns (mcs_per_pass, ctas_per_sm,
         ms_per_mcs) of the fastest."""
@@ -351,3 +387,22 @@ def probe_alu_peak(device: int = -1):
     a, b = C.c_double(0.0), C.c_double(0.0)
     check(lib.kpzb_probe_alu_peak(device, C.byref(a), C.byref(b)), "kpzb_probe_alu_peak")
     return a.value, b.value
+
+
+def make_sampling(mode: str = "exp", density: float = 0.1, interval: int = 0, random_mean: float = 0.0,
+                  seed: int = 0):
+    """kpzb_sampling for SamplingParam's modes (kpz/sampling.h:66-100): "exp" (density),
+    "linear" (interval) or "random" (mean)."""
+    m = {"exp": _lib.SAMPLE_EXP, "linear": _lib.SAMPLE_LINEAR, "random": _lib.SAMPLE_RANDOM}[mode]
+    return _lib.Sampling(m, density, interval, random_mean, seed)
+
+
+def sample_times(start: int, end: int, sampling=None):
+    """Measurement times after `start` up to and including `end` (kpzb_sample_times)."""
+    smp = sampling if sampling is not None else make_sampling()
+    n = C.c_int()
+    check(lib.kpzb_sample_times(C.byref(smp), start, end, None, 0, C.byref(n)), "kpzb_sample_times")
+    out = np.zeros(max(n.value, 1), dtype=np.uint64)
+    check(lib.kpzb_sample_times(C.byref(smp), start, end, out.ctypes.data_as(C.POINTER(C.c_uint64)),
+                                out.size, C.byref(n)), "kpzb_sample_times")
+    return out[: n.value]

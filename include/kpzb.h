@@ -93,6 +93,12 @@ kpzb_status kpzb_set_fusion(kpzb_handle* h, int mcs_per_pass);
 /* The MCS per pass the handle uses for its current rates (resolving the automatic choice,
  * which may run the autotuner once). */
 kpzb_status kpzb_get_fusion(kpzb_handle* h, int* mcs_per_pass);
+/* The full pass plan for the current rates: MCS per pass, CTAs per SM and the pass kernel
+ * (KPZB_PASS_HALF_STEPS: one launch per half-step; KPZB_PASS_BAND: band kernel;
+ * KPZB_PASS_STREAM: streaming wavefront kernel).  No counterpart in the reference
+ * (introspection of the measured choice, e.g. for launch accounting). */
+enum { KPZB_PASS_HALF_STEPS = 0, KPZB_PASS_BAND = 1, KPZB_PASS_STREAM = 2 };
+kpzb_status kpzb_get_plan(kpzb_handle* h, int* mcs_per_pass, int* ctas_per_sm, int* pass_kernel);
 /* Time every pass shape (MCS per pass x CTAs per SM) on scratch copies of the current
  * lattice and cache the fastest for this size and rate class (in memory, and in the file
  * named by KPZB_TUNE_CACHE if set).  The lattice itself is not modified.  No reference
@@ -185,6 +191,52 @@ kpzb_status kpzb_batch_push(kpzb_batch* b, int i, const uint32_t* words);
 kpzb_status kpzb_batch_pop(kpzb_batch* b, int i, uint32_t* words);
 /* W^2 of every replica, out[n]. */
 kpzb_status kpzb_batch_roughness(kpzb_batch* b, double* w2);
+
+/* ---------------- checkpoint / resume ----------------
+ * kpzb_save writes SchedulerService::saveBit's file (kpz/schedulerService.cpp:389-401):
+ * "<lx>\n<ly>\n" + meta + '\0' + the lattice words in the handle's encoding, and appends a
+ * trailer that a saveBit reader never reaches: "KPZBCKPT", version, dynamics, lx, ly, device
+ * MCS, seed, stream id, p, q, fusion and, when a correlator tag is held, its ENC_CBBIT snapshot
+ * words and mean height.  With the counter-based stream that is the complete state, so a run
+ * resumed from the file continues bit for bit (the reference keeps its RNG state in HDF5,
+ * kpz/schedulerService.cpp:582-611, and its loadBit is an empty stub, :86-89).
+ * kpzb_load reads such a file into a handle of the same size; a plain saveBit file (no
+ * trailer) restores the lattice words only. */
+kpzb_status kpzb_save(kpzb_handle* h, const char* path, const char* meta);
+kpzb_status kpzb_load(kpzb_handle* h, const char* path);
+
+/* ---------------- measurement scheduling ----------------
+ * The reference's frontend loop (kpz/kpzScaling.cpp:194-215) advances the scheduler to the
+ * next measurement time of its sampling mode (SamplingParam::nextEval, kpz/sampling.h:84-100),
+ * pops the whole lattice to the host and analyses it there (SchedulerService::correlate,
+ * kpz/schedulerService.cpp:292-297).  kpzb_measure_run keeps that schedule but leaves the
+ * analysis on the device: the MCS chunks and the height reductions of every measurement are
+ * enqueued back to back on the handle's stream, with one copy of the result records at the end
+ * and no lattice transfer. */
+enum { KPZB_SAMPLE_EXP = 0, KPZB_SAMPLE_LINEAR = 1, KPZB_SAMPLE_RANDOM = 2 };
+typedef struct {
+    int mode;              /* KPZB_SAMPLE_* */
+    double density;        /* EXP: next = ceil(exp(log(t + 10) + density)); reference default 0.1 */
+    uint32_t interval;     /* LINEAR: next = t + interval (> 0) */
+    double random_mean;    /* RANDOM: next = t + (unsigned)(u * mean + mean), u uniform in [0, 1)
+                              from the counter stream keyed by `seed` (the reference draws u from
+                              the scheduler's dSFMT, SchedulerService::genrand_close_open); at
+                              least t + 1 */
+    uint64_t seed;         /* RANDOM only */
+} kpzb_sampling;
+/* The measurement times after `start` up to `end`, `end` included (the reference's EndEvent,
+ * kpz/kpzFrontend.cpp:744-752).  Writes at most `max` times; *n = the full count. */
+kpzb_status kpzb_sample_times(const kpzb_sampling* s, uint64_t start, uint64_t end, uint64_t* times,
+                              int max, int* n);
+/* Advance the handle from its device MCS to `end`, measuring at every sample time.  Row i of
+ * `rows` (11 doubles) = {t, W^2, <h^1>..<h^7>, ch, cs} as kpzb_roughness / kpzb_correlate give
+ * them.  Correlator tag (SchedulerService::correlateTag, kpz/schedulerService.h:151): when
+ * corr_start >= the current MCS, a snapshot is taken at t = corr_start (which is also a row)
+ * and rows with corr_start < t <= corr_stop carry ch and cs; elsewhere they are NaN
+ * (corr_start < 0: no tag).  *n_rows = number of rows; KPZB_EINVAL when max_rows is smaller
+ * (nothing is run).  Synchronous. */
+kpzb_status kpzb_measure_run(kpzb_handle* h, const kpzb_sampling* s, uint64_t end, int64_t corr_start,
+                             uint64_t corr_stop, double* rows, int max_rows, int* n_rows);
 
 /* ---------------- exact height autocorrelator ----------------
  * Snapshots of one lattice (ENC_CBBIT words) are turned into relative heights, shifted by

@@ -123,6 +123,66 @@ def patch(work: Path) -> None:
     (work / "stub_io.h").write_text(STUB)
 
 
+GPU_SOURCES = [
+    "kpz/schedulerGPU.cu", "kpz/schedulerBase.cu", "kpz/GPURandom.cu", "kpz/GPUTinyMT.cu",
+    "kpz/kpzSCABit.cu", "kpz/schedulerSCABit.cu", "kpz/correlatorCuda.cu", "inc/kmcExceptCUDA.cu",
+    "kpz/kpz.cu", "kpz/schedulerDT.cu", "kpz/scheduler.cu",
+]
+NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
+
+
+def patch_gpu(work: Path) -> None:
+    """Prepare the CUDA sources: drop the libSplash include (the schedulers' RNG-state HDF5
+    methods then only name the forward-declared splash::DataCollector), make TinyMT32's HDF5
+    bodies no-ops, and -- because the non-Fermi build defines only the default and "dis" DT
+    layouts, which are the same type (kpz/schedulerDT.h:45-46) -- instantiate SchedulerDT once
+    per RNG instead of the Fermi list (kpz/schedulerDTInstances.h:30-44)."""
+    for p in work.rglob("*.cu"):
+        t = p.read_text(errors="replace")
+        t2 = re.sub(r"#include\s*<KMCsplash\.h>", "", t)
+        if t2 != t:
+            p.write_text(t2)
+    tmt = work / "kpz/GPUTinyMT.cu"
+    t = tmt.read_text()
+    t = cut_between(t, "void TinyMT32::writeH5", None)
+    t += ("void TinyMT32::writeH5(splash::DataCollector*, int, const std::string&) {}\n"
+          "bool TinyMT32::readH5(splash::DataCollector*, int, const std::string&) { return false; }\n")
+    tmt.write_text(t)
+    di = work / "kpz/schedulerDTInstances.h"
+    t = di.read_text()
+    a = t.index("\ttemplate class SchedulerDT<SLCG64, SchedulerDT_LocalLayoutDefault>;")
+    b = t.index("}", a)
+    t = (t[:a] + "\ttemplate class SchedulerDT<SLCG64, SchedulerDT_LocalLayoutDis>;\n"
+         "\ttemplate class SchedulerDT<TinyMT32, SchedulerDT_LocalLayoutDis>;\n" + t[b:])
+    di.write_text(t)
+
+
+def build_gpu(cpu_objs: list[str]) -> None:
+    """The reference's GPU SchedulerSCABit<SLCG64> for sm_100a, as its own Makefile builds it
+    (kpz/Makefile: -O3 -maxrregcount=32 -DMODE_CUDA), linked with oracle/ref_gpu_driver.cu into
+    oracle/_ref/kpz_ref_gpu.  -DNDEBUG drops the host assert in SLCG64::randomize
+    (kpz/GPURandom.cu:44), whose bound (30721 streams, kpz/kpzConst.h:85) is below the
+    151552 streams the scheduler asks for on 148 SMs; no device code changes."""
+    if not Path(NVCC).exists():
+        print("nvcc not found; skipping the reference GPU build", file=sys.stderr)
+        return
+    patch_gpu(WORK)
+    flags = ["-O3", "-std=c++14", "-w", "-gencode", "arch=compute_100a,code=sm_100a", "-maxrregcount=32",
+             "-DMODE_CUDA", "-DNDEBUG", "-DDSFMT_MEXP=19937", "-DKPZ_SWITCH_RNG=SLCG64",
+             f"-I{WORK / 'kpz'}", f"-I{WORK / 'inc'}", "-include", str(WORK / "stub_io.h"), "-Xcompiler", "-pthread"]
+    objs = []
+    for src in GPU_SOURCES:
+        obj = WORK / (Path(src).stem + ".cu.o")
+        subprocess.run([NVCC, *flags, "-c", str(WORK / src), "-o", str(obj)], check=True)
+        objs.append(str(obj))
+    drv = WORK / "ref_gpu_driver.o"
+    subprocess.run([NVCC, *flags, "-c", str(HERE / "ref_gpu_driver.cu"), "-o", str(drv)], check=True)
+    cpu = [o for o in cpu_objs if not o.endswith("ref_driver.o")]
+    subprocess.run([NVCC, "-gencode", "arch=compute_100a,code=sm_100a", "-o", str(OUT / "kpz_ref_gpu"),
+                    str(drv), *objs, *cpu, "-Xcompiler", "-pthread", "-lcudart"], check=True)
+    print(f"built {OUT / 'kpz_ref_gpu'}")
+
+
 def main() -> int:
     if not REF.is_dir():
         print(f"{REF} not present; skipping the reference build", file=sys.stderr)
@@ -148,6 +208,7 @@ def main() -> int:
     subprocess.run(["g++", *flags, "-c", str(HERE / "ref_driver.cpp"), "-o", str(drv)], check=True)
     subprocess.run(["g++", "-pthread", "-o", str(OUT / "kpz_ref"), str(drv), *objs], check=True)
     print(f"built {OUT / 'kpz_ref'}")
+    build_gpu(objs)
     return 0
 
 

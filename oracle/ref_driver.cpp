@@ -15,6 +15,7 @@
 //   check ENC LX IN                 SchedulerService::consitencyCheck(); prints 1/0
 //   bench-cbbit LX P Q N THR        time mcsPQSyncRng(N) of SchedulerCPUCBBit; prints upd/ns
 //   bench-rs LX N                   time SchedulerCPU::mcs(N); prints upd/ns
+//   savebit LX SEED N FILE [META]   SchedulerService::saveBit of the RS lattice after N MCS
 #include <chrono>
 #include <cstdio>
 #include <cstdlib>
@@ -120,6 +121,22 @@ int main(int argc, char** argv)
         }
         save(argv[argc - 1], s.system(), s.size().sizeW());
         return 0;
+    }
+    if (cmd == "savebit") {
+        // SchedulerService::saveBit (kpz/schedulerService.cpp:389-401) of the RS lattice after N MCS
+        const int lx = std::atoi(argv[2]);
+        const int seed = std::atoi(argv[3]);
+        const int n = std::atoi(argv[4]);
+        quiet();
+        Kpz::SchedulerCPU s(lx, lx);
+        s.supplySeed(1, seed);
+        s.initHomogeneous(Kpz::SchedulerService::ENC_LOCAL);
+        s.pushSystem();
+        s.mcs(n);
+        s.popSystem();
+        const bool ok = s.saveBit(argv[5], argc > 6 ? argv[6] : nullptr);
+        loud();
+        return ok ? 0 : 1;
     }
     if (cmd == "cbbit" || cmd == "cb") {
         const int lx = std::atoi(argv[2]);

@@ -1,0 +1,78 @@
+// ref_gpu_driver.cu -- MEASUREMENT INFRASTRUCTURE (reference arm only, never the product).
+//
+// Times the reference's own GPU scheduler, SchedulerSCABit<SLCG64> (kpz/schedulerSCABit.cu,
+// kpz/kpzSCABit.cu, kpz/kpzSCABitCores.cu), compiled from the CudaKpz sources by
+// oracle/build_ref.py into oracle/_ref/kpz_ref_gpu, through its public SchedulerService calls
+// exactly as the reference's kpzScaling driver uses them (kpz/kpzScaling.cpp:142-215):
+// supplySeed, randomize, initHomogeneous, setPQ, mcsPQSyncRng, popSystem.
+//
+// and SchedulerDT<SLCG64, SchedulerDT_LocalLayoutDis> (kpz/schedulerDT.cu, kpz/kpz.cu, the
+// default DBSH inner decomposition of kpz/param.h) the same way.
+//
+// usage:
+//   kpz_ref_gpu scabit LX P Q WARMUP MCS   warm-up MCS, then MCS timed; prints
+//   kpz_ref_gpu dt LX P Q WARMUP MCS       "<attempted updates/ns> <seconds> <W2>"
+#include <chrono>
+#include <cstdio>
+#include <cstdlib>
+#include <iomanip>
+#include <iostream>
+#include <string>
+
+#include "GPURandom.h"
+#include "correlator.h"
+#include "schedulerDT.h"
+#include "schedulerSCABit.h"
+
+// HDF5/libSplash entry points of SchedulerService are not built (not on the hot path).
+bool Kpz::SchedulerService::collectH5(splash::DataCollector*, const std::string&) { return false; }
+bool Kpz::SchedulerService::retrieveH5(splash::DataCollector*, const std::string&) { return false; }
+
+static double now()
+{
+    return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+template <class Sched>
+static int run(int lx, double p, double q, int warm, int n, Kpz::SchedulerService::Encoding enc)
+{
+    std::streambuf* keep = std::cout.rdbuf();
+    std::cout.rdbuf(nullptr);  // the schedulers print set-up chatter on std::cout
+    Sched s(lx, lx, 0);
+    s.supplySeed(1, 1);
+    s.randomize();
+    s.initHomogeneous(enc);
+    s.pushSystem();
+    s.setPQ(p, q);
+    if (warm > 0) s.mcsPQSyncRng(warm);
+    const double t0 = now();
+    s.mcsPQSyncRng(n);  // returns after cudaThreadSynchronize (kpz/schedulerSCABit.cu:64, schedulerDT.cu:57)
+    const double t1 = now();
+    s.popSystem();
+    Kpz::Correlator::setNThreads(1);  // host roughness walk on one thread
+    const auto r = s.roughness();
+    std::cout.rdbuf(keep);
+    std::cout << std::setprecision(9) << (double)s.size().size() * n / ((t1 - t0) * 1e9) << ' ' << (t1 - t0)
+              << ' ' << (double)r.w2 << '\n';
+    return 0;
+}
+
+int main(int argc, char** argv)
+{
+    if (argc < 2) {
+        std::cerr << "usage: kpz_ref_gpu scabit LX P Q WARMUP MCS\n";
+        return 2;
+    }
+    const std::string cmd = argv[1];
+    if ((cmd == "scabit" || cmd == "dt") && argc >= 7) {
+        const int lx = std::atoi(argv[2]);
+        const double p = std::atof(argv[3]), q = std::atof(argv[4]);
+        const int warm = std::atoi(argv[5]), n = std::atoi(argv[6]);
+        if (cmd == "scabit")
+            return run<Kpz::SchedulerSCABit<SLCG64>>(lx, p, q, warm, n, Kpz::SchedulerService::ENC_CBBIT);
+        return run<Kpz::SchedulerDT<SLCG64, Kpz::SchedulerDT_LocalLayoutDis>>(lx, p, q, warm, n,
+                                                                           Kpz::SchedulerService::ENC_LOCAL);
+    }
+    std::cerr << "unknown command " << cmd << "\n";
+    return 2;
+}

@@ -95,6 +95,10 @@ def main():
                 an[key + "_check_valid"] = np.array(int(run("check", enc, lx, tmp / "a.bin")[0]))
                 an[key + "_check_broken"] = np.array(int(run("check", enc, lx, tmp / "c.bin")[0]))
     np.savez_compressed(HERE / "ref_analysis.npz", **an)
+
+    # 5. SchedulerService::saveBit file of the RS lattice (256^2, seed 1, 16 MCS): the lattice
+    #    file format the checkpoint entry points keep (kpz/schedulerService.cpp:389-401)
+    run("savebit", 8, 1, 16, HERE / "ref_savebit_rs256.bin", "CudaKpz saveBit fixture")
     print("golden vectors written to", HERE)
 
 

@@ -53,15 +53,42 @@ def test_scabit_wide_rows_segment_carry(kpzb, oracle, lx, ly):
     assert first_diff(got, ref) is None, first_diff(got, ref)
 
 
+# pass kernels selectable for an explicit fusion depth (KPZB_PASS_KERNEL): the streaming
+# wavefront kernel with one or two chunks per SM, and the band kernel
+KERNELS = ["stream", "stream2", "band"]
+
+
+@pytest.mark.parametrize("kernel", KERNELS)
 @pytest.mark.parametrize("fusion", [2, 3, 5])
 @pytest.mark.parametrize("lx,ly,p,q", [(9, 9, 0.5, 0.5), (10, 10, 1.0, 0.0), (8, 10, 0.9, 0.1),
                                        (11, 6, 0.5, 0.5)])
-def test_fused_bit_exact(kpzb, oracle, lx, ly, p, q, fusion):
+def test_fused_bit_exact(kpzb, oracle, monkeypatch, lx, ly, p, q, fusion, kernel):
+    monkeypatch.setenv("KPZB_PASS_KERNEL", kernel)
     n = 2 * fusion + 1  # whole fused passes plus a single-step remainder
     init = oracle.random_lattice(lx, ly, oracle.ENC_CBBIT, seed=11, mcs=2)
     ref = init.copy()
     oracle.sca_mcs(ref, lx, ly, oracle.ENC_CBBIT, 77, 0, 0, n, p, q)
     got = run_gpu(kpzb, lx, ly, "scaBit", p, q, 77, n, init=init, fusion=fusion)
+    assert first_diff(got, ref) is None, first_diff(got, ref)
+
+
+@pytest.mark.parametrize("kernel", ["stream", "stream2"])
+@pytest.mark.parametrize("lx,ly,k,p,q", [
+    (8, 8, 2, 0.5, 0.5),    # one 4-word group per row
+    (8, 6, 3, 0.75, 0.25),  # fewer rows than chunks: one row per chunk
+    (10, 4, 2, 1.0, 0.0),   # 16 rows: each chunk's halo wraps the lattice
+    (12, 2, 8, 0.5, 0.5),   # 4 rows, deepest pass: rows loaded many times over
+    (13, 3, 6, 0.3, 0.7),   # wide rows, generic rates
+    (9, 11, 8, 1.0, 1.0),   # every candidate flips
+])
+def test_stream_kernel_edges(kpzb, oracle, monkeypatch, lx, ly, k, p, q, kernel):
+    """The streaming pass kernel at chunk, halo and ring corner cases, word for word."""
+    monkeypatch.setenv("KPZB_PASS_KERNEL", kernel)
+    n = 2 * k
+    init = oracle.random_lattice(lx, ly, oracle.ENC_CBBIT, seed=13, mcs=3)
+    ref = init.copy()
+    oracle.sca_mcs(ref, lx, ly, oracle.ENC_CBBIT, 5, 0, 0, n, p, q)
+    got = run_gpu(kpzb, lx, ly, "scaBit", p, q, 5, n, init=init, fusion=k)
     assert first_diff(got, ref) is None, first_diff(got, ref)
 
 
@@ -121,8 +148,10 @@ def test_counters_height_balance(kpzb, oracle):
     assert (dep, des) == (rdep, rdes)
 
 
+@pytest.mark.parametrize("kernel", KERNELS)
 @pytest.mark.parametrize("fusion", [1, 4])
-def test_counters_fused(kpzb, oracle, fusion):
+def test_counters_fused(kpzb, oracle, monkeypatch, fusion, kernel):
+    monkeypatch.setenv("KPZB_PASS_KERNEL", kernel)
     lx, ly = 10, 9
     s = kpzb.Scheduler(lx, ly)
     s.setPQ(0.6, 0.4)
@@ -134,12 +163,14 @@ def test_counters_fused(kpzb, oracle, fusion):
     assert s.counters() == oracle.sca_mcs(ref, lx, ly, oracle.ENC_CBBIT, 8, 0, 0, 8, 0.6, 0.4)
 
 
-def test_full_size_16384_properties(kpzb, oracle):
+@pytest.mark.parametrize("kernel", ["stream", "band"])
+def test_full_size_16384_properties(kpzb, oracle, monkeypatch, kernel):
     """16384^2 (C2 size): fused == unfused bit for bit, invariants hold, height balance."""
+    monkeypatch.setenv("KPZB_PASS_KERNEL", kernel)
     lx = ly = 14
     N = 1 << 28
     res = {}
-    for fusion in (1, 0):
+    for fusion in (1, 0, 4, 6):
         s = kpzb.Scheduler(lx, ly)
         s.setPQ(0.5, 0.5)
         s.supplySeed(42)
@@ -155,7 +186,8 @@ def test_full_size_16384_properties(kpzb, oracle):
         assert (s1b - s1a - 2 * (dep - des)) % (2 * N) == 0
         res[fusion] = s.popSystem()
         s.close()
-    assert first_diff(res[1], res[0]) is None
+    for f in (0, 4, 6):
+        assert first_diff(res[1], res[f]) is None, (f, first_diff(res[1], res[f]))
 
 
 def test_full_size_first_mcs_vs_oracle(kpzb, oracle):

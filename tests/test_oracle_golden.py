@@ -91,3 +91,27 @@ def test_consistency_check_matches_reference(oracle, lx):
     assert (oracle.check_invariants(w, lx, lx, 0) == [0, 0, 0]) == bool(z[k + "_check_valid"])
     w[3] ^= 1 << 4
     assert (oracle.check_invariants(w, lx, lx, 0) == [0, 0, 0]) == bool(z[k + "_check_broken"])
+
+
+def read_savebit(path):
+    """Parse SchedulerService::saveBit's layout (kpz/schedulerService.cpp:389-401):
+    "<lx>\\n<ly>\\n" + meta + '\\0' + the lattice words; returns (lx, ly, meta, words, rest)."""
+    b = Path(path).read_bytes()
+    nl1 = b.index(b"\n")
+    nl2 = b.index(b"\n", nl1 + 1)
+    lx, ly = int(b[:nl1]), int(b[nl1 + 1:nl2])
+    z = b.index(b"\0", nl2 + 1)
+    meta = b[nl2 + 1:z].decode()
+    nw = 1 << (lx + ly - 4)
+    words = np.frombuffer(b[z + 1:z + 1 + 4 * nw], dtype=np.uint32)
+    return lx, ly, meta, words, b[z + 1 + 4 * nw:]
+
+
+def test_savebit_fixture_is_the_rs_lattice(oracle):
+    """The reference's saveBit file of the RS run (256^2, seed 1, 16 MCS) holds exactly the
+    oracle's lattice after the same 16 MCS."""
+    lx, ly, meta, words, rest = read_savebit(G / "ref_savebit_rs256.bin")
+    assert (lx, ly, meta, rest) == (8, 8, "CudaKpz saveBit fixture", b"")
+    w = oracle.homogeneous(8, 8, oracle.ENC_LOCAL)
+    oracle.rs_mcs(w, 8, 8, oracle.DSFMT(1), 16)
+    assert np.array_equal(words, w)

@@ -58,6 +58,11 @@ struct kpzb_handle {
     int fusion = 0;
     bool count = false;
     unsigned long long* d_counters = nullptr;
+    // quenched disorder: rate-class words (ENC_LOCAL for DT, ENC_CBBIT form for SCA/SCABit)
+    // and the rates of classes 0..3 (class 0 = p, q)
+    uint32_t* d_dis = nullptr;
+    double pc[4] = {1.0, 1.0, 1.0, 1.0}, qc[4] = {0.0, 0.0, 0.0, 0.0};
+    bool class_set[4] = {true, false, false, false};
     AnalysisScratch an{};
     ScabitShape shape{};
     DtState dt{};
@@ -146,6 +151,7 @@ extern "C" kpzb_status kpzb_destroy(kpzb_handle* h)
     cudaFree(h->d_tmp);
     cudaFree(h->d_snap);
     cudaFree(h->d_counters);
+    cudaFree(h->d_dis);
     if (h->an.rowinfo) analysis_free(&h->an);
     dt_free(&h->dt);
     if (h->own_st) cudaStreamDestroy(h->own_st);
@@ -168,6 +174,42 @@ extern "C" kpzb_status kpzb_set_pq(kpzb_handle* h, double p, double q)
     if (!(p >= 0.0 && p <= 1.0 && q >= 0.0 && q <= 1.0)) return fail(KPZB_EINVAL, "p, q must lie in [0,1]");
     h->p = p;
     h->q = q;
+    for (int c = 0; c < 4; ++c)
+        if (c == 0 || !h->class_set[c]) {
+            h->pc[c] = p;
+            h->qc[c] = q;
+        }
+    return KPZB_OK;
+}
+
+extern "C" kpzb_status kpzb_set_pq_class(kpzb_handle* h, int n, double p, double q)
+{
+    if (!h) return fail(KPZB_EINVAL, "null handle");
+    if (n < 0 || n > 3) return fail(KPZB_EINVAL, "rate class must be 0..3");
+    if (n == 0) return kpzb_set_pq(h, p, q);
+    if (!(p >= 0.0 && p <= 1.0 && q >= 0.0 && q <= 1.0)) return fail(KPZB_EINVAL, "p, q must lie in [0,1]");
+    h->pc[n] = p;
+    h->qc[n] = q;
+    h->class_set[n] = true;
+    return KPZB_OK;
+}
+
+extern "C" kpzb_status kpzb_set_disorder(kpzb_handle* h, const uint32_t* local_words)
+{
+    KPZB_CHECK_H(h);
+    if (!local_words) return fail(KPZB_EINVAL, "null disorder words");
+    if (!h->d_dis) KPZB_CU(cudaMalloc(&h->d_dis, h->words() * 4), "cudaMalloc(disorder)");
+    if (h->dyn == KPZB_DYN_DT) {
+        KPZB_CU(cudaMemcpyAsync(h->d_dis, local_words, h->words() * 4, cudaMemcpyHostToDevice, h->st),
+                "disorder copy");
+    } else {
+        kpzb_status s = ensure_tmp(h);
+        if (s != KPZB_OK) return s;
+        KPZB_CU(cudaMemcpyAsync(h->d_tmp, local_words, h->words() * 4, cudaMemcpyHostToDevice, h->st),
+                "disorder copy");
+        KPZB_CU(local_to_cbbit_dev(h->d_tmp, h->d_dis, h->lx, h->ly, h->st), "disorder transcode");
+    }
+    KPZB_CU(cudaStreamSynchronize(h->st), "disorder sync");
     return KPZB_OK;
 }
 
@@ -330,6 +372,44 @@ extern "C" kpzb_status kpzb_mcs_async(kpzb_handle* h, int n)
     if (s != KPZB_OK) return s;
     h->tdev += (uint64_t)n;
     return KPZB_OK;
+}
+
+static uint64_t thresh_of(double p);
+
+extern "C" kpzb_status kpzb_mcs_disorder_async(kpzb_handle* h, int n)
+{
+    KPZB_CHECK_H(h);
+    if (n < 0) return fail(KPZB_EINVAL, "negative MCS count");
+    if (!h->d_dis) return fail(KPZB_ESTATE, "no disorder set (kpzb_set_disorder)");
+    if (h->tdev + (uint64_t)n >= (1ull << 31)) return fail(KPZB_EINVAL, "device MCS counter limit 2^31");
+    uint64_t Tp[4], Tq[4];
+    for (int c = 0; c < 4; ++c) {
+        Tp[c] = thresh_of(h->pc[c]);
+        Tq[c] = thresh_of(h->qc[c]);
+    }
+    unsigned long long* cnt = h->count ? h->d_counters : nullptr;
+    if (h->dyn == KPZB_DYN_DT) {
+        kpzb_status s = dt_enqueue(&h->dt, h->d_sys, h->lx, h->ly, h->tdev, n, h->p, h->q, h->seed, h->stream_id,
+                                   h->st, cnt, h->d_dis, Tp, Tq);
+        if (s != KPZB_OK) return s;
+    } else {
+        for (int i = 0; i < n; ++i) {
+            const uint64_t t = h->tdev + (uint64_t)i;
+            for (int sg = 0; sg < 2; ++sg)
+                KPZB_CU(scabit_half_dis(h->d_sys, h->d_dis, h->lx, h->ly, sg, (uint32_t)(2 * t + sg), h->seed,
+                                        h->stream_id, Tp, Tq, h->shape, cnt, h->st),
+                        "scabit_half_dis");
+        }
+    }
+    h->tdev += (uint64_t)n;
+    return KPZB_OK;
+}
+
+extern "C" kpzb_status kpzb_mcs_disorder(kpzb_handle* h, int n)
+{
+    kpzb_status s = kpzb_mcs_disorder_async(h, n);
+    if (s != KPZB_OK) return s;
+    return kpzb_join(h);
 }
 
 extern "C" kpzb_status kpzb_join(kpzb_handle* h)

@@ -31,16 +31,21 @@ constexpr int DT_BX = 4 * DT_BXW, DT_BY = 4 * DT_BYW;  // block in sites
 constexpr int DT_TW = DT_BXW + 1, DT_TH = DT_BYW + 1;  // shared tile with halo
 constexpr int DT_ROUNDS = 64;
 
-template <bool COUNT>
+// DIS: quenched disorder (Disorder2SyncRng_shared, kpz/kpzSimulationPrimitivesTemplates.cu:
+// 295-382): dis holds every site's 2-bit rate class in ENC_LOCAL words, copied into a second
+// shared tile beside the lattice's; the class picks dr.tp[c] / dr.tq[c].
+template <bool COUNT, bool DIS>
 __global__ void __launch_bounds__(DT_TX* DT_TY)
 dt_kernel(uint32_t* __restrict__ sys, int lxw, int lyw, int lnbx, int nblocks, int ox, int oy,
           int d, uint32_t t, Key key, uint32_t stream, Thresh tp, Thresh tq,
-          unsigned long long* __restrict__ counters)
+          unsigned long long* __restrict__ counters, const uint32_t* __restrict__ dis, DisorderRates dr)
 {
     __shared__ uint32_t tile[DT_TH * DT_TW];
+    __shared__ uint32_t dtile[DIS ? DT_TH * DT_TW : 1];
     const int tid = threadIdx.y * DT_TX + threadIdx.x;
     const uint32_t Wx = 1u << lxw, Wy = 1u << lyw;
-    const bool need_u = !(tp.always || tp.planes == 0) || !(tq.always || tq.planes == 0);
+    bool need_u = !(tp.always || tp.planes == 0) || !(tq.always || tq.planes == 0);
+    if (DIS) need_u = dr.planes > 0;
     unsigned long long ndep = 0, ndes = 0;
 
     for (int b = blockIdx.x; b < nblocks; b += gridDim.x) {
@@ -50,7 +55,9 @@ dt_kernel(uint32_t* __restrict__ sys, int lxw, int lyw, int lnbx, int nblocks, i
         const uint32_t wx0 = X0 >> 2, wy0 = Y0 >> 2;
         for (int i = tid; i < DT_TH * DT_TW; i += DT_TX * DT_TY) {
             const uint32_t r = i / DT_TW, c = i - r * DT_TW;
-            tile[i] = sys[(size_t)((wy0 + r) & (Wy - 1)) * Wx + ((wx0 + c) & (Wx - 1))];
+            const size_t gi = (size_t)((wy0 + r) & (Wy - 1)) * Wx + ((wx0 + c) & (Wx - 1));
+            tile[i] = sys[gi];
+            if (DIS) dtile[i] = dis[gi];
         }
         // block-wide sub-cell sequence: 2 bits per round (every thread derives the same words)
         const uint4 sub = philox4x32_10(
@@ -88,7 +95,9 @@ dt_kernel(uint32_t* __restrict__ sys, int lxw, int lyw, int lnbx, int nblocks, i
                                (int)(((tile[wd] >> (shd | 1)) & 1u) << 3);
             bool flip = false;
             if (config == 12 || config == 3) {
-                const Thresh& th = config == 12 ? tp : tq;
+                int cls = 0;
+                if (DIS) cls = (int)((dtile[wi] >> sh) & 3u);
+                const Thresh& th = DIS ? (config == 12 ? dr.tp[cls] : dr.tq[cls]) : (config == 12 ? tp : tq);
                 if (th.always) flip = true;
                 else if (th.planes) {
                     const uint32_t u = (r & 3) == 0 ? uu.x : (r & 3) == 1 ? uu.y : (r & 3) == 2 ? uu.z : uu.w;
@@ -189,7 +198,8 @@ static uint64_t thresh_dt(double p)
 
 kpzb_status dt_enqueue(DtState* s, uint32_t* d_local, int lx, int ly, uint64_t t0, int n, double p,
                        double q, uint64_t seed, uint32_t stream, cudaStream_t st,
-                       unsigned long long* d_counters)
+                       unsigned long long* d_counters, const uint32_t* dis, const uint64_t* dis_Tp,
+                       const uint64_t* dis_Tq)
 {
     if (!s->ready) return fail(KPZB_ESTATE, "DT state not initialised");
     const Key key = make_key(seed);
@@ -197,17 +207,30 @@ kpzb_status dt_enqueue(DtState* s, uint32_t* d_local, int lx, int ly, uint64_t t
     const int lnbx = lx - 9;
     const int nblocks = (1 << lnbx) * (1 << (ly - 8));
     const dim3 block(DT_TX, DT_TY);
+    const DisorderRates dr = dis ? make_disorder_rates(dis_Tp, dis_Tq) : DisorderRates{};
     for (int i = 0; i < n; ++i) {
         const uint32_t t = (uint32_t)(t0 + (uint64_t)i);
         int ox, oy, order[4];
         dt_plan(seed, stream, t, &ox, &oy, order);
         for (int a = 0; a < 4; ++a) {
-            if (d_counters)
-                dt_kernel<true><<<s->grid, block, 0, st>>>(d_local, lx - 2, ly - 2, lnbx, nblocks, ox, oy,
-                                                           order[a], t, key, stream, tp, tq, d_counters);
-            else
-                dt_kernel<false><<<s->grid, block, 0, st>>>(d_local, lx - 2, ly - 2, lnbx, nblocks, ox, oy,
-                                                            order[a], t, key, stream, tp, tq, nullptr);
+            if (dis) {
+                if (d_counters)
+                    dt_kernel<true, true><<<s->grid, block, 0, st>>>(d_local, lx - 2, ly - 2, lnbx, nblocks, ox,
+                                                                     oy, order[a], t, key, stream, tp, tq,
+                                                                     d_counters, dis, dr);
+                else
+                    dt_kernel<false, true><<<s->grid, block, 0, st>>>(d_local, lx - 2, ly - 2, lnbx, nblocks,
+                                                                      ox, oy, order[a], t, key, stream, tp, tq,
+                                                                      nullptr, dis, dr);
+            } else if (d_counters) {
+                dt_kernel<true, false><<<s->grid, block, 0, st>>>(d_local, lx - 2, ly - 2, lnbx, nblocks, ox,
+                                                                  oy, order[a], t, key, stream, tp, tq,
+                                                                  d_counters, nullptr, dr);
+            } else {
+                dt_kernel<false, false><<<s->grid, block, 0, st>>>(d_local, lx - 2, ly - 2, lnbx, nblocks, ox,
+                                                                   oy, order[a], t, key, stream, tp, tq, nullptr,
+                                                                   nullptr, dr);
+            }
         }
         const cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess) return cuda_fail(e, "dt_kernel");

@@ -46,8 +46,10 @@ struct DtState {
 };
 kpzb_status dt_init(DtState* s, int lx, int ly, int sm_count);
 void dt_free(DtState* s);
+// dis (optional): ENC_LOCAL rate-class words; dis_Tp / dis_Tq: the four classes' thresholds
 kpzb_status dt_enqueue(DtState* s, uint32_t* d_local, int lx, int ly, uint64_t t0, int n,
                        double p, double q, uint64_t seed, uint32_t stream, cudaStream_t st,
-                       unsigned long long* d_counters);
+                       unsigned long long* d_counters, const uint32_t* dis = nullptr,
+                       const uint64_t* dis_Tp = nullptr, const uint64_t* dis_Tq = nullptr);
 
 }  // namespace kpzb

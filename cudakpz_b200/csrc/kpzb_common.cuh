@@ -157,6 +157,79 @@ __device__ __forceinline__ uint4 decide4_mode(int mode, uint4 cp, uint4 cq, Thre
     return decide4(cp, cq, tp, tq, key, qgroup, step, stream);
 }
 
+// Quenched disorder (mcsDisorder2SyncRng): every site carries a 2-bit rate class c (bit 0 in
+// d0, bit 1 in d1) that picks thresholds tp[c] / tq[c]; the comparison u < T(site) runs on the
+// same random planes as decide4, so equal rates in every class give decide4's result.
+struct DisorderRates {
+    Thresh tp[4], tq[4];
+    int planes;  // most planes any of the eight thresholds can need
+};
+
+inline DisorderRates make_disorder_rates(const uint64_t Tp[4], const uint64_t Tq[4])
+{
+    DisorderRates dr{};
+    dr.planes = 0;
+    for (int c = 0; c < 4; ++c) {
+        dr.tp[c] = make_thresh(Tp[c]);
+        dr.tq[c] = make_thresh(Tq[c]);
+        if (dr.tp[c].planes > dr.planes) dr.planes = dr.tp[c].planes;
+        if (dr.tq[c].planes > dr.planes) dr.planes = dr.tq[c].planes;
+    }
+    return dr;
+}
+
+__device__ __forceinline__ uint32_t sel_class(uint32_t d0, uint32_t d1, uint32_t b0, uint32_t b1, uint32_t b2,
+                                              uint32_t b3)
+{
+    return (~d1 & ((~d0 & b0) | (d0 & b1))) | (d1 & ((~d0 & b2) | (d0 & b3)));
+}
+
+__device__ __forceinline__ uint32_t dis_word(uint32_t cp, uint32_t cq, uint32_t d0, uint32_t d1,
+                                             const uint32_t bp[4], const uint32_t bq[4])
+{
+    return (cp & sel_class(d0, d1, bp[0], bp[1], bp[2], bp[3])) |
+           (cq & sel_class(d0, d1, bq[0], bq[1], bq[2], bq[3]));
+}
+
+__device__ __forceinline__ uint4 decide4_dis(uint4 cp, uint4 cq, uint4 d0, uint4 d1, const DisorderRates& dr,
+                                             Key key, uint32_t qgroup, uint32_t step, uint32_t stream)
+{
+    uint32_t ap[4], aq[4], hp[4], hq[4];
+    for (int c = 0; c < 4; ++c) {
+        ap[c] = dr.tp[c].always ? 0xFFFFFFFFu : 0u;
+        aq[c] = dr.tq[c].always ? 0xFFFFFFFFu : 0u;
+        hp[c] = dr.tp[c].planes ? 0xFFFFFFFFu : 0u;
+        hq[c] = dr.tq[c].planes ? 0xFFFFFFFFu : 0u;
+    }
+    // decided flips (threshold 2^32) and sites still equal to their threshold's prefix
+    uint4 lt = make_uint4(dis_word(cp.x, cq.x, d0.x, d1.x, ap, aq), dis_word(cp.y, cq.y, d0.y, d1.y, ap, aq),
+                          dis_word(cp.z, cq.z, d0.z, d1.z, ap, aq), dis_word(cp.w, cq.w, d0.w, d1.w, ap, aq));
+    uint4 eq = make_uint4(dis_word(cp.x, cq.x, d0.x, d1.x, hp, hq), dis_word(cp.y, cq.y, d0.y, d1.y, hp, hq),
+                          dis_word(cp.z, cq.z, d0.z, d1.z, hp, hq), dis_word(cp.w, cq.w, d0.w, d1.w, hp, hq));
+    for (int k = 0; k < dr.planes; ++k) {
+        if (!(eq.x | eq.y | eq.z | eq.w)) break;
+        const uint4 r = philox4x32_10(make_uint4(qgroup, step, (uint32_t)k | (TAG_SCA << 8), stream), key);
+        uint32_t bp[4], bq[4], ep[4], eqn[4];
+        for (int c = 0; c < 4; ++c) {
+            bp[c] = ((dr.tp[c].t >> (31 - k)) & 1u) ? 0xFFFFFFFFu : 0u;
+            bq[c] = ((dr.tq[c].t >> (31 - k)) & 1u) ? 0xFFFFFFFFu : 0u;
+            // thresholds with no 1 bit left below this plane can no longer be exceeded from below
+            ep[c] = (k + 1 >= dr.tp[c].planes) ? 0xFFFFFFFFu : 0u;
+            eqn[c] = (k + 1 >= dr.tq[c].planes) ? 0xFFFFFFFFu : 0u;
+        }
+#define KPZB_DIS_PLANE(F)                                                   \
+    {                                                                       \
+        const uint32_t tb = dis_word(cp.F, cq.F, d0.F, d1.F, bp, bq);       \
+        lt.F |= eq.F & tb & ~r.F;                                           \
+        eq.F &= ~(tb ^ r.F);                                                \
+        eq.F &= ~dis_word(cp.F, cq.F, d0.F, d1.F, ep, eqn);                 \
+    }
+        KPZB_DIS_PLANE(x) KPZB_DIS_PLANE(y) KPZB_DIS_PLANE(z) KPZB_DIS_PLANE(w)
+#undef KPZB_DIS_PLANE
+    }
+    return lt;
+}
+
 __device__ __forceinline__ uint4 operator^(uint4 a, uint4 b)
 {
     return make_uint4(a.x ^ b.x, a.y ^ b.y, a.z ^ b.z, a.w ^ b.w);

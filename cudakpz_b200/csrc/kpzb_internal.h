@@ -14,6 +14,13 @@ cudaError_t scabit_half(uint32_t* d_sys, int lx, int ly, int sigma, uint32_t ste
                         uint32_t stream_id, uint64_t Tp, uint64_t Tq, const ScabitShape& sh,
                         unsigned long long* d_counters, cudaStream_t st);
 
+// Quenched disorder: one half-step with per-site rate classes (d_dis_cbbit: the class words in
+// ENC_CBBIT form), thresholds Tp[c], Tq[c] for classes c = 0..3.
+cudaError_t scabit_half_dis(uint32_t* d_sys, const uint32_t* d_dis_cbbit, int lx, int ly, int sigma,
+                            uint32_t step, uint64_t seed, uint32_t stream_id, const uint64_t Tp[4],
+                            const uint64_t Tq[4], const ScabitShape& sh, unsigned long long* d_counters,
+                            cudaStream_t st);
+
 // Temporal-blocked SCABit: k MCS (2k half-steps) per HBM pass over a band of rows.
 struct FusedShape {
     int band;      // output rows per CTA band

@@ -24,11 +24,16 @@ namespace kpzb {
 
 constexpr int SCABIT_THREADS = 256;
 
-template <bool COUNT>
+// DIS: quenched disorder -- dis holds every site's 2-bit rate class in ENC_CBBIT form (class
+// bit 0 in the X quadrants, bit 1 in the Y quadrants, i.e. the ENC_LOCAL class words put
+// through the lattice codec), dr the four classes' thresholds (Disorder2SyncRng,
+// kpz/kpzSCACores.cu:217-280).
+template <bool COUNT, bool DIS>
 __global__ void __launch_bounds__(SCABIT_THREADS)
 scabit_half_kernel(uint32_t* __restrict__ sys, int lx, int ly, int sigma, uint32_t step, Key key,
                    uint32_t stream, Thresh tp, Thresh tq, int TX, int TY,
-                   unsigned long long* __restrict__ counters)
+                   unsigned long long* __restrict__ counters, const uint32_t* __restrict__ dis,
+                   DisorderRates dr)
 {
     __shared__ uint32_t nxt_s[SCABIT_THREADS];
     __shared__ uint32_t carry_s[2][SCABIT_THREADS];
@@ -83,8 +88,15 @@ scabit_half_kernel(uint32_t* __restrict__ sys, int lx, int ly, int sigma, uint32
             cq.y = tX.y & tY.y & ~(xX.y | oY.y);
             cq.z = tX.z & tY.z & ~(xX.z | oY.z);
             cq.w = tX.w & tY.w & ~(xX.w | oY.w);
-            const uint4 m = decide4_mode(dec_mode(tp, tq), cp, cq, tp, tq, key,
-                                         (uint32_t)((roff + wi) >> 2), step, stream);
+            uint4 m;
+            if (DIS) {
+                const uint4 d0 = *reinterpret_cast<const uint4*>(dis + bthisX + roff + wi);
+                const uint4 d1 = *reinterpret_cast<const uint4*>(dis + bthisY + roff + wi);
+                m = decide4_dis(cp, cq, d0, d1, dr, key, (uint32_t)((roff + wi) >> 2), step, stream);
+            } else {
+                m = decide4_mode(dec_mode(tp, tq), cp, cq, tp, tq, key, (uint32_t)((roff + wi) >> 2), step,
+                                 stream);
+            }
             if (COUNT) {
                 ndep += __popc(m.x & cp.x) + __popc(m.y & cp.y) + __popc(m.z & cp.z) + __popc(m.w & cp.w);
                 ndes += __popc(m.x & cq.x) + __popc(m.y & cq.y) + __popc(m.z & cq.z) + __popc(m.w & cq.w);
@@ -152,14 +164,32 @@ cudaError_t scabit_half(uint32_t* d_sys, int lx, int ly, int sigma, uint32_t ste
     const Key key = make_key(seed);
     const Thresh tp = make_thresh(Tp), tq = make_thresh(Tq);
     dim3 block(sh.TX, sh.TY);
+    const DisorderRates dr{};
     if (d_counters)
-        scabit_half_kernel<true><<<sh.grid, block, 0, st>>>(d_sys, lx, ly, sigma, step, key,
-                                                            stream_id, tp, tq, sh.TX, sh.TY,
-                                                            d_counters);
+        scabit_half_kernel<true, false><<<sh.grid, block, 0, st>>>(d_sys, lx, ly, sigma, step, key, stream_id,
+                                                                   tp, tq, sh.TX, sh.TY, d_counters, nullptr, dr);
     else
-        scabit_half_kernel<false><<<sh.grid, block, 0, st>>>(d_sys, lx, ly, sigma, step, key,
-                                                             stream_id, tp, tq, sh.TX, sh.TY,
-                                                             nullptr);
+        scabit_half_kernel<false, false><<<sh.grid, block, 0, st>>>(d_sys, lx, ly, sigma, step, key, stream_id,
+                                                                    tp, tq, sh.TX, sh.TY, nullptr, nullptr, dr);
+    return cudaGetLastError();
+}
+
+cudaError_t scabit_half_dis(uint32_t* d_sys, const uint32_t* d_dis_cbbit, int lx, int ly, int sigma,
+                            uint32_t step, uint64_t seed, uint32_t stream_id, const uint64_t Tp[4],
+                            const uint64_t Tq[4], const ScabitShape& sh, unsigned long long* d_counters,
+                            cudaStream_t st)
+{
+    const Key key = make_key(seed);
+    const DisorderRates dr = make_disorder_rates(Tp, Tq);
+    dim3 block(sh.TX, sh.TY);
+    if (d_counters)
+        scabit_half_kernel<true, true><<<sh.grid, block, 0, st>>>(d_sys, lx, ly, sigma, step, key, stream_id,
+                                                                  dr.tp[0], dr.tq[0], sh.TX, sh.TY, d_counters,
+                                                                  d_dis_cbbit, dr);
+    else
+        scabit_half_kernel<false, true><<<sh.grid, block, 0, st>>>(d_sys, lx, ly, sigma, step, key, stream_id,
+                                                                   dr.tp[0], dr.tq[0], sh.TX, sh.TY, nullptr,
+                                                                   d_dis_cbbit, dr);
     return cudaGetLastError();
 }
 

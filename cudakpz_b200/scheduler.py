@@ -96,10 +96,29 @@ class Scheduler:
     def initHomogeneous(self) -> None:
         check(lib.kpzb_init_homogeneous(self._h), "kpzb_init_homogeneous")
 
-    def setPQ(self, p: float, q: float) -> bool:
-        check(lib.kpzb_set_pq(self._h, p, q), "kpzb_set_pq")
-        self._p, self._q = float(p), float(q)
+    def setPQ(self, p: float, q: float, n: int = 0) -> bool:
+        """SchedulerService::setPQ(p, q, n): rates of disorder class n (0 = the plain rates)."""
+        if n == 0:
+            check(lib.kpzb_set_pq(self._h, p, q), "kpzb_set_pq")
+            self._p, self._q = float(p), float(q)
+        else:
+            check(lib.kpzb_set_pq_class(self._h, n, p, q), "kpzb_set_pq_class")
         return True
+
+    def setDisorder(self, words: np.ndarray) -> None:
+        """Quenched disorder classes, ENC_LOCAL words (SchedulerService::m_disorder)."""
+        w = np.ascontiguousarray(words, dtype=np.uint32)
+        if w.size != self.size_words():
+            raise ValueError("disorder needs one word per lattice word (ENC_LOCAL layout)")
+        check(lib.kpzb_set_disorder(self._h, w.ctypes.data), "kpzb_set_disorder")
+
+    def mcsDisorder2SyncRng(self, n: int) -> None:
+        check(lib.kpzb_mcs_disorder(self._h, int(n)), "kpzb_mcs_disorder")
+        self._mcs += int(n)
+
+    def mcsDisorder2SyncRngAsync(self, n: int) -> None:
+        check(lib.kpzb_mcs_disorder_async(self._h, int(n)), "kpzb_mcs_disorder_async")
+        self._mcs += int(n)
 
     def rateP(self) -> float:
         return self._p

@@ -79,6 +79,22 @@ kpzb_status kpzb_set_pq(kpzb_handle* h, double p, double q);
  * kpz/GPUTinyMT.cu:74-103). `stream` separates replicas sharing a seed. */
 kpzb_status kpzb_seed(kpzb_handle* h, uint64_t seed, uint32_t stream);
 
+/* SchedulerService::setPQ(p, q, n) for rate class n = 0..3 (kpz/schedulerService.h:186-192):
+ * the rates a site of disorder class n uses in kpzb_mcs_disorder; class 0 is kpzb_set_pq's.
+ * Classes never set follow class 0. */
+kpzb_status kpzb_set_pq_class(kpzb_handle* h, int n, double p, double q);
+/* Quenched disorder (SchedulerService::m_disorder, generateDisorder2 at
+ * kpz/schedulerService.cpp:54-71): one word per lattice word in ENC_LOCAL layout for every
+ * dynamics; the 2 bits at a site's slope position are its rate class (generateDisorder2 sets
+ * only the low bit: classes 0 and 1). */
+kpzb_status kpzb_set_disorder(kpzb_handle* h, const uint32_t* local_words);
+/* mcsDisorder2SyncRng(n) (kpz/schedulerService.h:212; SCA: Disorder2SyncRng,
+ * kpz/kpzSCACores.cu:217-280; DT: caller_mcsDisorder2SyncRng, kpz/kpz.cu:238-246): n MCS in
+ * which a candidate site flips with its class's rate.  Same random stream as kpzb_mcs, so equal
+ * rates in every class give kpzb_mcs's lattice.  One launch per half-step (SCA/SCABit). */
+kpzb_status kpzb_mcs_disorder(kpzb_handle* h, int n);
+kpzb_status kpzb_mcs_disorder_async(kpzb_handle* h, int n);
+
 /* SchedulerService::mcsPQSyncRng(n) (kpz/schedulerService.h:211; SCA/SCABit doMcs at
  * kpz/schedulerSCA.cu:43-70, kpz/schedulerSCABit.cu:46-73; DT at kpz/schedulerDT.cu:38-78):
  * n Monte-Carlo steps with the rates from kpzb_set_pq. Synchronous. */

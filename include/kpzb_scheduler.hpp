@@ -50,12 +50,23 @@ public:
     size_t sizeW() const { return kpzb_size_words(h_); }
 
     void initHomogeneous() { check(kpzb_init_homogeneous(h_), "kpzb_init_homogeneous"); }
-    bool setPQ(double p, double q)
+    // SchedulerService::setPQ(p, q, n): n > 0 sets the rates of quenched-disorder class n
+    bool setPQ(double p, double q, int n = 0)
     {
+        if (n != 0) {
+            check(kpzb_set_pq_class(h_, n, p, q), "kpzb_set_pq_class");
+            return true;
+        }
         check(kpzb_set_pq(h_, p, q), "kpzb_set_pq");
         p_ = p;
         q_ = q;
         return true;
+    }
+    // SchedulerService::m_disorder: rate-class words in ENC_LOCAL layout
+    void setDisorder(const std::vector<uint32_t>& words)
+    {
+        if (words.size() != sizeW()) throw Error(KPZB_EINVAL, "setDisorder: one word per lattice word");
+        check(kpzb_set_disorder(h_, words.data()), "kpzb_set_disorder");
     }
     double rateP() const { return p_; }
     double rateQ() const { return q_; }
@@ -80,6 +91,38 @@ public:
         mcs_ += (unsigned)n;
     }
     void join() { check(kpzb_join(h_), "kpzb_join"); }
+    void mcsDisorder2SyncRng(int n)
+    {
+        check(kpzb_mcs_disorder(h_, n), "kpzb_mcs_disorder");
+        mcs_ += (unsigned)n;
+    }
+
+    // SchedulerService::saveBit (kpz/schedulerService.cpp:389-401) plus the resume trailer
+    bool saveBit(const char* file, const char* meta = nullptr)
+    {
+        check(kpzb_save(h_, file, meta), "kpzb_save");
+        return true;
+    }
+    bool loadBit(const char* file)
+    {
+        check(kpzb_load(h_, file), "kpzb_load");
+        mcs_ = (unsigned)deviceMcs();
+        return true;
+    }
+
+    // the frontend's measurement loop (kpz/kpzScaling.cpp:194-215) with device-side analysis:
+    // rows of {t, W^2, <h^1..7>, ch, cs}
+    std::vector<double> measureRun(uint64_t end, const kpzb_sampling& s, int64_t corrStart = -1,
+                                   uint64_t corrStop = 0)
+    {
+        int n = 0;
+        kpzb_status st = kpzb_measure_run(h_, &s, end, corrStart, corrStop, nullptr, 0, &n);
+        if (st != KPZB_OK && n == 0) check(st, "kpzb_measure_run");
+        std::vector<double> rows((size_t)n * 11);
+        check(kpzb_measure_run(h_, &s, end, corrStart, corrStop, rows.data(), n, &n), "kpzb_measure_run");
+        mcs_ = (unsigned)end;
+        return rows;
+    }
 
     // host copy (kpz/schedulerBase.cu:35-52), in the encoding of encoding()
     std::vector<uint32_t>& system() { return host_; }

@@ -164,9 +164,13 @@ static void flip_site(uint32_t* w, int lx, int ly, int enc, int x, int y, int bi
 /* xors both bits of (x,y), the x-bit of (x+1,y) and the y-bit of (x,y+1).   */
 /* All sites of one sublattice are independent, so loop order is free.     */
 /* ------------------------------------------------------------------------ */
-void ko_sca_halfstep(uint32_t* w, int lx, int ly, int encoding, int sigma,
-                     uint64_t seed, uint32_t stream, uint32_t step,
-                     uint64_t Tp, uint64_t Tq, int64_t* dep, int64_t* des)
+/* Half-step with per-site rate classes: class c = the 2 bits of dis (ENC_LOCAL words, the
+ * layout of SchedulerService::m_disorder) at the site, or 0 when dis is NULL; thresholds
+ * Tp[c], Tq[c] (Disorder2SyncRng::update, kpz/kpzSCACores.cu:238-261: the site's own disorder
+ * bits pick DEVICE_CONST_DISORDER2_P/Q). */
+void ko_sca_halfstep_dis(uint32_t* w, int lx, int ly, int encoding, int sigma, uint64_t seed,
+                         uint32_t stream, uint32_t step, const uint64_t Tp[4], const uint64_t Tq[4],
+                         const uint32_t* dis, int64_t* dep, int64_t* des)
 {
     int L = 1 << lx, M = 1 << ly;
     int64_t nd = 0, nr = 0;
@@ -177,9 +181,10 @@ void ko_sca_halfstep(uint32_t* w, int lx, int ly, int encoding, int sigma,
             int r = get_site(w, lx, ly, encoding, (x + 1) & (L - 1), y) & 1;
             int l = (get_site(w, lx, ly, encoding, x, (y + 1) & (M - 1)) >> 1) & 1;
             int config = c | (r << 2) | (l << 3);
+            int cls = dis ? ko_local_get(dis, lx, x, y) : 0;
             uint64_t T;
-            if (config == 12) T = Tp;
-            else if (config == 3) T = Tq;
+            if (config == 12) T = Tp[cls];
+            else if (config == 3) T = Tq[cls];
             else continue;
             if (T == 0) continue;
             if (T < ((uint64_t)1 << 32)) {
@@ -195,6 +200,32 @@ void ko_sca_halfstep(uint32_t* w, int lx, int ly, int encoding, int sigma,
         }
     if (dep) *dep += nd;
     if (des) *des += nr;
+}
+
+void ko_sca_halfstep(uint32_t* w, int lx, int ly, int encoding, int sigma,
+                     uint64_t seed, uint32_t stream, uint32_t step,
+                     uint64_t Tp, uint64_t Tq, int64_t* dep, int64_t* des)
+{
+    const uint64_t P[4] = {Tp, Tp, Tp, Tp}, Q[4] = {Tq, Tq, Tq, Tq};
+    ko_sca_halfstep_dis(w, lx, ly, encoding, sigma, seed, stream, step, P, Q, NULL, dep, des);
+}
+
+/* kpz/schedulerSCA.cu mcsDisorder2SyncRng: n MCS with rate classes p[c], q[c] */
+void ko_sca_mcs_dis(uint32_t* w, int lx, int ly, int encoding, uint64_t seed, uint32_t stream,
+                    uint64_t t0, int n, const double p[4], const double q[4], const uint32_t* dis,
+                    int64_t* dep, int64_t* des)
+{
+    uint64_t Tp[4], Tq[4];
+    for (int c = 0; c < 4; ++c) {
+        Tp[c] = ko_threshold(p[c]);
+        Tq[c] = ko_threshold(q[c]);
+    }
+    for (int i = 0; i < n; ++i) {
+        uint64_t t = t0 + (uint64_t)i;
+        for (int s = 0; s < 2; ++s)
+            ko_sca_halfstep_dis(w, lx, ly, encoding, s, seed, stream, (uint32_t)(2 * t + s), Tp, Tq, dis,
+                                dep, des);
+    }
 }
 
 /* kpz/schedulerSCABit.cu:46-73 (caller(0); caller(1); per MCS) */
@@ -372,10 +403,21 @@ void ko_dt_plan(uint64_t seed, uint32_t stream, uint64_t t, int* ox, int* oy, in
 void ko_dt_mcs(uint32_t* w, int lx, int ly, uint64_t seed, uint32_t stream, uint64_t t0, int n,
                double p, double q, int64_t* dep, int64_t* des)
 {
+    const double P[4] = {p, p, p, p}, Q[4] = {q, q, q, q};
+    ko_dt_mcs_dis(w, lx, ly, seed, stream, t0, n, P, Q, NULL, dep, des);
+}
+
+void ko_dt_mcs_dis(uint32_t* w, int lx, int ly, uint64_t seed, uint32_t stream, uint64_t t0, int n,
+                   const double p[4], const double q[4], const uint32_t* dis, int64_t* dep, int64_t* des)
+{
     const int L = 1 << lx, M = 1 << ly;
     const int BX = 256, BY = 128;
     const int nbx = L / (2 * BX), nby = M / (2 * BY);
-    const uint64_t Tp = ko_threshold(p), Tq = ko_threshold(q);
+    uint64_t Tpc[4], Tqc[4];
+    for (int c = 0; c < 4; ++c) {
+        Tpc[c] = ko_threshold(p[c]);
+        Tqc[c] = ko_threshold(q[c]);
+    }
     int64_t nd = 0, nr = 0;
     for (int i = 0; i < n; ++i) {
         const uint64_t t = t0 + (uint64_t)i;
@@ -406,9 +448,10 @@ void ko_dt_mcs(uint32_t* w, int lx, int ly, uint64_t seed, uint32_t stream, uint
                         const int rr = ko_local_get(w, lx, (x + 1) & (L - 1), y) & 1;
                         const int ll = (ko_local_get(w, lx, x, (y + 1) & (M - 1)) >> 1) & 1;
                         const int config = c | (rr << 2) | (ll << 3);
+                        const int cls = dis ? ko_local_get(dis, lx, x, y) : 0;
                         uint64_t T;
-                        if (config == 12) T = Tp;
-                        else if (config == 3) T = Tq;
+                        if (config == 12) T = Tpc[cls];
+                        else if (config == 3) T = Tqc[cls];
                         else continue;
                         if (T == 0) continue;
                         if (T < ((uint64_t)1 << 32)) {
@@ -548,6 +591,52 @@ void ko_rs_mcs_count(uint32_t* w, int lx, int ly, ko_dsfmt* s, int n, int pq, do
                     if (ko_dsfmt_close_open(s) >= q) continue;
                 } else continue;
             }
+            ko_local_flip(w, lx, x, y, 3);
+            ko_local_flip(w, lx, (x + 1) & (L - 1), y, 1);
+            ko_local_flip(w, lx, x, (y + 1) & (M - 1), 2);
+            if (config == 12) ++nd; else ++nr;
+        }
+    }
+    if (dep) *dep += nd;
+    if (des) *des += nr;
+}
+
+/* SchedulerService::generateDisorder2 (kpz/schedulerService.cpp:54-71): for every word, bit s
+ * (s = 0, 2, ..., 30: the x-slope bit of each of its 16 sites) is set when a dSFMT draw is
+ * below `fill`; words in index order. */
+void ko_generate_disorder2(uint32_t* dis, int lx, int ly, ko_dsfmt* s, double fill)
+{
+    const uint64_t nw = ko_size_words(lx, ly);
+    for (uint64_t a = 0; a < nw; ++a) {
+        uint32_t t = 0;
+        for (int b = 0; b < 32; b += 2)
+            if (ko_dsfmt_close_open(s) < fill) t |= 1u << b;
+        dis[a] = t;
+    }
+}
+
+/* SchedulerCPU::mcsDisorder2 (kpz/schedulerCPU.cpp:48-80): as mcsPQ, with the rates of the
+ * site's disorder class c(m_disorder) (the 2 bits of dis at the site). */
+void ko_rs_mcs_dis(uint32_t* w, int lx, int ly, ko_dsfmt* s, int n, const double p[4], const double q[4],
+                   const uint32_t* dis, int64_t* dep, int64_t* des)
+{
+    int64_t nd = 0, nr = 0;
+    int L = 1 << lx, M = 1 << ly;
+    uint64_t N = (uint64_t)1 << (lx + ly);
+    for (; n > 0; --n) {
+        for (uint64_t a = 0; a < N; ++a) {
+            int x = (int)(ko_dsfmt_close_open(s) * L);
+            int y = (int)(ko_dsfmt_close_open(s) * M);
+            int c = ko_local_get(w, lx, x, y);
+            int r = ko_local_get(w, lx, (x + 1) & (L - 1), y) & 1;
+            int l = (ko_local_get(w, lx, x, (y + 1) & (M - 1)) >> 1) & 1;
+            int config = c | (r << 2) | (l << 3);
+            int cls = ko_local_get(dis, lx, x, y);
+            if (config == 12) {
+                if (ko_dsfmt_close_open(s) >= p[cls]) continue;
+            } else if (config == 3) {
+                if (ko_dsfmt_close_open(s) >= q[cls]) continue;
+            } else continue;
             ko_local_flip(w, lx, x, y, 3);
             ko_local_flip(w, lx, (x + 1) & (L - 1), y, 1);
             ko_local_flip(w, lx, x, (y + 1) & (M - 1), 2);

@@ -66,6 +66,15 @@ void ko_sca_halfstep(uint32_t* w, int lx, int ly, int encoding, int sigma,
                      uint64_t seed, uint32_t stream, uint32_t step,
                      uint64_t Tp, uint64_t Tq, int64_t* dep, int64_t* des);
 /* n MCS starting at device MCS count t0 (sublattice 0 then 1 each MCS). */
+/* Quenched disorder (mcsDisorder2SyncRng): rate class c = the 2 bits of `dis` (ENC_LOCAL words,
+ * SchedulerService::m_disorder's layout) at the site picks Tp[c] / Tq[c]; the random stream is
+ * the same as without disorder. */
+void ko_sca_halfstep_dis(uint32_t* w, int lx, int ly, int encoding, int sigma, uint64_t seed,
+                         uint32_t stream, uint32_t step, const uint64_t Tp[4], const uint64_t Tq[4],
+                         const uint32_t* dis, int64_t* dep, int64_t* des);
+void ko_sca_mcs_dis(uint32_t* w, int lx, int ly, int encoding, uint64_t seed, uint32_t stream,
+                    uint64_t t0, int n, const double p[4], const double q[4], const uint32_t* dis,
+                    int64_t* dep, int64_t* des);
 void ko_sca_mcs(uint32_t* w, int lx, int ly, int encoding, uint64_t seed, uint32_t stream,
                 uint64_t t0, int n, double p, double q, int64_t* dep, int64_t* des);
 
@@ -102,6 +111,8 @@ void ko_check_invariants(const uint32_t* w, int lx, int ly, int encoding, int64_
 #define KO_TAG_DT_POS 5u
 void ko_dt_mcs(uint32_t* w, int lx, int ly, uint64_t seed, uint32_t stream, uint64_t t0, int n,
                double p, double q, int64_t* dep, int64_t* des);
+void ko_dt_mcs_dis(uint32_t* w, int lx, int ly, uint64_t seed, uint32_t stream, uint64_t t0, int n,
+                   const double p[4], const double q[4], const uint32_t* dis, int64_t* dep, int64_t* des);
 /* the per-MCS origin (sites) and domain-set order used by ko_dt_mcs */
 void ko_dt_plan(uint64_t seed, uint32_t stream, uint64_t t, int* ox, int* oy, int order[4]);
 
@@ -118,6 +129,10 @@ void ko_rs_mcs(uint32_t* w, int lx, int ly, ko_dsfmt* s, int n, int pq, double p
 /* the same, also counting depositions and desorptions */
 void ko_rs_mcs_count(uint32_t* w, int lx, int ly, ko_dsfmt* s, int n, int pq, double p, double q,
                      int64_t* dep, int64_t* des);
+/* SchedulerService::generateDisorder2(fill) and SchedulerCPU::mcsDisorder2 with rate classes */
+void ko_generate_disorder2(uint32_t* dis, int lx, int ly, ko_dsfmt* s, double fill);
+void ko_rs_mcs_dis(uint32_t* w, int lx, int ly, ko_dsfmt* s, int n, const double p[4], const double q[4],
+                   const uint32_t* dis, int64_t* dep, int64_t* des);
 
 #ifdef __cplusplus
 }

@@ -60,6 +60,13 @@ def _load():
                              C.c_double]),
         "ko_rs_mcs_count": (None, [u32p, C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_int,
                                    C.c_double, C.c_double, i64p, i64p]),
+        "ko_sca_mcs_dis": (None, [u32p, C.c_int, C.c_int, C.c_int, C.c_uint64, C.c_uint32, C.c_uint64,
+                                  C.c_int, dblp, dblp, u32p, i64p, i64p]),
+        "ko_dt_mcs_dis": (None, [u32p, C.c_int, C.c_int, C.c_uint64, C.c_uint32, C.c_uint64, C.c_int,
+                                 dblp, dblp, u32p, i64p, i64p]),
+        "ko_generate_disorder2": (None, [u32p, C.c_int, C.c_int, C.c_void_p, C.c_double]),
+        "ko_rs_mcs_dis": (None, [u32p, C.c_int, C.c_int, C.c_void_p, C.c_int, dblp, dblp, u32p, i64p,
+                                 i64p]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
@@ -124,6 +131,44 @@ def dt_mcs(w: np.ndarray, lx: int, ly: int, seed: int, stream: int, t0: int, n: 
     """Double-tiling RS emulation (ENC_LOCAL, in place); returns (#deposits, #desorptions)."""
     dep, des = C.c_int64(0), C.c_int64(0)
     lib.ko_dt_mcs(_u32(w), lx, ly, seed, stream, t0, n, p, q, C.byref(dep), C.byref(des))
+    return dep.value, des.value
+
+
+def _rates4(r):
+    r = list(r) + [r[-1]] * (4 - len(r))
+    return (C.c_double * 4)(*r[:4])
+
+
+def sca_mcs_dis(w: np.ndarray, lx: int, ly: int, encoding: int, seed: int, stream: int, t0: int,
+                n: int, p, q, dis: np.ndarray):
+    """Quenched disorder: rate class = the 2 bits of `dis` (ENC_LOCAL) at each site picks
+    p[c], q[c] (lists of up to 4; missing classes repeat the last).  In place; (#dep, #des)."""
+    dep, des = C.c_int64(0), C.c_int64(0)
+    lib.ko_sca_mcs_dis(_u32(w), lx, ly, encoding, seed, stream, t0, n, _rates4(p), _rates4(q), _u32(dis),
+                       C.byref(dep), C.byref(des))
+    return dep.value, des.value
+
+
+def dt_mcs_dis(w: np.ndarray, lx: int, ly: int, seed: int, stream: int, t0: int, n: int, p, q,
+               dis: np.ndarray):
+    dep, des = C.c_int64(0), C.c_int64(0)
+    lib.ko_dt_mcs_dis(_u32(w), lx, ly, seed, stream, t0, n, _rates4(p), _rates4(q), _u32(dis),
+                      C.byref(dep), C.byref(des))
+    return dep.value, des.value
+
+
+def generate_disorder2(lx: int, ly: int, rng: "DSFMT", fill: float) -> np.ndarray:
+    """SchedulerService::generateDisorder2 (ENC_LOCAL words, one class bit per site)."""
+    d = np.empty(size_words(lx, ly), dtype=np.uint32)
+    lib.ko_generate_disorder2(_u32(d), lx, ly, rng.ptr, fill)
+    return d
+
+
+def rs_mcs_dis(w: np.ndarray, lx: int, ly: int, rng: "DSFMT", n: int, p, q, dis: np.ndarray):
+    """SchedulerCPU::mcsDisorder2 in place; returns (#dep, #des)."""
+    dep, des = C.c_int64(0), C.c_int64(0)
+    lib.ko_rs_mcs_dis(_u32(w), lx, ly, rng.ptr, n, _rates4(p), _rates4(q), _u32(dis), C.byref(dep),
+                      C.byref(des))
     return dep.value, des.value
 
 

@@ -16,6 +16,7 @@
 //   bench-cbbit LX P Q N THR        time mcsPQSyncRng(N) of SchedulerCPUCBBit; prints upd/ns
 //   bench-rs LX N                   time SchedulerCPU::mcs(N); prints upd/ns
 //   savebit LX SEED N FILE [META]   SchedulerService::saveBit of the RS lattice after N MCS
+//   rsdis LX SEED FILL N P0 Q0 P1 Q1 DISFILE LATFILE   generateDisorder2 + SchedulerCPU::mcsDisorder2
 #include <chrono>
 #include <cstdio>
 #include <cstdlib>
@@ -120,6 +121,30 @@ int main(int argc, char** argv)
             std::cout << '\n';
         }
         save(argv[argc - 1], s.system(), s.size().sizeW());
+        return 0;
+    }
+    if (cmd == "rsdis") {
+        // generateDisorder2(fill) (kpz/schedulerService.cpp:54-71), then
+        // SchedulerCPU::mcsDisorder2(N) (kpz/schedulerCPU.cpp:48-80) with classes 0 and 1
+        const int lx = std::atoi(argv[2]);
+        const int seed = std::atoi(argv[3]);
+        const double fill = std::atof(argv[4]);
+        const int n = std::atoi(argv[5]);
+        const double p0 = std::atof(argv[6]), q0 = std::atof(argv[7]);
+        const double p1 = std::atof(argv[8]), q1 = std::atof(argv[9]);
+        quiet();
+        Kpz::SchedulerCPU s(lx, lx);
+        s.supplySeed(1, seed);
+        s.initHomogeneous(Kpz::SchedulerService::ENC_LOCAL);
+        s.pushSystem();
+        s.generateDisorder2(fill);
+        s.setPQ(p0, q0, 0);
+        s.setPQ(p1, q1, 1);
+        s.mcsDisorder2(n);
+        s.popSystem();
+        loud();
+        save(argv[10], s.disorder(), s.size().sizeW());
+        save(argv[11], s.system(), s.size().sizeW());
         return 0;
     }
     if (cmd == "savebit") {

@@ -96,7 +96,14 @@ def main():
                 an[key + "_check_broken"] = np.array(int(run("check", enc, lx, tmp / "c.bin")[0]))
     np.savez_compressed(HERE / "ref_analysis.npz", **an)
 
-    # 5. SchedulerService::saveBit file of the RS lattice (256^2, seed 1, 16 MCS): the lattice
+    # 5. quenched binary disorder: generateDisorder2(0.3) then SchedulerCPU::mcsDisorder2(20)
+    #    with class rates (p0,q0) = (0.9,0.1), (p1,q1) = (0.3,0.6); 256^2, seed 3
+    run("rsdis", 8, 3, 0.3, 20, 0.9, 0.1, 0.3, 0.6, tmp / "dis.bin", tmp / "lat.bin")
+    np.savez_compressed(HERE / "ref_disorder.npz",
+                        disorder=np.fromfile(tmp / "dis.bin", dtype=np.uint32),
+                        lattice=np.fromfile(tmp / "lat.bin", dtype=np.uint32))
+
+    # 6. SchedulerService::saveBit file of the RS lattice (256^2, seed 1, 16 MCS): the lattice
     #    file format the checkpoint entry points keep (kpz/schedulerService.cpp:389-401)
     run("savebit", 8, 1, 16, HERE / "ref_savebit_rs256.bin", "CudaKpz saveBit fixture")
     print("golden vectors written to", HERE)

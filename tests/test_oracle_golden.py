@@ -115,3 +115,27 @@ def test_savebit_fixture_is_the_rs_lattice(oracle):
     w = oracle.homogeneous(8, 8, oracle.ENC_LOCAL)
     oracle.rs_mcs(w, 8, 8, oracle.DSFMT(1), 16)
     assert np.array_equal(words, w)
+
+
+def test_disorder_generation_and_rs_dynamics(oracle):
+    """SchedulerService::generateDisorder2 and SchedulerCPU::mcsDisorder2 (256^2, seed 3,
+    fill 0.3, 20 MCS, class rates (0.9,0.1) and (0.3,0.6)), reproduced bit for bit."""
+    z = np.load(G / "ref_disorder.npz")
+    rng = oracle.DSFMT(3)
+    d = oracle.generate_disorder2(8, 8, rng, 0.3)
+    assert np.array_equal(d, z["disorder"])
+    w = oracle.homogeneous(8, 8, oracle.ENC_LOCAL)
+    oracle.rs_mcs_dis(w, 8, 8, rng, 20, [0.9, 0.3], [0.1, 0.6], d)
+    assert np.array_equal(w, z["lattice"])
+
+
+def test_disorder_with_equal_rates_is_the_plain_dynamics(oracle):
+    """The counter-stream disorder restatement with every class at the same rates is the plain
+    SCA / DT dynamics (same random stream)."""
+    lx = ly = 9
+    dis = oracle.random_lattice(lx, ly, oracle.ENC_LOCAL, seed=4)  # arbitrary class bits
+    a = oracle.homogeneous(lx, ly, oracle.ENC_CBBIT)
+    b = a.copy()
+    oracle.sca_mcs(a, lx, ly, oracle.ENC_CBBIT, 5, 0, 0, 3, 0.7, 0.2)
+    oracle.sca_mcs_dis(b, lx, ly, oracle.ENC_CBBIT, 5, 0, 0, 3, [0.7] * 4, [0.2] * 4, dis)
+    assert np.array_equal(a, b)

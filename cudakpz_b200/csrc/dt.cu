@@ -42,11 +42,31 @@ dt_kernel(uint32_t* __restrict__ sys, int lxw, int lyw, int lnbx, int nblocks, i
 {
     __shared__ uint32_t tile[DT_TH * DT_TW];
     __shared__ uint32_t dtile[DIS ? DT_TH * DT_TW : 1];
+    // Site geometry of every (sub-cell s, in-cell position pb) pair, relative to a thread's cell:
+    // the origin's offset inside a word (ox & 3, oy & 3) is the same for every block and thread
+    // of the launch, so the word offsets and bit shifts of the site, its right neighbour and its
+    // lower neighbour form one 64-entry table:
+    //   bits 0-7 word offset, 8-12 site shift, 13-17 right-neighbour x-slope shift,
+    //   18-22 lower-neighbour y-slope shift, 23 right neighbour in the next word,
+    //   24 lower neighbour in the next word row.
+    __shared__ uint32_t lut[64];
     const int tid = threadIdx.y * DT_TX + threadIdx.x;
     const uint32_t Wx = 1u << lxw, Wy = 1u << lyw;
     bool need_u = !(tp.always || tp.planes == 0) || !(tq.always || tq.planes == 0);
     if (DIS) need_u = dr.planes > 0;
     unsigned long long ndep = 0, ndes = 0;
+    if (tid < 64) {
+        const int sc = tid >> 4, pb = tid & 15;
+        const int ax = (ox & 3) + (pb & 3), ay = (oy & 3) + (pb >> 2);
+        const int col = (sc & 1) + (ax >> 2), row = (sc >> 1) + (ay >> 2);
+        const int xb = ax & 3, yb = ay & 3;
+        const uint32_t sh = (uint32_t)((xb << 1) | (yb << 3));
+        const uint32_t shr = (uint32_t)((((ax + 1) & 3) << 1) | (yb << 3));
+        const uint32_t shd = (uint32_t)((xb << 1) | (((ay + 1) & 3) << 3) | 1);
+        lut[tid] = (uint32_t)(row * DT_TW + col) | (sh << 8) | (shr << 13) | (shd << 18) |
+                   ((xb == 3 ? 1u : 0u) << 23) | ((yb == 3 ? 1u : 0u) << 24);
+    }
+    const int tbase = 2 * threadIdx.y * DT_TW + 2 * threadIdx.x;
 
     for (int b = blockIdx.x; b < nblocks; b += gridDim.x) {
         const int bx = b & ((1 << lnbx) - 1), by = b >> lnbx;
@@ -63,57 +83,62 @@ dt_kernel(uint32_t* __restrict__ sys, int lxw, int lyw, int lnbx, int nblocks, i
         const uint4 sub = philox4x32_10(
             make_uint4((uint32_t)b, t, (TAG_DT_SUB << 24) | ((uint32_t)d << 16), stream), key);
         const uint32_t cid = (uint32_t)b * (DT_TX * DT_TY) + (uint32_t)tid;
-        const int sx0 = (int)(X0 & 3u) + threadIdx.x * 8;
-        const int sy0 = (int)(Y0 & 3u) + threadIdx.y * 8;
         __syncthreads();
         uint4 pos = make_uint4(0, 0, 0, 0), uu = make_uint4(0, 0, 0, 0);
-        for (int r = 0; r < DT_ROUNDS; ++r) {
-            if ((r & 31) == 0)
+        for (int rb = 0; rb < DT_ROUNDS; rb += 8) {
+            if ((rb & 31) == 0)
                 pos = philox4x32_10(
-                    make_uint4(cid, t, (TAG_DT_POS << 24) | ((uint32_t)d << 16) | (uint32_t)(r >> 5), stream),
+                    make_uint4(cid, t, (TAG_DT_POS << 24) | ((uint32_t)d << 16) | (uint32_t)(rb >> 5), stream),
                     key);
-            if (need_u && (r & 3) == 0)
-                uu = philox4x32_10(
-                    make_uint4(cid, t, (TAG_DT << 24) | ((uint32_t)d << 16) | (uint32_t)(r >> 2), stream),
-                    key);
-            const uint32_t sw = (r < 16) ? sub.x : (r < 32) ? sub.y : (r < 48) ? sub.z : sub.w;
-            const int s = (int)((sw >> (2 * (r & 15))) & 3u);
-            const int pq = (r & 31) >> 3;
+            const uint32_t sw = (rb < 16) ? sub.x : (rb < 32) ? sub.y : (rb < 48) ? sub.z : sub.w;
+            const int pq = (rb & 31) >> 3;
             const uint32_t pw = pq == 0 ? pos.x : pq == 1 ? pos.y : pq == 2 ? pos.z : pos.w;
-            const int pb = (int)((pw >> (4 * (r & 7))) & 15u);
-            const int x = sx0 + (s & 1) * 4 + (pb & 3);
-            const int y = sy0 + (s >> 1) * 4 + (pb >> 2);
-            // ENC_LOCAL word / bit inside the tile (kpz/systemSize.h:94-100)
-            const int wi = (y >> 2) * DT_TW + (x >> 2);
-            const int sh = ((x & 3) << 1) | ((y & 3) << 3);
-            const int wr = (y >> 2) * DT_TW + ((x + 1) >> 2);
-            const int shr = (((x + 1) & 3) << 1) | ((y & 3) << 3);
-            const int wd = ((y + 1) >> 2) * DT_TW + (x >> 2);
-            const int shd = ((x & 3) << 1) | (((y + 1) & 3) << 3);
-            const uint32_t cw = tile[wi];
-            const int config = (int)((cw >> sh) & 3u) | (int)(((tile[wr] >> shr) & 1u) << 2) |
-                               (int)(((tile[wd] >> (shd | 1)) & 1u) << 3);
-            bool flip = false;
-            if (config == 12 || config == 3) {
-                int cls = 0;
-                if (DIS) cls = (int)((dtile[wi] >> sh) & 3u);
-                const Thresh& th = DIS ? (config == 12 ? dr.tp[cls] : dr.tq[cls]) : (config == 12 ? tp : tq);
-                if (th.always) flip = true;
-                else if (th.planes) {
-                    const uint32_t u = (r & 3) == 0 ? uu.x : (r & 3) == 1 ? uu.y : (r & 3) == 2 ? uu.z : uu.w;
-                    flip = u < th.t;
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                const int r = rb + j;
+                if (need_u && (j & 3) == 0)
+                    uu = philox4x32_10(
+                        make_uint4(cid, t, (TAG_DT << 24) | ((uint32_t)d << 16) | (uint32_t)(r >> 2), stream), key);
+                const uint32_t sc = (sw >> (2 * (r & 15))) & 3u;
+                const uint32_t pb = (pw >> (4 * j)) & 15u;
+                const uint32_t e = lut[sc * 16u + pb];
+                const int w = tbase + (int)(e & 255u);
+                const uint32_t sh = (e >> 8) & 31u, shr = (e >> 13) & 31u, shd = (e >> 18) & 31u;
+                const bool dxr = (e >> 23) & 1u, dyd = (e >> 24) & 1u;
+                uint32_t cw = tile[w];
+                uint32_t rw = dxr ? tile[w + 1] : cw;
+                uint32_t dw = dyd ? tile[w + DT_TW] : cw;
+                const uint32_t c = (cw >> sh) & 3u, rbit = (rw >> shr) & 1u, lbit = (dw >> shd) & 1u;
+                const bool is_p = c == 0u && rbit && lbit;      // local minimum (config 12)
+                const bool is_q = c == 3u && !rbit && !lbit;    // local maximum (config 3)
+                bool flip = false;
+                if (is_p || is_q) {
+                    int cls = 0;
+                    if (DIS) cls = (int)((dtile[w] >> sh) & 3u);
+                    const Thresh& th = DIS ? (is_p ? dr.tp[cls] : dr.tq[cls]) : (is_p ? tp : tq);
+                    if (th.always) flip = true;
+                    else if (th.planes) {
+                        const uint32_t u = (j & 3) == 0 ? uu.x : (j & 3) == 1 ? uu.y : (j & 3) == 2 ? uu.z : uu.w;
+                        flip = u < th.t;
+                    }
                 }
-            }
-            if (flip) {
-                tile[wi] ^= 3u << sh;
-                tile[wr] ^= 1u << shr;
-                tile[wd] ^= 1u << (shd | 1);
-                if (COUNT) {
-                    if (config == 12) ++ndep;
-                    else ++ndes;
+                if (flip) {
+                    // the words of this round's site and neighbours belong to this thread alone
+                    cw ^= 3u << sh;
+                    if (dxr) rw ^= 1u << shr;
+                    else cw ^= 1u << shr;
+                    if (dyd) dw ^= 1u << shd;
+                    else cw ^= 1u << shd;
+                    tile[w] = cw;
+                    if (dxr) tile[w + 1] = rw;
+                    if (dyd) tile[w + DT_TW] = dw;
+                    if (COUNT) {
+                        if (is_p) ++ndep;
+                        else ++ndes;
+                    }
                 }
+                __syncthreads();
             }
-            __syncthreads();
         }
         for (int i = tid; i < DT_TH * DT_TW; i += DT_TX * DT_TY) {
             const uint32_t r = i / DT_TW, c = i - r * DT_TW;

@@ -38,8 +38,8 @@ UNIT = "attempted site updates/ns"
 # Per-launch DRAM traffic (dram__bytes_read.sum + dram__bytes_write.sum) of the fused pass
 # kernel at 16384^2, from one ncu capture per (p, q, MCS per pass); the commands and the
 # full figures are in profiles/scabit_fused_16384.md.
-NCU_TRAFFIC_PER_LAUNCH = {(1.0, 0.0, "band", 7): 67.326e6 + 23.604e6,
-                          (0.5, 0.5, "band", 4): 67.237e6 + 18.461e6}
+NCU_TRAFFIC_PER_LAUNCH = {(1.0, 0.0, "band", 7): 67.324e6 + 23.171e6,
+                          (0.5, 0.5, "band", 4): 67.218e6 + 17.975e6}
 
 
 def parse():

@@ -9,7 +9,10 @@
 // Exactness: snapshot s keeps its path-relative heights (kpz/correlator.cpp:47-96) shifted
 // by c_s = floor(<h_s>): v = h - c_s, split into three balanced base-128 digits
 // v = l0 + 128 l1 + 16384 l2 with l_a in [-64, 63] (|v| < 1,056,832).  Row a*64+s of the
-// limb matrix A (192 x N, int8, K-major) holds l_a of snapshot s.  The limb Gram A A^T is
+// limb matrix A (192 x N, int8) holds l_a of snapshot s, stored K-tile-major: the 192 rows x
+// 128 sites of K tile kt are one contiguous 24 KB block (element (r, k) at
+// (k / 128) * 24576 + r * 128 + k % 128), so the tensor-core kernel's TMA box of one tile is a
+// single contiguous read.  The limb Gram A A^T is
 // exact in int32 over windows of 2^18 sites (|l l'| <= 2^12) and summed in int64; then
 //   sum v_s v_t = sum_{a,b} 128^(a+b) Glimb[a*64+s][b*64+t],
 //   sum h_s h_t = sum v_s v_t + c_t S1v_s + c_s S1v_t + N c_s c_t,
@@ -26,10 +29,18 @@
 
 namespace kpzb {
 
-// v = h - c split into balanced base-128 limbs; flags |v| too large for three limbs.
-__global__ void limb_kernel(const int32_t* __restrict__ h, uint64_t n, int32_t c, int8_t* __restrict__ a0,
-                            uint64_t row_stride, unsigned long long* __restrict__ sums,
-                            unsigned int* __restrict__ err)
+constexpr uint64_t LIMB_TILE = 128;                 // sites per K tile
+constexpr uint64_t LIMB_TILE_BYTES = 192 * LIMB_TILE;  // one tile of all 192 rows
+
+__host__ __device__ inline uint64_t limb_index(int row, uint64_t k)
+{
+    return (k / LIMB_TILE) * LIMB_TILE_BYTES + (uint64_t)row * LIMB_TILE + (k % LIMB_TILE);
+}
+
+// v = h - c split into balanced base-128 limbs (snapshot s: rows s, 64+s, 128+s); flags |v|
+// too large for three limbs.
+__global__ void limb_kernel(const int32_t* __restrict__ h, uint64_t n, int32_t c, int8_t* __restrict__ A, int s,
+                            unsigned long long* __restrict__ sums, unsigned int* __restrict__ err)
 {
     long long s0 = 0, s1 = 0, s2 = 0;
     const uint64_t n16 = n / 16;
@@ -59,7 +70,8 @@ __global__ void limb_kernel(const int32_t* __restrict__ h, uint64_t n, int32_t c
             w[2][q] = p2;
         }
         for (int a = 0; a < 3; ++a)
-            reinterpret_cast<uint4*>(a0 + a * row_stride)[j] = make_uint4(w[a][0], w[a][1], w[a][2], w[a][3]);
+            *reinterpret_cast<uint4*>(A + limb_index(a * 64 + s, 16 * j)) =
+                make_uint4(w[a][0], w[a][1], w[a][2], w[a][3]);
     }
     for (int o = 16; o > 0; o >>= 1) {
         s0 += __shfl_xor_sync(0xffffffffu, s0, o);
@@ -78,8 +90,7 @@ __global__ void limb_kernel(const int32_t* __restrict__ h, uint64_t n, int32_t c
 // owns a 4x4 block of (s,t) pairs with int64 accumulators; CTA results go to G by atomics.
 constexpr int G64_KC = 128;
 __global__ void __launch_bounds__(256)
-gram_int64_kernel(const int8_t* __restrict__ A, uint64_t n, uint64_t row_stride, int ns,
-                  unsigned long long* __restrict__ G)
+gram_int64_kernel(const int8_t* __restrict__ A, uint64_t n, int ns, unsigned long long* __restrict__ G)
 {
     __shared__ int32_t v[64][G64_KC + 1];
     const int ts = (threadIdx.x >> 4) * 4, tt = (threadIdx.x & 15) * 4;
@@ -93,8 +104,8 @@ gram_int64_kernel(const int8_t* __restrict__ A, uint64_t n, uint64_t row_stride,
             int32_t val = 0;
             if (s < ns) {
                 const uint64_t idx = k0 + kk;
-                val = (int32_t)A[(uint64_t)s * row_stride + idx] + 128 * (int32_t)A[(uint64_t)(64 + s) * row_stride + idx] +
-                      16384 * (int32_t)A[(uint64_t)(128 + s) * row_stride + idx];
+                val = (int32_t)A[limb_index(s, idx)] + 128 * (int32_t)A[limb_index(64 + s, idx)] +
+                      16384 * (int32_t)A[limb_index(128 + s, idx)];
             }
             v[s][kk] = val;
         }
@@ -221,8 +232,7 @@ extern "C" kpzb_status kpzb_gram_add_device(kpzb_gram* g, const uint32_t* d_cbbi
     if (m.hmax - c > 1000000 || c - m.hmin > 1000000) return fail(KPZB_EINVAL, "heights exceed three int8 limbs");
     GCU(analysis_heights(d_cbbit, g->lx, g->ly, &g->an, g->d_heights, g->st), "snapshot heights");
     const int grid = (int)std::min<uint64_t>(g->N / 16 / 256 + 1, (uint64_t)g->sm_count * 8);
-    limb_kernel<<<grid, 256, 0, g->st>>>(g->d_heights, g->N, (int32_t)c, g->d_limbs + (uint64_t)s * g->N,
-                                         64ull * g->N, g->d_sums + 3 * s,
+    limb_kernel<<<grid, 256, 0, g->st>>>(g->d_heights, g->N, (int32_t)c, g->d_limbs, s, g->d_sums + 3 * s,
                                          reinterpret_cast<unsigned int*>(g->d_sums + 192));
     GCU(cudaGetLastError(), "limb_kernel");
     unsigned long long flag = 0;
@@ -273,7 +283,7 @@ extern "C" kpzb_status kpzb_gram_compute(kpzb_gram* g, int method, int64_t* G, i
     if (method == 1) {
         GCU(cudaMemsetAsync(g->d_g, 0, 64 * 64 * 8, g->st), "memset G");
         const int grid = (int)std::min<uint64_t>(g->N / G64_KC, (uint64_t)g->sm_count * 4);
-        gram_int64_kernel<<<grid, 256, 0, g->st>>>(g->d_limbs, g->N, g->N, n, g->d_g);
+        gram_int64_kernel<<<grid, 256, 0, g->st>>>(g->d_limbs, g->N, n, g->d_g);
         GCU(cudaGetLastError(), "gram_int64_kernel");
         GCU(cudaMemcpyAsync(gv.data(), g->d_g, 64 * 64 * 8, cudaMemcpyDeviceToHost, g->st), "G copy");
         GCU(cudaStreamSynchronize(g->st), "gram sync");

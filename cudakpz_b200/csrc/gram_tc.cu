@@ -1,8 +1,8 @@
-// gram_tc.cu -- exact int8 limb Gram A A^T (A: 192 x N, K-major) on tcgen05 tensor cores.
+// gram_tc.cu -- exact int8 limb Gram A A^T (A: 192 x N, K-tile-major) on tcgen05 tensor cores.
 //
 // One persistent CTA per SM takes a contiguous K range.  Warp 0 streams 192-row x 128-byte
-// K tiles of A into a ring of shared-memory stages with 2D TMA (SWIZZLE_128B, local HBM
-// only, no multicast); warp 1 allocates 256 TMEM columns and issues, per 32-byte K step,
+// K tiles of A -- each a contiguous 24 KB block of the tile-major limb matrix -- into a ring
+// of shared-memory stages with 2D TMA (SWIZZLE_128B, local HBM only, no multicast); warp 1 allocates 256 TMEM columns and issues, per 32-byte K step,
 //   D1[0:128, 0:192]   += A[0:128]   . A[0:192]^T   (M=128, N=192)
 //   D2[0:128, 0:64]    += A[64:192]  . A[128:192]^T (M=128, N=64)
 // (kind::i8, signed, int32 accumulators in TMEM); together they cover every (row <= col)
@@ -129,7 +129,7 @@ gram_tc_kernel(const __grid_constant__ CUtensorMap tmap, uint64_t nkt, long long
                     break;
                 }
                 mbar_expect_tx(&full[s], TC_STAGE);
-                tma_load_2d(smem + s * TC_STAGE, &tmap, (int)((kt0 + i) * TC_KT), 0, &full[s]);
+                tma_load_2d(smem + s * TC_STAGE, &tmap, 0, (int)((kt0 + i) * TC_ROWS), &full[s]);
                 issued = i + 1;
             }
             // copies still in flight land before the CTA retires (bounded)
@@ -226,8 +226,9 @@ kpzb_status gram_tc_setup(GramTC* tc, const int8_t* d_limbs, uint64_t N, int sm_
                                             cudaEnableDefault, &q);
     if (e != cudaSuccess || !encode || q != cudaDriverEntryPointSuccess)
         return fail(KPZB_ECUDA, "cuTensorMapEncodeTiled unavailable");
-    const cuuint64_t dims[2] = {(cuuint64_t)N, (cuuint64_t)TC_ROWS};
-    const cuuint64_t strides[1] = {(cuuint64_t)N};  // bytes between limb rows
+    // the tile-major matrix as 2D: 128-byte rows, 192 rows per K tile, N / 128 tiles
+    const cuuint64_t dims[2] = {(cuuint64_t)TC_KT, (cuuint64_t)TC_ROWS * (N / TC_KT)};
+    const cuuint64_t strides[1] = {(cuuint64_t)TC_KT};  // bytes between rows
     const cuuint32_t box[2] = {(cuuint32_t)TC_KT, (cuuint32_t)TC_ROWS};
     const cuuint32_t estr[2] = {1, 1};
     CUtensorMap* map = reinterpret_cast<CUtensorMap*>(tc->tmap);

@@ -94,26 +94,44 @@ struct BandGeom {
 // drops the maximum-candidate mask.  The carry crosses groups with shared-memory atomicXor on
 // disjoint bits (bit 0 of the next group's first word; bits 1..31 of this group's), so
 // neighbouring groups of a row may be updated concurrently.
-template <int MODE, bool USEQ, bool COUNT>
-__device__ __forceinline__ void sca_update_group(uint32_t* pTX, uint32_t* pTY, uint32_t* pOX,
-                                                 uint32_t* pOY, uint32_t* nbp, bool shifted,
-                                                 int mode_rt, const Thresh& tp, const Thresh& tq,
-                                                 Key key, uint32_t qgroup, uint32_t step,
-                                                 uint32_t stream, bool count_row,
-                                                 unsigned long long& ndep, unsigned long long& ndes)
+// The words one group update reads (loaded ahead of the update when the caller pipelines rows).
+struct GroupIn {
+    uint4 tX, tY, oX, oY;
+    uint32_t nb;
+};
+
+__device__ __forceinline__ GroupIn sca_load_group(const uint32_t* pTX, const uint32_t* pTY, const uint32_t* pOX,
+                                                  const uint32_t* pOY, const uint32_t* nbp)
 {
-    uint4* ptX = reinterpret_cast<uint4*>(pTX);
-    uint4* ptY = reinterpret_cast<uint4*>(pTY);
-    uint4* poX = reinterpret_cast<uint4*>(pOX);
-    uint4* poY = reinterpret_cast<uint4*>(pOY);
-    const uint4 tX = *ptX, tY = *ptY, oX = *poX, oY = *poY;
+    GroupIn in;
+    in.tX = *reinterpret_cast<const uint4*>(pTX);
+    in.tY = *reinterpret_cast<const uint4*>(pTY);
+    in.oX = *reinterpret_cast<const uint4*>(pOX);
+    in.oY = *reinterpret_cast<const uint4*>(pOY);
+    in.nb = *nbp;
+    return in;
+}
+
+// The update of one group from its loaded words.  Within a half-step a group may be loaded
+// before other groups are stored: an update reads its row's this-X/this-Y/other-X words and
+// the next row's other-Y words and writes the same words, which no other row or group of the
+// half-step reads or writes, except the next group's first other-X word, whose bit 0 it
+// changes by an atomic XOR -- a bit the owner neither reads (the one-bit right shift drops it)
+// nor stores (it XORs its own mask in atomically).
+template <int MODE, bool USEQ, bool COUNT>
+__device__ __forceinline__ void sca_update_loaded(const GroupIn& in, uint32_t* pTX, uint32_t* pTY, uint32_t* pOX,
+                                                  uint32_t* pOY, uint32_t* nbp, bool shifted, int mode_rt,
+                                                  const Thresh& tp, const Thresh& tq, Key key, uint32_t qgroup,
+                                                  uint32_t step, uint32_t stream, bool count_row,
+                                                  unsigned long long& ndep, unsigned long long& ndes)
+{
+    const uint4 tX = in.tX, tY = in.tY, oX = in.oX, oY = in.oY;
     uint4 xX = oX;
     if (shifted) {
-        const uint32_t nb = *nbp;
         xX.x = __funnelshift_r(oX.x, oX.y, 1);
         xX.y = __funnelshift_r(oX.y, oX.z, 1);
         xX.z = __funnelshift_r(oX.z, oX.w, 1);
-        xX.w = __funnelshift_r(oX.w, nb, 1);
+        xX.w = __funnelshift_r(oX.w, in.nb, 1);
     }
     uint4 cp, cq = make_uint4(0, 0, 0, 0);
     cp.x = ~(tX.x | tY.x) & xX.x & oY.x;
@@ -143,9 +161,9 @@ __device__ __forceinline__ void sca_update_group(uint32_t* pTX, uint32_t* pTY, u
         ndep += __popc(m.x & cp.x) + __popc(m.y & cp.y) + __popc(m.z & cp.z) + __popc(m.w & cp.w);
         if (USEQ) ndes += __popc(m.x & cq.x) + __popc(m.y & cq.y) + __popc(m.z & cq.z) + __popc(m.w & cq.w);
     }
-    *ptX = tX ^ m;
-    *ptY = tY ^ m;
-    *poY = oY ^ m;
+    *reinterpret_cast<uint4*>(pTX) = tX ^ m;
+    *reinterpret_cast<uint4*>(pTY) = tY ^ m;
+    *reinterpret_cast<uint4*>(pOY) = oY ^ m;
     if (shifted) {
         atomicXor(pOX, m.x << 1);
         pOX[1] = oX.y ^ __funnelshift_l(m.x, m.y, 1);
@@ -153,8 +171,30 @@ __device__ __forceinline__ void sca_update_group(uint32_t* pTX, uint32_t* pTY, u
         pOX[3] = oX.w ^ __funnelshift_l(m.z, m.w, 1);
         if (m.w >> 31) atomicXor(nbp, 1u);
     } else {
-        *poX = oX ^ m;
+        *reinterpret_cast<uint4*>(pOX) = oX ^ m;
     }
+}
+
+// One 4-word group (128 sites, one Philox group) of one half-step: the rule of
+// kpz/kpzSCABit.cu:179-290 with the masks of kpz/kpzSCABitCores.cu:69-74,139-145.
+// pTX/pTY: this sublattice's X/Y words of the row; pOX: the other sublattice's X words of the
+// row; pOY: the other sublattice's Y words of the next row; nbp: the first word of the next
+// group of the other X row (the one-bit carry of shifted rows).  MODE is a DecMode, or -1 to
+// decide with the runtime mode `mode_rt`; USEQ false when maxima never flip (q = 0), which
+// drops the maximum-candidate mask.  The carry crosses groups with shared-memory atomicXor on
+// disjoint bits (bit 0 of the next group's first word; bits 1..31 of this group's), so
+// neighbouring groups of a row may be updated concurrently.
+template <int MODE, bool USEQ, bool COUNT>
+__device__ __forceinline__ void sca_update_group(uint32_t* pTX, uint32_t* pTY, uint32_t* pOX,
+                                                 uint32_t* pOY, uint32_t* nbp, bool shifted,
+                                                 int mode_rt, const Thresh& tp, const Thresh& tq,
+                                                 Key key, uint32_t qgroup, uint32_t step,
+                                                 uint32_t stream, bool count_row,
+                                                 unsigned long long& ndep, unsigned long long& ndes)
+{
+    const GroupIn in = sca_load_group(pTX, pTY, pOX, pOY, nbp);
+    sca_update_loaded<MODE, USEQ, COUNT>(in, pTX, pTY, pOX, pOY, nbp, shifted, mode_rt, tp, tq, key, qgroup,
+                                         step, stream, count_row, ndep, ndes);
 }
 
 // Runs one band; returns false (after flagging *err) when the TMA load did not complete in

@@ -181,6 +181,22 @@ def build_gpu(cpu_objs: list[str]) -> None:
     subprocess.run([NVCC, "-gencode", "arch=compute_100a,code=sm_100a", "-o", str(OUT / "kpz_ref_gpu"),
                     str(drv), *objs, *cpu, "-Xcompiler", "-pthread", "-lcudart"], check=True)
     print(f"built {OUT / 'kpz_ref_gpu'}")
+    # second build with the reference's single-hit double-tiling inner scheme (KPZ_INNER_DT,
+    # kpz/kpzConst.h:26) instead of its default DBSH (kpz/param.h), the scheme the DT kernel
+    # here follows: a like-for-like statistical comparison of the two DT implementations
+    param = WORK / "kpz/param.h"
+    t = param.read_text()
+    param.write_text(t.replace("#define KPZ_INNER_DD KPZ_INNER_DBSH", "#define KPZ_INNER_DD KPZ_INNER_DT"))
+    objs2 = []
+    for src in GPU_SOURCES:
+        obj = WORK / (Path(src).stem + ".innerdt.cu.o")
+        subprocess.run([NVCC, *flags, "-c", str(WORK / src), "-o", str(obj)], check=True)
+        objs2.append(str(obj))
+    subprocess.run([NVCC, *flags, "-c", str(HERE / "ref_gpu_driver.cu"), "-o", str(drv)], check=True)
+    subprocess.run([NVCC, "-gencode", "arch=compute_100a,code=sm_100a", "-o", str(OUT / "kpz_ref_gpu_innerdt"),
+                    str(drv), *objs2, *cpu, "-Xcompiler", "-pthread", "-lcudart"], check=True)
+    param.write_text(t)
+    print(f"built {OUT / 'kpz_ref_gpu_innerdt'}")
 
 
 def main() -> int:

@@ -12,11 +12,14 @@
 // usage:
 //   kpz_ref_gpu scabit LX P Q WARMUP MCS   warm-up MCS, then MCS timed; prints
 //   kpz_ref_gpu dt LX P Q WARMUP MCS       "<attempted updates/ns> <seconds> <W2>"
+//   kpz_ref_gpu dtcurve LX P Q SEED T1 T2 ...      supplySeed(1, SEED); "<t> <W2> <h>" per time
+//   kpz_ref_gpu scabitcurve LX P Q SEED T1 T2 ...
 #include <chrono>
 #include <cstdio>
 #include <cstdlib>
 #include <iomanip>
 #include <iostream>
+#include <sstream>
 #include <string>
 
 #include "GPURandom.h"
@@ -57,6 +60,35 @@ static int run(int lx, double p, double q, int warm, int n, Kpz::SchedulerServic
     return 0;
 }
 
+// W^2 and <h> at increasing times (a growth curve): "<t> <W2> <h1>" per line.
+template <class Sched>
+static int curve(int lx, double p, double q, int seed, char** ts, int nt, Kpz::SchedulerService::Encoding enc)
+{
+    std::streambuf* keep = std::cout.rdbuf();
+    std::cout.rdbuf(nullptr);
+    Sched s(lx, lx, 0);
+    s.supplySeed(1, seed);
+    s.randomize();
+    s.initHomogeneous(enc);
+    s.pushSystem();
+    s.setPQ(p, q);
+    Kpz::Correlator::setNThreads(1);
+    int t = 0;
+    std::ostringstream out;
+    out << std::setprecision(12);
+    for (int i = 0; i < nt; ++i) {
+        const int target = std::atoi(ts[i]);
+        s.mcsPQSyncRng(target - t);
+        t = target;
+        s.popSystem();
+        const auto r = s.roughness();
+        out << t << ' ' << (double)r.w2 << ' ' << (double)r.h[0] << '\n';
+    }
+    std::cout.rdbuf(keep);
+    std::cout << out.str();
+    return 0;
+}
+
 int main(int argc, char** argv)
 {
     if (argc < 2) {
@@ -72,6 +104,16 @@ int main(int argc, char** argv)
             return run<Kpz::SchedulerSCABit<SLCG64>>(lx, p, q, warm, n, Kpz::SchedulerService::ENC_CBBIT);
         return run<Kpz::SchedulerDT<SLCG64, Kpz::SchedulerDT_LocalLayoutDis>>(lx, p, q, warm, n,
                                                                            Kpz::SchedulerService::ENC_LOCAL);
+    }
+    if ((cmd == "dtcurve" || cmd == "scabitcurve") && argc >= 7) {
+        const int lx = std::atoi(argv[2]);
+        const double p = std::atof(argv[3]), q = std::atof(argv[4]);
+        const int seed = std::atoi(argv[5]);
+        if (cmd == "scabitcurve")
+            return curve<Kpz::SchedulerSCABit<SLCG64>>(lx, p, q, seed, argv + 6, argc - 6,
+                                                       Kpz::SchedulerService::ENC_CBBIT);
+        return curve<Kpz::SchedulerDT<SLCG64, Kpz::SchedulerDT_LocalLayoutDis>>(lx, p, q, seed, argv + 6, argc - 6,
+                                                                              Kpz::SchedulerService::ENC_LOCAL);
     }
     std::cerr << "unknown command " << cmd << "\n";
     return 2;

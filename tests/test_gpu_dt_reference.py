@@ -1,0 +1,56 @@
+"""DT statistics against the reference's own GPU DT scheduler (config C3: W^2(t) and beta
+within error bars).  The reference's SchedulerDT<SLCG64, dis> with its single-hit
+double-tiling inner scheme (KPZ_INNER_DT, kpz/kpzSimulationPrimitivesTemplates.cu:108-141 --
+the scheme the DT kernel here follows) is built from the CudaKpz sources by
+oracle/build_ref.py into oracle/_ref/kpz_ref_gpu_innerdt and run on the same GPU; both
+implementations use independent random streams, so the comparison is statistical: the
+seed-averaged W^2 at t = 2^k and the fitted growth exponent must agree within their
+standard errors (|z| < 4.5 at every time, beta within 4 sigma)."""
+import subprocess
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+REF = Path(__file__).resolve().parent.parent / "oracle" / "_ref" / "kpz_ref_gpu_innerdt"
+LX, SEEDS, P, Q = 11, 12, 0.95, 0.05
+TS = [2 ** i for i in range(10)]
+
+
+def beta_of(w2):
+    t = np.array(TS, dtype=float)
+    sel = t >= 16
+    return np.polyfit(np.log(t[sel]), np.log(w2[sel]), 1)[0] / 2
+
+
+@pytest.mark.skipif(not REF.exists(), reason="reference GPU DT not built (needs the CudaKpz sources)")
+def test_dt_statistics_match_reference_gpu_dt(kpzb):
+    ref = []
+    for s in range(1, SEEDS + 1):
+        r = subprocess.run([str(REF), "dtcurve", str(LX), str(P), str(Q), str(s)] + [str(t) for t in TS],
+                           capture_output=True, text=True, check=True, timeout=600)
+        rows = [ln.split() for ln in r.stdout.splitlines() if ln and not ln.startswith("#")]
+        assert [int(x[0]) for x in rows] == TS
+        ref.append([float(x[1]) for x in rows])
+    ours = []
+    for s in range(1, SEEDS + 1):
+        h = kpzb.Scheduler(LX, LX, scheduler="dt")
+        h.setPQ(P, Q)
+        h.supplySeed(1000 + s)
+        t, cur = 0, []
+        for T in TS:
+            h.mcsPQSyncRng(T - t)
+            t = T
+            cur.append(h.roughness().w2)
+        ours.append(cur)
+        h.close()
+    ref, ours = np.array(ref), np.array(ours)
+    m_r, m_o = ref.mean(0), ours.mean(0)
+    se = np.sqrt(ref.var(0, ddof=1) / SEEDS + ours.var(0, ddof=1) / SEEDS)
+    z = (m_o - m_r) / se
+    assert np.all(np.abs(z) < 4.5), (z, m_o, m_r)
+    b_r = np.array([beta_of(x) for x in ref])
+    b_o = np.array([beta_of(x) for x in ours])
+    sb = np.sqrt(b_r.var(ddof=1) / SEEDS + b_o.var(ddof=1) / SEEDS)
+    assert abs(b_o.mean() - b_r.mean()) < 4 * sb + 1e-3, (b_o.mean(), b_r.mean(), sb)

@@ -14,6 +14,7 @@
 //   kpz_ref_gpu dt LX P Q WARMUP MCS       "<attempted updates/ns> <seconds> <W2>"
 //   kpz_ref_gpu dtcurve LX P Q SEED T1 T2 ...      supplySeed(1, SEED); "<t> <W2> <h>" per time
 //   kpz_ref_gpu scabitcurve LX P Q SEED T1 T2 ...
+//   kpz_ref_gpu scabitdump LX P Q N FILE          lattice words after N MCS (flat start)
 #include <chrono>
 #include <cstdio>
 #include <cstdlib>
@@ -104,6 +105,29 @@ int main(int argc, char** argv)
             return run<Kpz::SchedulerSCABit<SLCG64>>(lx, p, q, warm, n, Kpz::SchedulerService::ENC_CBBIT);
         return run<Kpz::SchedulerDT<SLCG64, Kpz::SchedulerDT_LocalLayoutDis>>(lx, p, q, warm, n,
                                                                            Kpz::SchedulerService::ENC_LOCAL);
+    }
+    if (cmd == "scabitdump" && argc >= 7) {
+        // the lattice words after N MCS from the flat start (deterministic rates only)
+        const int lx = std::atoi(argv[2]);
+        const double p = std::atof(argv[3]), q = std::atof(argv[4]);
+        const int n = std::atoi(argv[5]);
+        std::streambuf* keep = std::cout.rdbuf();
+        std::cout.rdbuf(nullptr);
+        Kpz::SchedulerSCABit<SLCG64> s(lx, lx, 0);
+        s.supplySeed(1, 1);
+        s.randomize();
+        s.initHomogeneous(Kpz::SchedulerService::ENC_CBBIT);
+        s.pushSystem();
+        s.setPQ(p, q);
+        s.mcsPQSyncRng(n);
+        s.popSystem();
+        std::cout.rdbuf(keep);
+        FILE* f = std::fopen(argv[6], "wb");
+        if (!f) return 3;
+        const size_t nw = s.size().sizeW();
+        const bool ok = std::fwrite(s.system(), 4, nw, f) == nw;
+        std::fclose(f);
+        return ok ? 0 : 3;
     }
     if ((cmd == "dtcurve" || cmd == "scabitcurve") && argc >= 7) {
         const int lx = std::atoi(argv[2]);

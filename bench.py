@@ -59,7 +59,7 @@ def parse():
     ap.add_argument("--reference-gpu", action="store_true",
                     help="with --impl reference: time the reference's own CUDA scheduler on this GPU "
                          "(oracle/_ref/kpz_ref_gpu) instead of its CPU scheduler")
-    ap.add_argument("--workload", choices=["scabit", "dt", "batch", "gram"], default="scabit",
+    ap.add_argument("--workload", choices=["scabit", "dt", "batch", "gram", "measure"], default="scabit",
                     help="scabit: the headline 16384^2 SCA runs; dt / batch / gram: the other configs")
     return ap.parse_args()
 
@@ -333,7 +333,8 @@ def alu_ops_per_word(p, q):
 
 def run_e2e(args, torch, kpzb, scheds, N, M, world):
     """Public API with host buffers: push (pinned H2D) -> mcs -> pop (D2H) -> roughness, every
-    step, both lattices, through the asynchronous push/pop entry points."""
+    step, both lattices, through the asynchronous push/pop entry points; each step's W^2 is
+    read while the other lattice's step runs."""
     import numpy as np
     nw = scheds[0].size_words()
     host = [torch.empty(nw, dtype=torch.int32).pin_memory() for _ in scheds]
@@ -348,13 +349,24 @@ def run_e2e(args, torch, kpzb, scheds, N, M, world):
     torch.cuda.synchronize()
     barrier(world)
     t0 = time.perf_counter()
+    L = len(scheds)
+    unread = [False] * L
     for _ in range(steps):
-        # each lattice on its own stream: one lattice's copies overlap the other's MCS
-        for h, o, s in zip(host, outs, scheds):
+        # each lattice on its own stream; after enqueueing one lattice's step (push, MCS, pop)
+        # the host reads the previous lattice's W^2 while this one runs, so copies and reads
+        # overlap the other lattice's MCS across step boundaries too
+        for j, (h, o, s) in enumerate(zip(host, outs, scheds)):
             s.pushSystemAsync(h.numpy().view(np.uint32))
             s.mcsPQSyncRngAsync(M)
             s.popSystemAsync(o.numpy().view(np.uint32))
-        for s in scheds:
+            unread[j] = True
+            prev = (j - 1) % L  # with one lattice: itself, read at once
+            if unread[prev]:
+                scheds[prev].join()
+                scheds[prev].roughness()
+                unread[prev] = False
+    for j, s in enumerate(scheds):  # every step's result is read before the clock stops
+        if unread[j]:
             s.join()
             s.roughness()
     torch.cuda.synchronize()
@@ -616,6 +628,68 @@ def run_batch(args, world, rank, local):
                  timing="host wall clock around synchronous batch calls")
 
 
+def run_measure(args, world, rank, local):
+    """Row f1 (measurement scheduling): a 16384^2 SCABit run at (1/2,1/2) to --mcs-per-step x
+    10 MCS measured on the reference's default exponential schedule (SamplingParam::makeExp(0,
+    0.1), kpz/sampling.h:84-100) three ways: kpzb_measure_run (MCS chunks and height reductions
+    enqueued back to back, one record copy at the end); the frontend loop of
+    kpz/kpzScaling.cpp:194-215 with the analysis on the device (kpzb_mcs + kpzb_roughness per
+    sample); and the same loop with the reference's lattice pop per sample (64 MiB D2H, the
+    host analysis itself not counted).  value = attempted updates/ns of the first."""
+    import numpy as np
+    import torch
+    torch.cuda.set_device(local)
+    import cudakpz_b200 as kpzb
+    lx = args.lx or LX
+    end = args.mcs_per_step * 10
+    smp = kpzb.make_sampling("exp", density=0.1)
+    times = kpzb.sample_times(0, end, smp)
+    N = float(1 << (2 * lx))
+
+    def fresh():
+        s = kpzb.Scheduler(lx, lx, scheduler="scaBit", device=local)
+        s.setPQ(0.5, 0.5)
+        s.supplySeed(SEED, rank)
+        s.fusion()  # resolve the pass plan (tuner) outside the timed region
+        return s
+
+    out = {}
+    for mode in ("measure_run", "device_roughness_loop", "pop_loop"):
+        best = None
+        for rep in range(max(1, args.warmup // 3) + 1):  # first repetition warms up
+            s = fresh()
+            # pinned, as the reference registers its host lattice (kpz/schedulerBase.cu:76-80)
+            host = torch.empty(s.size_words(), dtype=torch.int32).pin_memory().numpy().view(np.uint32)
+            torch.cuda.synchronize()
+            barrier(world)
+            t0 = time.perf_counter()
+            if mode == "measure_run":
+                rows = s.measureRun(end, smp)
+            else:
+                t = 0
+                for T in times:
+                    s.mcsPQSyncRng(int(T) - t)
+                    t = int(T)
+                    if mode == "device_roughness_loop":
+                        s.roughness()
+                    else:
+                        s.popSystem(host)
+            torch.cuda.synchronize()
+            dt = max_over_ranks(time.perf_counter() - t0, world)
+            s.close()
+            if rep > 0 or max(1, args.warmup // 3) == 0:
+                best = dt if best is None else min(best, dt)
+        out[mode] = N * end * world / (best * 1e9)
+        if mode == "measure_run":
+            best_run = best
+    return _line(out["measure_run"], best_run * 1e3, args, world,
+                 {"workload": f"SCABit {1 << lx}^2 (0.5,0.5) to t={end}, exp sampling density 0.1 "
+                              f"({len(times)} measurements)", "parallelism": f"replicas x{world}"},
+                 device_roughness_loop=round(out["device_roughness_loop"], 1),
+                 pop_loop=round(out["pop_loop"], 1), measurements=int(len(times)),
+                 timing="host wall clock around each whole run (includes every measurement)")
+
+
 def run_gram(args, world, rank, local):
     """Config C5: exact height autocorrelator, 64 snapshots of a 16384^2 SCA run at p=1 q=0
     (snapshots after MCS 1..64), full 64x64 Gram over 2^28 sites on tcgen05 INT8 vs int64."""
@@ -668,7 +742,7 @@ def main():
     args = parse()
     world, rank, local = dist_setup(args.gpus)
     if args.workload != "scabit" and args.impl == "ours":
-        fn = {"dt": run_dt, "batch": run_batch, "gram": run_gram}[args.workload]
+        fn = {"dt": run_dt, "batch": run_batch, "gram": run_gram, "measure": run_measure}[args.workload]
         line = fn(args, world, rank, local)
         if rank == 0:
             print(json.dumps(line), flush=True)

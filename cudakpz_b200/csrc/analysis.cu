@@ -241,18 +241,33 @@ walk_kernel(const uint32_t* __restrict__ sys, const uint32_t* __restrict__ snap,
     }
 }
 
-__global__ void final_reduce_kernel(const Partial* __restrict__ partials, int n, Partial* out)
+// Sum of the per-CTA partials in a fixed order (so repeated runs agree bit for bit): thread t
+// adds partials t, t + 256, ... in turn, then a fixed pairwise tree over the 256 threads.
+constexpr int FR_THREADS = 256;
+
+__device__ __forceinline__ void merge_partial(Partial& p, const Partial& q)
 {
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
-    Partial p = partials[0];
-    for (int i = 1; i < n; ++i) {
-        const Partial& q = partials[i];
-        p.s1 += q.s1; p.s2 += q.s2; p.cross += q.cross; p.agree += q.agree;
-        p.snap_s1 += q.snap_s1;
-        p.hmin = min(p.hmin, q.hmin); p.hmax = max(p.hmax, q.hmax);
-        for (int k = 0; k < 5; ++k) p.s[k] += q.s[k];
+    p.s1 += q.s1; p.s2 += q.s2; p.cross += q.cross; p.agree += q.agree;
+    p.snap_s1 += q.snap_s1;
+    p.hmin = min(p.hmin, q.hmin); p.hmax = max(p.hmax, q.hmax);
+    for (int k = 0; k < 5; ++k) p.s[k] += q.s[k];
+}
+
+__global__ void __launch_bounds__(FR_THREADS) final_reduce_kernel(const Partial* __restrict__ partials, int n,
+                                                                  Partial* out)
+{
+    __shared__ Partial red[FR_THREADS];
+    Partial p{};
+    p.hmin = 0x7fffffffffffffffll;
+    p.hmax = -0x7fffffffffffffffll;
+    for (int i = threadIdx.x; i < n; i += FR_THREADS) merge_partial(p, partials[i]);
+    red[threadIdx.x] = p;
+    __syncthreads();
+    for (int w = FR_THREADS / 2; w > 0; w >>= 1) {
+        if ((int)threadIdx.x < w) merge_partial(red[threadIdx.x], red[threadIdx.x + w]);
+        __syncthreads();
     }
-    *out = p;
+    if (threadIdx.x == 0) *out = red[0];
 }
 
 cudaError_t analysis_alloc(AnalysisScratch* s, int ly)
@@ -331,7 +346,7 @@ cudaError_t analysis_moments_record(const uint32_t* d_sys, const uint32_t* d_sna
         walk_kernel<0><<<grid, AN_THREADS, 0, st>>>(d_sys, nullptr, lx, ly, ri, rs, nullptr,
                                                     nullptr, nullptr, parts);
     }
-    final_reduce_kernel<<<1, 32, 0, st>>>(parts, grid, reinterpret_cast<Partial*>(d_rec));
+    final_reduce_kernel<<<1, FR_THREADS, 0, st>>>(parts, grid, reinterpret_cast<Partial*>(d_rec));
     return cudaGetLastError();
 }
 
@@ -356,7 +371,7 @@ cudaError_t analysis_moments(const uint32_t* d_sys, const uint32_t* d_snap, int 
         walk_kernel<0><<<grid, AN_THREADS, 0, st>>>(d_sys, nullptr, lx, ly, ri, rs, nullptr,
                                                     nullptr, nullptr, parts);
     }
-    final_reduce_kernel<<<1, 32, 0, st>>>(parts, grid, fin);
+    final_reduce_kernel<<<1, FR_THREADS, 0, st>>>(parts, grid, fin);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     Partial h;
     if ((e = cudaMemcpyAsync(&h, fin, sizeof(Partial), cudaMemcpyDeviceToHost, st)) != cudaSuccess)

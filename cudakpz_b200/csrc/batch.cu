@@ -75,6 +75,8 @@ batch_pass_kernel(const RepDesc* __restrict__ reps, const Item* __restrict__ ite
         const BandCtl ctl{&bar, &abort_flag, phase};
         const BandGeom g{r.buf[par], r.buf[par ^ 1u], r.lx, r.ly, (int64_t)it.band * r.B, r.B, k,
                          r.resident != 0, t0, r.key, r.stream, r.tp, r.tq};
+        // rates differ between replicas of one launch: the run-time decision mode (a per-item
+        // dispatch to rate-specialised copies measured 2-5 % slower: larger code, more registers)
         if (!scabit_band<-1, true, false, BATCH_THREADS>(smem, ctl, g, nd, nr, &st->err)) return;
         phase ^= 1u;
     }

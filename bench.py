@@ -375,7 +375,7 @@ def run_e2e(args, torch, kpzb, scheds, N, M, world):
     updates = float(N) * M * len(scheds) * steps * world
     return {"value": round(updates / (dt * 1e9), 3), "unit": UNIT,
             "h2d_bytes_per_step": nw * 4 * len(scheds),
-            "d2h_bytes_per_step": (nw * 4 + 64) * len(scheds), "steps": steps}
+            "d2h_bytes_per_step": (nw * 4 + 128) * len(scheds), "steps": steps}  # words + the W^2 record
 
 
 REF_BIN = ROOT / "oracle" / "_ref" / "kpz_ref"

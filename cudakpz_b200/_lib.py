@@ -78,6 +78,8 @@ SIGNATURES = {
     "kpzb_size_words": (C.c_size_t, [_vp]),
     "kpzb_encoding": (C.c_int, [_vp]),
     "kpzb_roughness": (C.c_int, [_vp, _dblp]),
+    "kpzb_roughness_async": (C.c_int, [_vp]),
+    "kpzb_roughness_join": (C.c_int, [_vp, _dblp]),
     "kpzb_roughness_noalloc": (C.c_int, [_vp, C.c_int, C.c_int, _dblp, _vp]),
     "kpzb_height_sums": (C.c_int, [_vp, _i64p, _i64p]),
     "kpzb_corr_tag": (C.c_int, [_vp, _dblp]),

@@ -61,6 +61,11 @@ struct kpzb_handle {
     // quenched disorder: rate-class words (ENC_LOCAL for DT, ENC_CBBIT form for SCA/SCABit)
     // and the rates of classes 0..3 (class 0 = p, q)
     uint32_t* d_dis = nullptr;
+    // asynchronous roughness (kpzb_roughness_async / kpzb_roughness_join): the reduction's
+    // final record on the device and its pinned host copy
+    void* d_rough = nullptr;
+    void* h_rough = nullptr;
+    bool rough_pending = false;
     double pc[4] = {1.0, 1.0, 1.0, 1.0}, qc[4] = {0.0, 0.0, 0.0, 0.0};
     bool class_set[4] = {true, false, false, false};
     AnalysisScratch an{};
@@ -152,6 +157,8 @@ extern "C" kpzb_status kpzb_destroy(kpzb_handle* h)
     cudaFree(h->d_snap);
     cudaFree(h->d_counters);
     cudaFree(h->d_dis);
+    cudaFree(h->d_rough);
+    if (h->h_rough) cudaFreeHost(h->h_rough);
     if (h->an.rowinfo) analysis_free(&h->an);
     dt_free(&h->dt);
     if (h->own_st) cudaStreamDestroy(h->own_st);
@@ -539,6 +546,35 @@ extern "C" kpzb_status kpzb_roughness(kpzb_handle* h, double out[8])
     MomentsOut m;
     KPZB_CU(analysis_moments(v, nullptr, h->lx, h->ly, &h->an, &m, h->st), "roughness");
     fill_roughness(m, h->lx, h->ly, out, nullptr);
+    return KPZB_OK;
+}
+
+extern "C" kpzb_status kpzb_roughness_async(kpzb_handle* h)
+{
+    KPZB_CHECK_H(h);
+    const size_t rb = analysis_record_bytes();
+    if (!h->d_rough) KPZB_CU(cudaMalloc(&h->d_rough, rb), "cudaMalloc(roughness record)");
+    if (!h->h_rough) KPZB_CU(cudaMallocHost(&h->h_rough, rb), "cudaMallocHost(roughness record)");
+    const uint32_t* v;
+    kpzb_status s = cbbit_view(h, &v);
+    if (s != KPZB_OK) return s;
+    KPZB_CU(analysis_moments_record(v, nullptr, h->lx, h->ly, &h->an, h->d_rough, h->st), "roughness");
+    KPZB_CU(cudaMemcpyAsync(h->h_rough, h->d_rough, rb, cudaMemcpyDeviceToHost, h->st), "roughness record");
+    h->rough_pending = true;
+    return KPZB_OK;
+}
+
+extern "C" kpzb_status kpzb_roughness_join(kpzb_handle* h, double out[8])
+{
+    KPZB_CHECK_H(h);
+    if (!out) return fail(KPZB_EINVAL, "null output");
+    if (!h->rough_pending) return fail(KPZB_ESTATE, "no asynchronous roughness pending");
+    kpzb_status s = kpzb_join(h);
+    if (s != KPZB_OK) return s;
+    MomentsOut m;
+    analysis_decode_record(h->h_rough, &m);
+    fill_roughness(m, h->lx, h->ly, out, nullptr);
+    h->rough_pending = false;
     return KPZB_OK;
 }
 

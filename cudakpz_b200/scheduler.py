@@ -273,6 +273,16 @@ class Scheduler:
         check(lib.kpzb_roughness(self._h, out), "kpzb_roughness")
         return Roughness.from_array(out)
 
+    def roughnessAsync(self) -> None:
+        """SchedulerService::roughnessAsync: enqueue the roughness behind the enqueued work."""
+        check(lib.kpzb_roughness_async(self._h), "kpzb_roughness_async")
+
+    def joinRoughness(self) -> Roughness:
+        """Wait for the handle's stream and return the roughness enqueued by roughnessAsync."""
+        out = (C.c_double * 8)()
+        check(lib.kpzb_roughness_join(self._h, out), "kpzb_roughness_join")
+        return Roughness.from_array(out)
+
     def heightSums(self):
         s = (C.c_int64 * 2)()
         mm = (C.c_int64 * 2)()

@@ -141,6 +141,13 @@ int kpzb_encoding(const kpzb_handle* h);
 /* SchedulerService::roughness (kpz/schedulerService.cpp:292-297, kpz/correlator.cpp:607-697):
  * out[0] = W^2, out[1..7] = <h^k> of the path-relative heights (kpz/correlator.cpp:47-96). */
 kpzb_status kpzb_roughness(kpzb_handle* h, double out[8]);
+/* SchedulerService::roughnessAsync / joinRoughness (kpz/schedulerService.h:150-170): enqueue
+ * the roughness of the lattice as it will be after the work already enqueued, on the handle's
+ * stream, and return at once; kpzb_roughness_join waits for the handle's stream and returns it
+ * (out as kpzb_roughness).  One result is held at a time: a second kpzb_roughness_async before
+ * the join replaces the first. */
+kpzb_status kpzb_roughness_async(kpzb_handle* h);
+kpzb_status kpzb_roughness_join(kpzb_handle* h, double out[8]);
 /* Roughness (as kpzb_roughness) of a caller's device ENC_CBBIT lattice, without allocating:
  * no cudaMalloc/cudaFree or allocating library call; scratch lives in a fixed device array
  * of about 1.2 MB held by every GPU that loads the library.  For callers that cannot

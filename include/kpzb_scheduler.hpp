@@ -139,6 +139,14 @@ public:
         check(kpzb_roughness(h_, o), "kpzb_roughness");
         return toR(o);
     }
+    // SchedulerService::roughnessAsync / joinRoughness
+    void roughnessAsync() { check(kpzb_roughness_async(h_), "kpzb_roughness_async"); }
+    Roughness joinRoughness()
+    {
+        double o[8];
+        check(kpzb_roughness_join(h_, o), "kpzb_roughness_join");
+        return toR(o);
+    }
     Roughness correlateTag()
     {
         double o[8];

@@ -89,3 +89,27 @@ def test_measure_run_small_buffer_and_tag_now(kpzb):
     assert not np.isnan(rows[1:, 9]).any()
     assert rows[:, 0].tolist() == [5, 10, 15, 20, 25, 30]
     s.close()
+
+
+@pytest.mark.parametrize("sched", ["scaBit", "sca", "dt"])
+def test_roughness_async_equals_sync(kpzb, sched):
+    """kpzb_roughness_async / kpzb_roughness_join (SchedulerService::roughnessAsync /
+    joinRoughness): the value of the lattice at enqueue time, equal to kpzb_roughness."""
+    lx, ly = (10, 9)
+    s = kpzb.Scheduler(lx, ly, scheduler=sched)
+    s.setPQ(0.7, 0.2)
+    s.supplySeed(4)
+    with pytest.raises(kpzb.KpzbError):
+        s.joinRoughness()  # nothing pending
+    s.mcsPQSyncRngAsync(5)
+    s.roughnessAsync()
+    s.mcsPQSyncRngAsync(3)  # enqueued after: not part of the pending result
+    r_async = s.joinRoughness()
+    s.close()
+    t = kpzb.Scheduler(lx, ly, scheduler=sched)
+    t.setPQ(0.7, 0.2)
+    t.supplySeed(4)
+    t.mcsPQSyncRng(5)
+    r = t.roughness()
+    t.close()
+    assert r_async.w2 == r.w2 and r_async.h == r.h

@@ -54,6 +54,7 @@ SIGNATURES = {
     "kpzb_set_pq": (C.c_int, [_vp, C.c_double, C.c_double]),
     "kpzb_seed": (C.c_int, [_vp, C.c_uint64, C.c_uint32]),
     "kpzb_mcs": (C.c_int, [_vp, C.c_int]),
+    "kpzb_set_dt_inner": (C.c_int, [_vp, C.c_int]),
     "kpzb_set_pq_class": (C.c_int, [_vp, C.c_int, C.c_double, C.c_double]),
     "kpzb_set_disorder": (C.c_int, [_vp, _vp]),
     "kpzb_mcs_disorder": (C.c_int, [_vp, C.c_int]),

@@ -189,6 +189,15 @@ extern "C" kpzb_status kpzb_set_pq(kpzb_handle* h, double p, double q)
     return KPZB_OK;
 }
 
+extern "C" kpzb_status kpzb_set_dt_inner(kpzb_handle* h, int inner)
+{
+    if (!h) return fail(KPZB_EINVAL, "null handle");
+    if (h->dyn != KPZB_DYN_DT) return fail(KPZB_EUNSUPPORTED, "the inner decomposition applies to DT handles");
+    if (inner != KPZB_DT_INNER_DT && inner != KPZB_DT_INNER_DBSH) return fail(KPZB_EINVAL, "unknown DT inner scheme");
+    h->dt.scheme = inner == KPZB_DT_INNER_DBSH ? DT_SCHEME_DBSH : DT_SCHEME_DT;
+    return KPZB_OK;
+}
+
 extern "C" kpzb_status kpzb_set_pq_class(kpzb_handle* h, int n, double p, double q)
 {
     if (!h) return fail(KPZB_EINVAL, "null handle");

@@ -25,6 +25,8 @@ namespace kpzb {
 
 constexpr uint32_t TAG_DT_SUB = 4u;
 constexpr uint32_t TAG_DT_POS = 5u;
+constexpr uint32_t TAG_DBSH_ORIGIN = 7u;
+constexpr uint32_t TAG_DBSH_POS = 8u;
 constexpr int DT_TX = 32, DT_TY = 16;
 constexpr int DT_BXW = 64, DT_BYW = 32;           // block in words
 constexpr int DT_BX = 4 * DT_BXW, DT_BY = 4 * DT_BYW;  // block in sites
@@ -34,7 +36,7 @@ constexpr int DT_ROUNDS = 64;
 // DIS: quenched disorder (Disorder2SyncRng_shared, kpz/kpzSimulationPrimitivesTemplates.cu:
 // 295-382): dis holds every site's 2-bit rate class in ENC_LOCAL words, copied into a second
 // shared tile beside the lattice's; the class picks dr.tp[c] / dr.tq[c].
-template <bool COUNT, bool DIS>
+template <bool COUNT, bool DIS, bool DBSH>
 __global__ void __launch_bounds__(DT_TX* DT_TY)
 dt_kernel(uint32_t* __restrict__ sys, int lxw, int lyw, int lnbx, int nblocks, int ox, int oy,
           int d, uint32_t t, Key key, uint32_t stream, Thresh tp, Thresh tq,
@@ -85,7 +87,69 @@ dt_kernel(uint32_t* __restrict__ sys, int lxw, int lyw, int lnbx, int nblocks, i
         const uint32_t cid = (uint32_t)b * (DT_TX * DT_TY) + (uint32_t)tid;
         __syncthreads();
         uint4 pos = make_uint4(0, 0, 0, 0), uu = make_uint4(0, 0, 0, 0);
-        for (int rb = 0; rb < DT_ROUNDS; rb += 8) {
+        if (DBSH) {
+            // the reference's default inner scheme (BaseDTInnerDBSH::systemLoopDC,
+            // kpz/kpzSimulationPrimitivesTemplates_BaseInnerDB.cu:110-163): per round one
+            // block-wide offset shifts every thread cell, each thread picks a site of its shifted
+            // cell, and sites on a cell's last column/row wait for phases 1 (off the corner) and
+            // 2 (the corner); the flips use shared-memory atomics as the reference's do
+            const int ax = ox & 3, ay = oy & 3;
+            for (int rb = 0; rb < DT_ROUNDS; rb += 16) {
+                const uint4 ow = philox4x32_10(
+                    make_uint4((uint32_t)b, t, (TAG_DBSH_ORIGIN << 24) | ((uint32_t)d << 16) | (uint32_t)(rb >> 4),
+                               stream), key);
+                const uint4 pw = philox4x32_10(
+                    make_uint4(cid, t, (TAG_DBSH_POS << 24) | ((uint32_t)d << 16) | (uint32_t)(rb >> 4), stream),
+                    key);
+#pragma unroll 4
+                for (int j = 0; j < 16; ++j) {
+                    const int r = rb + j;
+                    if (need_u && (j & 3) == 0)
+                        uu = philox4x32_10(
+                            make_uint4(cid, t, (TAG_DT << 24) | ((uint32_t)d << 16) | (uint32_t)(r >> 2), stream), key);
+                    const uint32_t owd = (j >> 2) == 0 ? ow.x : (j >> 2) == 1 ? ow.y : (j >> 2) == 2 ? ow.z : ow.w;
+                    const uint32_t pwd = (j >> 2) == 0 ? pw.x : (j >> 2) == 1 ? pw.y : (j >> 2) == 2 ? pw.z : pw.w;
+                    const uint32_t ob = (owd >> (8 * (j & 3))) & 0xFFu, pb = (pwd >> (8 * (j & 3))) & 0xFFu;
+                    const int px = (int)(pb & 7u), py = (int)((pb >> 3) & 7u);
+                    const int ph = (px == 7 && py == 7) ? 2 : (px == 7 || py == 7) ? 1 : 0;
+                    const int xt = (threadIdx.x * 8 + ax + px + (int)(ob & 7u)) & (DT_BX - 1);
+                    const int yt = (threadIdx.y * 8 + ay + py + (int)((ob >> 3) & 7u)) & (DT_BY - 1);
+                    const int wi = (yt >> 2) * DT_TW + (xt >> 2);
+                    const uint32_t sh = (uint32_t)(((xt & 3) << 1) | ((yt & 3) << 3));
+                    const int wr = (yt >> 2) * DT_TW + ((xt + 1) >> 2);
+                    const uint32_t shr = (uint32_t)((((xt + 1) & 3) << 1) | ((yt & 3) << 3));
+                    const int wd = ((yt + 1) >> 2) * DT_TW + (xt >> 2);
+                    const uint32_t shd = (uint32_t)(((xt & 3) << 1) | (((yt + 1) & 3) << 3) | 1);
+                    const uint32_t u = (j & 3) == 0 ? uu.x : (j & 3) == 1 ? uu.y : (j & 3) == 2 ? uu.z : uu.w;
+                    for (int phase = 0; phase < 3; ++phase) {
+                        if (ph == phase) {
+                            const uint32_t c = (tile[wi] >> sh) & 3u, rbit = (tile[wr] >> shr) & 1u,
+                                           lbit = (tile[wd] >> shd) & 1u;
+                            const bool is_p = c == 0u && rbit && lbit, is_q = c == 3u && !rbit && !lbit;
+                            bool flip = false;
+                            if (is_p || is_q) {
+                                int cls = 0;
+                                if (DIS) cls = (int)((dtile[wi] >> sh) & 3u);
+                                const Thresh& th = DIS ? (is_p ? dr.tp[cls] : dr.tq[cls]) : (is_p ? tp : tq);
+                                if (th.always) flip = true;
+                                else if (th.planes) flip = u < th.t;
+                            }
+                            if (flip) {
+                                atomicXor(&tile[wi], 3u << sh);
+                                atomicXor(&tile[wr], 1u << shr);
+                                atomicXor(&tile[wd], 1u << shd);
+                                if (COUNT) {
+                                    if (is_p) ++ndep;
+                                    else ++ndes;
+                                }
+                            }
+                        }
+                        __syncthreads();
+                    }
+                }
+            }
+        }
+        for (int rb = 0; !DBSH && rb < DT_ROUNDS; rb += 8) {
             if ((rb & 31) == 0)
                 pos = philox4x32_10(
                     make_uint4(cid, t, (TAG_DT_POS << 24) | ((uint32_t)d << 16) | (uint32_t)(rb >> 5), stream),
@@ -238,23 +302,21 @@ kpzb_status dt_enqueue(DtState* s, uint32_t* d_local, int lx, int ly, uint64_t t
         int ox, oy, order[4];
         dt_plan(seed, stream, t, &ox, &oy, order);
         for (int a = 0; a < 4; ++a) {
-            if (dis) {
-                if (d_counters)
-                    dt_kernel<true, true><<<s->grid, block, 0, st>>>(d_local, lx - 2, ly - 2, lnbx, nblocks, ox,
-                                                                     oy, order[a], t, key, stream, tp, tq,
-                                                                     d_counters, dis, dr);
-                else
-                    dt_kernel<false, true><<<s->grid, block, 0, st>>>(d_local, lx - 2, ly - 2, lnbx, nblocks,
-                                                                      ox, oy, order[a], t, key, stream, tp, tq,
-                                                                      nullptr, dis, dr);
-            } else if (d_counters) {
-                dt_kernel<true, false><<<s->grid, block, 0, st>>>(d_local, lx - 2, ly - 2, lnbx, nblocks, ox,
-                                                                  oy, order[a], t, key, stream, tp, tq,
-                                                                  d_counters, nullptr, dr);
+            auto go = [&](auto kern) {
+                kern<<<s->grid, block, 0, st>>>(d_local, lx - 2, ly - 2, lnbx, nblocks, ox, oy, order[a], t, key,
+                                                 stream, tp, tq, d_counters, dis, dr);
+            };
+            const bool c = d_counters != nullptr, ds = dis != nullptr, sh = s->scheme == DT_SCHEME_DBSH;
+            if (sh) {
+                if (c && ds) go(dt_kernel<true, true, true>);
+                else if (c) go(dt_kernel<true, false, true>);
+                else if (ds) go(dt_kernel<false, true, true>);
+                else go(dt_kernel<false, false, true>);
             } else {
-                dt_kernel<false, false><<<s->grid, block, 0, st>>>(d_local, lx - 2, ly - 2, lnbx, nblocks, ox,
-                                                                   oy, order[a], t, key, stream, tp, tq, nullptr,
-                                                                   nullptr, dr);
+                if (c && ds) go(dt_kernel<true, true, false>);
+                else if (c) go(dt_kernel<true, false, false>);
+                else if (ds) go(dt_kernel<false, true, false>);
+                else go(dt_kernel<false, false, false>);
             }
         }
         const cudaError_t e = cudaGetLastError();

@@ -40,9 +40,11 @@ cudaError_t tune_plan(uint32_t* d_src, int lx, int ly, uint64_t seed, uint32_t s
 void philox_host(const uint32_t ctr[4], uint64_t seed, uint32_t out[4]);
 
 // Double-tiling random-sequential scheduler state (dt.cu).
+enum DtScheme { DT_SCHEME_DT = 0, DT_SCHEME_DBSH = 1 };
 struct DtState {
     int grid = 0;
     bool ready = false;
+    int scheme = DT_SCHEME_DT;  // inner decomposition of a block
 };
 kpzb_status dt_init(DtState* s, int lx, int ly, int sm_count);
 void dt_free(DtState* s);

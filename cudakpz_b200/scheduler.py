@@ -105,6 +105,11 @@ class Scheduler:
             check(lib.kpzb_set_pq_class(self._h, n, p, q), "kpzb_set_pq_class")
         return True
 
+    def setDtInner(self, inner: str) -> None:
+        """DT handles: "dt" (single-hit double tiling, default) or "dbsh" (the reference's
+        default single-hit dead border inner decomposition)."""
+        check(lib.kpzb_set_dt_inner(self._h, {"dt": 0, "dbsh": 1}[inner]), "kpzb_set_dt_inner")
+
     def setDisorder(self, words: np.ndarray) -> None:
         """Quenched disorder classes, ENC_LOCAL words (SchedulerService::m_disorder)."""
         w = np.ascontiguousarray(words, dtype=np.uint32)

@@ -474,6 +474,97 @@ void ko_dt_mcs_dis(uint32_t* w, int lx, int ly, uint64_t seed, uint32_t stream, 
     if (des) *des += nr;
 }
 
+/* One attempt of the RS rule at global site (x, y) with acceptance word u (used only when
+ * the threshold is strictly between 0 and 2^32); class from dis. */
+static void dt_attempt(uint32_t* w, int lx, int ly, int x, int y, const uint64_t* Tpc, const uint64_t* Tqc,
+                       const uint32_t* dis, uint32_t u, int64_t* nd, int64_t* nr)
+{
+    const int L = 1 << lx, M = 1 << ly;
+    const int c = ko_local_get(w, lx, x, y);
+    const int rr = ko_local_get(w, lx, (x + 1) & (L - 1), y) & 1;
+    const int ll = (ko_local_get(w, lx, x, (y + 1) & (M - 1)) >> 1) & 1;
+    const int config = c | (rr << 2) | (ll << 3);
+    const int cls = dis ? ko_local_get(dis, lx, x, y) : 0;
+    uint64_t T;
+    if (config == 12) T = Tpc[cls];
+    else if (config == 3) T = Tqc[cls];
+    else return;
+    if (T == 0) return;
+    if (T < ((uint64_t)1 << 32) && (uint64_t)u >= T) return;
+    ko_local_flip(w, lx, x, y, 3);
+    ko_local_flip(w, lx, (x + 1) & (L - 1), y, 1);
+    ko_local_flip(w, lx, x, (y + 1) & (M - 1), 2);
+    if (config == 12) ++*nd; else ++*nr;
+}
+
+/* DT with the single-hit dead-border inner scheme of the reference's default DT build
+ * (BaseDTInnerDBSH::systemLoopDC, kpz/kpzSimulationPrimitivesTemplates_BaseInnerDB.cu:110-163):
+ * the same blocks, domain sets and origins as ko_dt_mcs_dis; inside a block, every round
+ * shifts all 8x8 thread cells by one block-wide offset (ox_r, oy_r) in [0,8)^2, each thread
+ * picks a site (px, py) in its shifted cell, sites on the cell's last column or row are
+ * delayed: phase 0 interior sites, phase 1 border sites off the corner, phase 2 the corner.
+ * Site coordinates in the block tile are taken modulo the block (256 x 128 sites measured
+ * from the tile's first word), as the reference masks them (`x &= M_BLOCK_DIM_X`).
+ * Counter stream: offset byte r&15 of Philox(ctr=(block, t, TAG_DBSH_ORIGIN<<24 | d<<16 |
+ * r>>4, stream)) word (r&15)>>2 (bits 0-2 x, 3-5 y); the position byte the same from
+ * (cell, t, TAG_DBSH_POS<<24 | d<<16 | r>>4); acceptance u as ko_dt_mcs_dis. */
+void ko_dt_mcs_dbsh(uint32_t* w, int lx, int ly, uint64_t seed, uint32_t stream, uint64_t t0, int n,
+                    const double p[4], const double q[4], const uint32_t* dis, int64_t* dep, int64_t* des)
+{
+    const int L = 1 << lx, M = 1 << ly;
+    const int BX = 256, BY = 128;
+    const int nbx = L / (2 * BX), nby = M / (2 * BY);
+    uint64_t Tpc[4], Tqc[4];
+    for (int c = 0; c < 4; ++c) {
+        Tpc[c] = ko_threshold(p[c]);
+        Tqc[c] = ko_threshold(q[c]);
+    }
+    int64_t nd = 0, nr = 0;
+    for (int i = 0; i < n; ++i) {
+        const uint64_t t = t0 + (uint64_t)i;
+        int ox, oy, order[4];
+        ko_dt_plan(seed, stream, t, &ox, &oy, order);
+        for (int a = 0; a < 4; ++a) {
+            const int d = order[a];
+            for (int b = 0; b < nbx * nby; ++b) {
+                const int bx = b % nbx, by = b / nbx;
+                const int X0 = ox + (2 * bx + (d & 1)) * BX;
+                const int Y0 = oy + (2 * by + (d >> 1)) * BY;
+                for (int r = 0; r < 64; ++r) {
+                    uint32_t ow[4];
+                    philox_u32(seed, (uint32_t)b, (uint32_t)t,
+                               (KO_TAG_DBSH_ORIGIN << 24) | ((uint32_t)d << 16) | (uint32_t)(r >> 4), stream, ow);
+                    const uint32_t ob = (ow[(r & 15) >> 2] >> (8 * (r & 3))) & 0xFFu;
+                    const int orx = (int)(ob & 7u), ory = (int)((ob >> 3) & 7u);
+                    for (int phase = 0; phase < 3; ++phase)
+                        for (int cell = 0; cell < 512; ++cell) {
+                            const int tx = cell & 31, ty = cell >> 5;
+                            const uint32_t cid = (uint32_t)b * 512u + (uint32_t)cell;
+                            uint32_t pw[4];
+                            philox_u32(seed, cid, (uint32_t)t,
+                                       (KO_TAG_DBSH_POS << 24) | ((uint32_t)d << 16) | (uint32_t)(r >> 4), stream,
+                                       pw);
+                            const uint32_t pb = (pw[(r & 15) >> 2] >> (8 * (r & 3))) & 0xFFu;
+                            const int px = (int)(pb & 7u), py = (int)((pb >> 3) & 7u);
+                            const int ph = (px == 7 && py == 7) ? 2 : (px == 7 || py == 7) ? 1 : 0;
+                            if (ph != phase) continue;
+                            const int xt = (tx * 8 + (X0 & 3) + px + orx) & (BX - 1);
+                            const int yt = (ty * 8 + (Y0 & 3) + py + ory) & (BY - 1);
+                            const int x = ((X0 & ~3) + xt) & (L - 1);
+                            const int y = ((Y0 & ~3) + yt) & (M - 1);
+                            uint32_t uw[4];
+                            philox_u32(seed, cid, (uint32_t)t,
+                                       (KO_TAG_DT << 24) | ((uint32_t)d << 16) | (uint32_t)(r >> 2), stream, uw);
+                            dt_attempt(w, lx, ly, x, y, Tpc, Tqc, dis, uw[r & 3], &nd, &nr);
+                        }
+                }
+            }
+        }
+    }
+    if (dep) *dep += nd;
+    if (des) *des += nr;
+}
+
 /* ------------------------------------------------------------------------ */
 /* dSFMT-19937 (vendored BSD third-party code in the reference,             */
 /* inc/dSFMT/dSFMT.{h,cpp}, parameters inc/dSFMT/dSFMT-params19937.h;       */

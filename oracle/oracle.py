@@ -64,6 +64,8 @@ def _load():
                                   C.c_int, dblp, dblp, u32p, i64p, i64p]),
         "ko_dt_mcs_dis": (None, [u32p, C.c_int, C.c_int, C.c_uint64, C.c_uint32, C.c_uint64, C.c_int,
                                  dblp, dblp, u32p, i64p, i64p]),
+        "ko_dt_mcs_dbsh": (None, [u32p, C.c_int, C.c_int, C.c_uint64, C.c_uint32, C.c_uint64, C.c_int,
+                                  dblp, dblp, u32p, i64p, i64p]),
         "ko_generate_disorder2": (None, [u32p, C.c_int, C.c_int, C.c_void_p, C.c_double]),
         "ko_rs_mcs_dis": (None, [u32p, C.c_int, C.c_int, C.c_void_p, C.c_int, dblp, dblp, u32p, i64p,
                                  i64p]),
@@ -154,6 +156,18 @@ def dt_mcs_dis(w: np.ndarray, lx: int, ly: int, seed: int, stream: int, t0: int,
     dep, des = C.c_int64(0), C.c_int64(0)
     lib.ko_dt_mcs_dis(_u32(w), lx, ly, seed, stream, t0, n, _rates4(p), _rates4(q), _u32(dis),
                       C.byref(dep), C.byref(des))
+    return dep.value, des.value
+
+
+def dt_mcs_dbsh(w: np.ndarray, lx: int, ly: int, seed: int, stream: int, t0: int, n: int, p, q,
+                dis: np.ndarray = None):
+    """DT with the reference's default DBSH inner scheme (ENC_LOCAL, in place); (#dep, #des)."""
+    dep, des = C.c_int64(0), C.c_int64(0)
+    d = None if dis is None else _u32(dis)
+    pp = p if isinstance(p, (list, tuple)) else [p]
+    qq = q if isinstance(q, (list, tuple)) else [q]
+    lib.ko_dt_mcs_dbsh(_u32(w), lx, ly, seed, stream, t0, n, _rates4(pp), _rates4(qq), d, C.byref(dep),
+                       C.byref(des))
     return dep.value, des.value
 
 

@@ -120,3 +120,41 @@ def test_dt_statistics_match_random_sequential(kpzb, oracle):
     assert np.all(rel < 0.035), (m1, m2, rel)
     assert abs(mv1 - mv2) / abs(mv2) < 0.01, (mv1, mv2)
     assert abs(b_dt - b_rs) < 0.03, (b_dt, b_rs)
+
+
+@pytest.mark.parametrize("p,q", [(1.0, 0.0), (0.95, 0.05), (0.5, 0.5), (1.0, 1.0)])
+@pytest.mark.parametrize("lx,ly", [(9, 8), (10, 9)])
+def test_dbsh_inner_scheme_bit_exact(kpzb, oracle, lx, ly, p, q):
+    """The reference's default DBSH inner decomposition (three phases per round, shared
+    atomics) against its CPU emulation, word for word, with counters."""
+    n = 3
+    ref = oracle.homogeneous(lx, ly, oracle.ENC_LOCAL)
+    rc = oracle.dt_mcs_dbsh(ref, lx, ly, 42, 0, 0, n, p, q)
+    s = kpzb.Scheduler(lx, ly, scheduler="dt")
+    s.setDtInner("dbsh")
+    s.setPQ(p, q)
+    s.supplySeed(42)
+    s.enableCounters(True)
+    s.mcsPQSyncRng(n)
+    got = s.popSystem()
+    cnt = s.counters()
+    s.close()
+    assert np.array_equal(got, ref)
+    assert cnt == rc
+
+
+def test_dbsh_with_disorder_and_stream(kpzb, oracle):
+    lx, ly = 10, 9
+    dis = oracle.generate_disorder2(lx, ly, oracle.DSFMT(6), 0.4)
+    ref = oracle.homogeneous(lx, ly, oracle.ENC_LOCAL)
+    oracle.dt_mcs_dbsh(ref, lx, ly, 9, 2, 0, 3, [0.9, 0.4], [0.1, 0.5], dis)
+    s = kpzb.Scheduler(lx, ly, scheduler="dt")
+    s.setDtInner("dbsh")
+    s.setPQ(0.9, 0.1)
+    s.setPQ(0.4, 0.5, 1)
+    s.supplySeed(9, 2)
+    s.setDisorder(dis)
+    s.mcsDisorder2SyncRng(3)
+    got = s.popSystem()
+    s.close()
+    assert np.array_equal(got, ref)

@@ -24,11 +24,18 @@ def beta_of(w2):
     return np.polyfit(np.log(t[sel]), np.log(w2[sel]), 1)[0] / 2
 
 
-@pytest.mark.skipif(not REF.exists(), reason="reference GPU DT not built (needs the CudaKpz sources)")
-def test_dt_statistics_match_reference_gpu_dt(kpzb):
+REF_DBSH = REF.parent / "kpz_ref_gpu"
+
+
+@pytest.mark.parametrize("inner,binary", [("dt", REF), ("dbsh", REF_DBSH)])
+def test_dt_statistics_match_reference_gpu_dt(kpzb, inner, binary):
+    """inner "dt": the reference built with KPZ_INNER_DT; "dbsh": its default build
+    (KPZ_INNER_DBSH, kpz/param.h) against this library's DBSH inner scheme."""
+    if not binary.exists():
+        pytest.skip("reference GPU DT not built (needs the CudaKpz sources)")
     ref = []
     for s in range(1, SEEDS + 1):
-        r = subprocess.run([str(REF), "dtcurve", str(LX), str(P), str(Q), str(s)] + [str(t) for t in TS],
+        r = subprocess.run([str(binary), "dtcurve", str(LX), str(P), str(Q), str(s)] + [str(t) for t in TS],
                            capture_output=True, text=True, check=True, timeout=600)
         rows = [ln.split() for ln in r.stdout.splitlines() if ln and not ln.startswith("#")]
         assert [int(x[0]) for x in rows] == TS
@@ -36,6 +43,7 @@ def test_dt_statistics_match_reference_gpu_dt(kpzb):
     ours = []
     for s in range(1, SEEDS + 1):
         h = kpzb.Scheduler(LX, LX, scheduler="dt")
+        h.setDtInner(inner)
         h.setPQ(P, Q)
         h.supplySeed(1000 + s)
         t, cur = 0, []

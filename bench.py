@@ -56,6 +56,8 @@ def parse():
                     help="run only lattice i of the headline pair (profiling a single rate)")
     ap.add_argument("--lx", type=int, default=0,
                     help="override the workload's log2 lattice side (small cases for ncu)")
+    ap.add_argument("--dt-inner", choices=["dt", "dbsh", "db"], default="dt",
+                    help="--workload dt: the DT kernel's inner decomposition (dbsh = the reference's default)")
     ap.add_argument("--reference-gpu", action="store_true",
                     help="with --impl reference: time the reference's own CUDA scheduler on this GPU "
                          "(oracle/_ref/kpz_ref_gpu) instead of its CPU scheduler")
@@ -529,6 +531,7 @@ def run_dt(args, world, rank, local):
     lx = args.lx or 16
     st = torch.cuda.Stream()
     s = kpzb.Scheduler(lx, lx, scheduler="dt", device=local)
+    s.setDtInner(args.dt_inner)
     s.setPQ(0.95, 0.05)
     s.supplySeed(1 + rank)
     s.setStream(st.cuda_stream)
@@ -554,7 +557,8 @@ def run_dt(args, world, rank, local):
     s.close()
     return _line(value, ms / args.steps, args, world,
                  {"workload": f"DT random-sequential {1 << lx}^2 periodic ({N // 4 >> 20} MiB ENC_LOCAL), "
-                              "flat start, p=0.95 q=0.05, random origin + shuffled domain sets per MCS",
+                              f"flat start, p=0.95 q=0.05, random origin + shuffled domain sets per MCS, "
+                              f"inner scheme {args.dt_inner.upper()}",
                   "mcs_per_step": m, "lattice": f"{1 << lx}x{1 << lx}", "parallelism": f"replicas x{world}"},
                  roofline={"bound": "hbm", "kernel": "dt_kernel", "achieved": round(ach, 1), "peak": peak,
                            "unit": "GB/s", "frac": round(ach / peak, 4), "traffic": None,

@@ -193,8 +193,9 @@ extern "C" kpzb_status kpzb_set_dt_inner(kpzb_handle* h, int inner)
 {
     if (!h) return fail(KPZB_EINVAL, "null handle");
     if (h->dyn != KPZB_DYN_DT) return fail(KPZB_EUNSUPPORTED, "the inner decomposition applies to DT handles");
-    if (inner != KPZB_DT_INNER_DT && inner != KPZB_DT_INNER_DBSH) return fail(KPZB_EINVAL, "unknown DT inner scheme");
-    h->dt.scheme = inner == KPZB_DT_INNER_DBSH ? DT_SCHEME_DBSH : DT_SCHEME_DT;
+    if (inner != KPZB_DT_INNER_DT && inner != KPZB_DT_INNER_DBSH && inner != KPZB_DT_INNER_DB)
+        return fail(KPZB_EINVAL, "unknown DT inner scheme");
+    h->dt.scheme = inner == KPZB_DT_INNER_DBSH ? DT_SCHEME_DBSH : inner == KPZB_DT_INNER_DB ? DT_SCHEME_DB : DT_SCHEME_DT;
     return KPZB_OK;
 }
 

@@ -15,6 +15,7 @@
 // MCS).  All random numbers come from the counter stream (see oracle/kpz_oracle.h), so the
 // CPU emulation ko_dt_mcs reproduces every lattice bit for bit.
 #include <cmath>
+#include <type_traits>
 #include <cstring>
 
 #include "kpzb_api_internal.h"
@@ -36,7 +37,9 @@ constexpr int DT_ROUNDS = 64;
 // DIS: quenched disorder (Disorder2SyncRng_shared, kpz/kpzSimulationPrimitivesTemplates.cu:
 // 295-382): dis holds every site's 2-bit rate class in ENC_LOCAL words, copied into a second
 // shared tile beside the lattice's; the class picks dr.tp[c] / dr.tq[c].
-template <bool COUNT, bool DIS, bool DBSH>
+// SCHEME: DT_SCHEME_DT, DT_SCHEME_DBSH or DT_SCHEME_DB (the dead-border phases without the
+// per-round cell offset).
+template <bool COUNT, bool DIS, int SCHEME>
 __global__ void __launch_bounds__(DT_TX* DT_TY)
 dt_kernel(uint32_t* __restrict__ sys, int lxw, int lyw, int lnbx, int nblocks, int ox, int oy,
           int d, uint32_t t, Key key, uint32_t stream, Thresh tp, Thresh tq,
@@ -87,6 +90,7 @@ dt_kernel(uint32_t* __restrict__ sys, int lxw, int lyw, int lnbx, int nblocks, i
         const uint32_t cid = (uint32_t)b * (DT_TX * DT_TY) + (uint32_t)tid;
         __syncthreads();
         uint4 pos = make_uint4(0, 0, 0, 0), uu = make_uint4(0, 0, 0, 0);
+        constexpr bool DBSH = SCHEME != DT_SCHEME_DT;
         if (DBSH) {
             // the reference's default inner scheme (BaseDTInnerDBSH::systemLoopDC,
             // kpz/kpzSimulationPrimitivesTemplates_BaseInnerDB.cu:110-163): per round one
@@ -112,8 +116,10 @@ dt_kernel(uint32_t* __restrict__ sys, int lxw, int lyw, int lnbx, int nblocks, i
                     const uint32_t ob = (owd >> (8 * (j & 3))) & 0xFFu, pb = (pwd >> (8 * (j & 3))) & 0xFFu;
                     const int px = (int)(pb & 7u), py = (int)((pb >> 3) & 7u);
                     const int ph = (px == 7 && py == 7) ? 2 : (px == 7 || py == 7) ? 1 : 0;
-                    const int xt = (threadIdx.x * 8 + ax + px + (int)(ob & 7u)) & (DT_BX - 1);
-                    const int yt = (threadIdx.y * 8 + ay + py + (int)((ob >> 3) & 7u)) & (DT_BY - 1);
+                    const int orx = SCHEME == DT_SCHEME_DB ? 0 : (int)(ob & 7u);
+                    const int ory = SCHEME == DT_SCHEME_DB ? 0 : (int)((ob >> 3) & 7u);
+                    const int xt = (threadIdx.x * 8 + ax + px + orx) & (DT_BX - 1);
+                    const int yt = (threadIdx.y * 8 + ay + py + ory) & (DT_BY - 1);
                     const int wi = (yt >> 2) * DT_TW + (xt >> 2);
                     const uint32_t sh = (uint32_t)(((xt & 3) << 1) | ((yt & 3) << 3));
                     const int wr = (yt >> 2) * DT_TW + ((xt + 1) >> 2);
@@ -306,18 +312,17 @@ kpzb_status dt_enqueue(DtState* s, uint32_t* d_local, int lx, int ly, uint64_t t
                 kern<<<s->grid, block, 0, st>>>(d_local, lx - 2, ly - 2, lnbx, nblocks, ox, oy, order[a], t, key,
                                                  stream, tp, tq, d_counters, dis, dr);
             };
-            const bool c = d_counters != nullptr, ds = dis != nullptr, sh = s->scheme == DT_SCHEME_DBSH;
-            if (sh) {
-                if (c && ds) go(dt_kernel<true, true, true>);
-                else if (c) go(dt_kernel<true, false, true>);
-                else if (ds) go(dt_kernel<false, true, true>);
-                else go(dt_kernel<false, false, true>);
-            } else {
-                if (c && ds) go(dt_kernel<true, true, false>);
-                else if (c) go(dt_kernel<true, false, false>);
-                else if (ds) go(dt_kernel<false, true, false>);
-                else go(dt_kernel<false, false, false>);
-            }
+            const bool c = d_counters != nullptr, ds = dis != nullptr;
+            auto pick = [&](auto scheme_tag) {
+                constexpr int S = decltype(scheme_tag)::value;
+                if (c && ds) go(dt_kernel<true, true, S>);
+                else if (c) go(dt_kernel<true, false, S>);
+                else if (ds) go(dt_kernel<false, true, S>);
+                else go(dt_kernel<false, false, S>);
+            };
+            if (s->scheme == DT_SCHEME_DBSH) pick(std::integral_constant<int, DT_SCHEME_DBSH>{});
+            else if (s->scheme == DT_SCHEME_DB) pick(std::integral_constant<int, DT_SCHEME_DB>{});
+            else pick(std::integral_constant<int, DT_SCHEME_DT>{});
         }
         const cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess) return cuda_fail(e, "dt_kernel");

@@ -40,7 +40,7 @@ cudaError_t tune_plan(uint32_t* d_src, int lx, int ly, uint64_t seed, uint32_t s
 void philox_host(const uint32_t ctr[4], uint64_t seed, uint32_t out[4]);
 
 // Double-tiling random-sequential scheduler state (dt.cu).
-enum DtScheme { DT_SCHEME_DT = 0, DT_SCHEME_DBSH = 1 };
+enum DtScheme { DT_SCHEME_DT = 0, DT_SCHEME_DBSH = 1, DT_SCHEME_DB = 2 };
 struct DtState {
     int grid = 0;
     bool ready = false;

@@ -106,9 +106,9 @@ class Scheduler:
         return True
 
     def setDtInner(self, inner: str) -> None:
-        """DT handles: "dt" (single-hit double tiling, default) or "dbsh" (the reference's
-        default single-hit dead border inner decomposition)."""
-        check(lib.kpzb_set_dt_inner(self._h, {"dt": 0, "dbsh": 1}[inner]), "kpzb_set_dt_inner")
+        """DT handles: "dt" (single-hit double tiling, default), "dbsh" (the reference's
+        default single-hit dead border inner decomposition) or "db" (dead border, no offset)."""
+        check(lib.kpzb_set_dt_inner(self._h, {"dt": 0, "dbsh": 1, "db": 2}[inner]), "kpzb_set_dt_inner")
 
     def setDisorder(self, words: np.ndarray) -> None:
         """Quenched disorder classes, ENC_LOCAL words (SchedulerService::m_disorder)."""

@@ -81,9 +81,10 @@ kpzb_status kpzb_seed(kpzb_handle* h, uint64_t seed, uint32_t stream);
 
 /* DT only: the inner decomposition of a block, the reference's compile-time KPZ_INNER_DD
  * (kpz/param.h, kpz/kpzConst.h:26-35): KPZB_DT_INNER_DT (single-hit double tiling, the
- * default here) or KPZB_DT_INNER_DBSH (single-hit dead border, the reference's default:
- * BaseDTInnerDBSH, kpz/kpzSimulationPrimitivesTemplates_BaseInnerDB.cu:110-163). */
-enum { KPZB_DT_INNER_DT = 0, KPZB_DT_INNER_DBSH = 1 };
+ * default here), KPZB_DT_INNER_DBSH (single-hit dead border, the reference's default:
+ * BaseDTInnerDBSH, kpz/kpzSimulationPrimitivesTemplates_BaseInnerDB.cu:110-163) or
+ * KPZB_DT_INNER_DB (dead border without the per-round cell offset: BaseDTInnerDB, :30-74). */
+enum { KPZB_DT_INNER_DT = 0, KPZB_DT_INNER_DBSH = 1, KPZB_DT_INNER_DB = 2 };
 kpzb_status kpzb_set_dt_inner(kpzb_handle* h, int inner);
 /* SchedulerService::setPQ(p, q, n) for rate class n = 0..3 (kpz/schedulerService.h:186-192):
  * the rates a site of disorder class n uses in kpzb_mcs_disorder; class 0 is kpzb_set_pq's.

@@ -184,19 +184,22 @@ def build_gpu(cpu_objs: list[str]) -> None:
     # second build with the reference's single-hit double-tiling inner scheme (KPZ_INNER_DT,
     # kpz/kpzConst.h:26) instead of its default DBSH (kpz/param.h), the scheme the DT kernel
     # here follows: a like-for-like statistical comparison of the two DT implementations
+    # further builds with the other inner schemes the DT kernel here implements: single-hit
+    # double tiling (KPZ_INNER_DT) and dead border (KPZ_INNER_DB), kpz/kpzConst.h:26-35
     param = WORK / "kpz/param.h"
     t = param.read_text()
-    param.write_text(t.replace("#define KPZ_INNER_DD KPZ_INNER_DBSH", "#define KPZ_INNER_DD KPZ_INNER_DT"))
-    objs2 = []
-    for src in GPU_SOURCES:
-        obj = WORK / (Path(src).stem + ".innerdt.cu.o")
-        subprocess.run([NVCC, *flags, "-c", str(WORK / src), "-o", str(obj)], check=True)
-        objs2.append(str(obj))
-    subprocess.run([NVCC, *flags, "-c", str(HERE / "ref_gpu_driver.cu"), "-o", str(drv)], check=True)
-    subprocess.run([NVCC, "-gencode", "arch=compute_100a,code=sm_100a", "-o", str(OUT / "kpz_ref_gpu_innerdt"),
-                    str(drv), *objs2, *cpu, "-Xcompiler", "-pthread", "-lcudart"], check=True)
+    for tag, dd in (("innerdt", "KPZ_INNER_DT"), ("innerdb", "KPZ_INNER_DB")):
+        param.write_text(t.replace("#define KPZ_INNER_DD KPZ_INNER_DBSH", f"#define KPZ_INNER_DD {dd}"))
+        objs2 = []
+        for src in GPU_SOURCES:
+            obj = WORK / (Path(src).stem + f".{tag}.cu.o")
+            subprocess.run([NVCC, *flags, "-c", str(WORK / src), "-o", str(obj)], check=True)
+            objs2.append(str(obj))
+        subprocess.run([NVCC, *flags, "-c", str(HERE / "ref_gpu_driver.cu"), "-o", str(drv)], check=True)
+        subprocess.run([NVCC, "-gencode", "arch=compute_100a,code=sm_100a", "-o", str(OUT / f"kpz_ref_gpu_{tag}"),
+                        str(drv), *objs2, *cpu, "-Xcompiler", "-pthread", "-lcudart"], check=True)
+        print(f"built {OUT / f'kpz_ref_gpu_{tag}'}")
     param.write_text(t)
-    print(f"built {OUT / 'kpz_ref_gpu_innerdt'}")
 
 
 def main() -> int:

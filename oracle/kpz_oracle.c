@@ -508,8 +508,27 @@ static void dt_attempt(uint32_t* w, int lx, int ly, int x, int y, const uint64_t
  * Counter stream: offset byte r&15 of Philox(ctr=(block, t, TAG_DBSH_ORIGIN<<24 | d<<16 |
  * r>>4, stream)) word (r&15)>>2 (bits 0-2 x, 3-5 y); the position byte the same from
  * (cell, t, TAG_DBSH_POS<<24 | d<<16 | r>>4); acceptance u as ko_dt_mcs_dis. */
+static void dt_mcs_border(uint32_t* w, int lx, int ly, uint64_t seed, uint32_t stream, uint64_t t0, int n,
+                          const double p[4], const double q[4], const uint32_t* dis, int shift, int64_t* dep,
+                          int64_t* des);
+
 void ko_dt_mcs_dbsh(uint32_t* w, int lx, int ly, uint64_t seed, uint32_t stream, uint64_t t0, int n,
                     const double p[4], const double q[4], const uint32_t* dis, int64_t* dep, int64_t* des)
+{
+    dt_mcs_border(w, lx, ly, seed, stream, t0, n, p, q, dis, 1, dep, des);
+}
+
+/* The dead-border scheme without the per-round shift of the cells (BaseDTInnerDB,
+ * kpz/kpzSimulationPrimitivesTemplates_BaseInnerDB.cu:30-74): ko_dt_mcs_dbsh with offset 0. */
+void ko_dt_mcs_db(uint32_t* w, int lx, int ly, uint64_t seed, uint32_t stream, uint64_t t0, int n,
+                  const double p[4], const double q[4], const uint32_t* dis, int64_t* dep, int64_t* des)
+{
+    dt_mcs_border(w, lx, ly, seed, stream, t0, n, p, q, dis, 0, dep, des);
+}
+
+static void dt_mcs_border(uint32_t* w, int lx, int ly, uint64_t seed, uint32_t stream, uint64_t t0, int n,
+                          const double p[4], const double q[4], const uint32_t* dis, int shift, int64_t* dep,
+                          int64_t* des)
 {
     const int L = 1 << lx, M = 1 << ly;
     const int BX = 256, BY = 128;
@@ -535,7 +554,7 @@ void ko_dt_mcs_dbsh(uint32_t* w, int lx, int ly, uint64_t seed, uint32_t stream,
                     philox_u32(seed, (uint32_t)b, (uint32_t)t,
                                (KO_TAG_DBSH_ORIGIN << 24) | ((uint32_t)d << 16) | (uint32_t)(r >> 4), stream, ow);
                     const uint32_t ob = (ow[(r & 15) >> 2] >> (8 * (r & 3))) & 0xFFu;
-                    const int orx = (int)(ob & 7u), ory = (int)((ob >> 3) & 7u);
+                    const int orx = shift ? (int)(ob & 7u) : 0, ory = shift ? (int)((ob >> 3) & 7u) : 0;
                     for (int phase = 0; phase < 3; ++phase)
                         for (int cell = 0; cell < 512; ++cell) {
                             const int tx = cell & 31, ty = cell >> 5;

@@ -119,6 +119,9 @@ void ko_dt_mcs_dis(uint32_t* w, int lx, int ly, uint64_t seed, uint32_t stream, 
 #define KO_TAG_DBSH_POS 8u
 void ko_dt_mcs_dbsh(uint32_t* w, int lx, int ly, uint64_t seed, uint32_t stream, uint64_t t0, int n,
                     const double p[4], const double q[4], const uint32_t* dis, int64_t* dep, int64_t* des);
+/* the dead-border scheme without the per-round cell offset (DB) */
+void ko_dt_mcs_db(uint32_t* w, int lx, int ly, uint64_t seed, uint32_t stream, uint64_t t0, int n,
+                  const double p[4], const double q[4], const uint32_t* dis, int64_t* dep, int64_t* des);
 /* the per-MCS origin (sites) and domain-set order used by ko_dt_mcs */
 void ko_dt_plan(uint64_t seed, uint32_t stream, uint64_t t, int* ox, int* oy, int order[4]);
 

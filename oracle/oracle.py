@@ -66,6 +66,8 @@ def _load():
                                  dblp, dblp, u32p, i64p, i64p]),
         "ko_dt_mcs_dbsh": (None, [u32p, C.c_int, C.c_int, C.c_uint64, C.c_uint32, C.c_uint64, C.c_int,
                                   dblp, dblp, u32p, i64p, i64p]),
+        "ko_dt_mcs_db": (None, [u32p, C.c_int, C.c_int, C.c_uint64, C.c_uint32, C.c_uint64, C.c_int,
+                                dblp, dblp, u32p, i64p, i64p]),
         "ko_generate_disorder2": (None, [u32p, C.c_int, C.c_int, C.c_void_p, C.c_double]),
         "ko_rs_mcs_dis": (None, [u32p, C.c_int, C.c_int, C.c_void_p, C.c_int, dblp, dblp, u32p, i64p,
                                  i64p]),
@@ -160,14 +162,15 @@ def dt_mcs_dis(w: np.ndarray, lx: int, ly: int, seed: int, stream: int, t0: int,
 
 
 def dt_mcs_dbsh(w: np.ndarray, lx: int, ly: int, seed: int, stream: int, t0: int, n: int, p, q,
-                dis: np.ndarray = None):
-    """DT with the reference's default DBSH inner scheme (ENC_LOCAL, in place); (#dep, #des)."""
+                dis: np.ndarray = None, shift: bool = True):
+    """DT with the reference's default DBSH inner scheme (shift=False: DB, no per-round cell
+    offset), ENC_LOCAL, in place; returns (#dep, #des)."""
     dep, des = C.c_int64(0), C.c_int64(0)
     d = None if dis is None else _u32(dis)
     pp = p if isinstance(p, (list, tuple)) else [p]
     qq = q if isinstance(q, (list, tuple)) else [q]
-    lib.ko_dt_mcs_dbsh(_u32(w), lx, ly, seed, stream, t0, n, _rates4(pp), _rates4(qq), d, C.byref(dep),
-                       C.byref(des))
+    fn = lib.ko_dt_mcs_dbsh if shift else lib.ko_dt_mcs_db
+    fn(_u32(w), lx, ly, seed, stream, t0, n, _rates4(pp), _rates4(qq), d, C.byref(dep), C.byref(des))
     return dep.value, des.value
 
 

@@ -122,16 +122,18 @@ def test_dt_statistics_match_random_sequential(kpzb, oracle):
     assert abs(b_dt - b_rs) < 0.03, (b_dt, b_rs)
 
 
+@pytest.mark.parametrize("inner", ["dbsh", "db"])
 @pytest.mark.parametrize("p,q", [(1.0, 0.0), (0.95, 0.05), (0.5, 0.5), (1.0, 1.0)])
 @pytest.mark.parametrize("lx,ly", [(9, 8), (10, 9)])
-def test_dbsh_inner_scheme_bit_exact(kpzb, oracle, lx, ly, p, q):
-    """The reference's default DBSH inner decomposition (three phases per round, shared
-    atomics) against its CPU emulation, word for word, with counters."""
+def test_dbsh_inner_scheme_bit_exact(kpzb, oracle, lx, ly, p, q, inner):
+    """The reference's dead-border inner decompositions (DBSH, its default, and DB: three
+    phases per round, shared atomics) against their CPU emulation, word for word, with
+    counters."""
     n = 3
     ref = oracle.homogeneous(lx, ly, oracle.ENC_LOCAL)
-    rc = oracle.dt_mcs_dbsh(ref, lx, ly, 42, 0, 0, n, p, q)
+    rc = oracle.dt_mcs_dbsh(ref, lx, ly, 42, 0, 0, n, p, q, shift=inner == "dbsh")
     s = kpzb.Scheduler(lx, ly, scheduler="dt")
-    s.setDtInner("dbsh")
+    s.setDtInner(inner)
     s.setPQ(p, q)
     s.supplySeed(42)
     s.enableCounters(True)

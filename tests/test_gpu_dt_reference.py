@@ -27,10 +27,12 @@ def beta_of(w2):
 REF_DBSH = REF.parent / "kpz_ref_gpu"
 
 
-@pytest.mark.parametrize("inner,binary", [("dt", REF), ("dbsh", REF_DBSH)])
+@pytest.mark.parametrize("inner,binary", [("dt", REF), ("dbsh", REF_DBSH),
+                                          ("db", REF.parent / "kpz_ref_gpu_innerdb")])
 def test_dt_statistics_match_reference_gpu_dt(kpzb, inner, binary):
     """inner "dt": the reference built with KPZ_INNER_DT; "dbsh": its default build
-    (KPZ_INNER_DBSH, kpz/param.h) against this library's DBSH inner scheme."""
+    (KPZ_INNER_DBSH, kpz/param.h); "db": built with KPZ_INNER_DB -- each against this
+    library's DT kernel with the same inner scheme."""
     if not binary.exists():
         pytest.skip("reference GPU DT not built (needs the CudaKpz sources)")
     ref = []

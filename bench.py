@@ -56,13 +56,14 @@ def parse():
                     help="run only lattice i of the headline pair (profiling a single rate)")
     ap.add_argument("--lx", type=int, default=0,
                     help="override the workload's log2 lattice side (small cases for ncu)")
-    ap.add_argument("--dt-inner", choices=["dt", "dbsh", "db"], default="dt",
+    ap.add_argument("--dt-inner", choices=["dt", "dbsh", "db", "dtdbsh", "dbshrep"], default="dt",
                     help="--workload dt: the DT kernel's inner decomposition (dbsh = the reference's default)")
     ap.add_argument("--reference-gpu", action="store_true",
                     help="with --impl reference: time the reference's own CUDA scheduler on this GPU "
                          "(oracle/_ref/kpz_ref_gpu) instead of its CPU scheduler")
-    ap.add_argument("--workload", choices=["scabit", "dt", "batch", "gram", "measure"], default="scabit",
-                    help="scabit: the headline 16384^2 SCA runs; dt / batch / gram: the other configs")
+    ap.add_argument("--workload", choices=["scabit", "dt", "db4", "batch", "gram", "measure"], default="scabit",
+                    help="scabit: the headline 16384^2 SCA runs; dt / batch / gram: the other configs; "
+                         "db4: the C3 lattice under the DB4 scheduler")
     return ap.parse_args()
 
 
@@ -314,6 +315,15 @@ def fused_traffic(pqs, plans, M, lx):
     return round(tot / n) if n else None
 
 
+# Algorithmic integer-ALU operations of one random-sequential attempt (DT, DB4), counted as
+# alu_ops_per_word counts the SCABit rule: the acceptance word (Philox4x32-10's 20 three-way
+# XORs per call / 4 words = 5; its multiplies run on the FMA pipe), the 4-bit position (5/8,
+# rounded to 1), extracting the site's 2 slope bits and its neighbours' 2 bits (2 each: shift
+# and mask), classifying the 4-bit configuration as 12 or 3 (2), the threshold compare (1)
+# and the 3 XOR flips -- the kpz/kpzSimulationPrimitivesTemplates.cu:229-268 rule.
+DT_ALU_OPS_PER_ATTEMPT = 5 + 1 + 6 + 2 + 1 + 3
+
+
 def alu_ops_per_word(p, q):
     """Algorithmic integer-ALU operations per 32-site word per half-step of the SCABit rule
     (kpz/kpzSCABitCores.cu:69-74,139-145), counted as 3-input LOP3 / funnel-shift steps:
@@ -452,6 +462,9 @@ def run_reference(args, world, rank):
 
 
 REF_GPU_BIN = ROOT / "oracle" / "_ref" / "kpz_ref_gpu"
+# the reference's DT built with each KPZ_INNER_DD (kpz_ref_gpu itself: the default DBSH)
+REF_GPU_DT_BIN = {"dt": "kpz_ref_gpu_innerdt", "dbsh": "kpz_ref_gpu", "db": "kpz_ref_gpu_innerdb",
+                  "dtdbsh": "kpz_ref_gpu_innerdtdbsh", "dbshrep": "kpz_ref_gpu_innerdbshrep"}
 
 
 def run_reference_gpu(args, world, rank, local):
@@ -468,12 +481,17 @@ def run_reference_gpu(args, world, rank, local):
     env = dict(os.environ, CUDA_VISIBLE_DEVICES=os.environ.get("CUDA_VISIBLE_DEVICES", str(local)))
     clocks = ClockSampler(local)
     runs = []
-    if args.workload == "dt":
+    binary = REF_GPU_BIN
+    if args.workload in ("dt", "db4"):
         lx = args.lx or 16
         m = args.steps * max(1, args.mcs_per_step // 100)
-        jobs = [("dt", lx, 0.95, 0.05, max(1, args.warmup // 3), m)]
-        config = {"workload": f"reference SchedulerDT<SLCG64, dis> (DBSH), {1 << lx}^2, p=0.95 q=0.05",
-                  "mcs_timed": m}
+        jobs = [(args.workload, lx, 0.95, 0.05, max(1, args.warmup // 3), m)]
+        if args.workload == "dt":
+            binary = REF_GPU_BIN.parent / REF_GPU_DT_BIN[args.dt_inner]
+            name = f"SchedulerDT<SLCG64, dis> ({args.dt_inner.upper()})"
+        else:
+            name = "Scheduler<SLCG64, LocalLayoutDB4> (db4)"
+        config = {"workload": f"reference {name}, {1 << lx}^2, p=0.95 q=0.05", "mcs_timed": m}
     else:
         lx = args.lx or LX
         m = args.steps * args.mcs_per_step
@@ -482,7 +500,10 @@ def run_reference_gpu(args, world, rank, local):
                               "(0.5,0.5)", "mcs_timed_per_lattice": m}
     clocks.start()
     for (cmd, lxx, p, q, warm, n) in jobs:
-        r = subprocess.run([str(REF_GPU_BIN), cmd, str(lxx), str(p), str(q), str(warm), str(n)],
+        if not binary.exists():
+            clocks.stop()
+            return {"impl": "reference", "device": "gpu", "unavailable": f"{binary.name} not built"}
+        r = subprocess.run([str(binary), cmd, str(lxx), str(p), str(q), str(warm), str(n)],
                            capture_output=True, text=True, env=env, timeout=1200)
         if r.returncode != 0:
             clocks.stop()
@@ -524,14 +545,17 @@ def _timed(torch, stream, fn, steps):
 
 
 def run_dt(args, world, rank, local):
-    """Config C3: DT random-sequential, 65536^2 (1 GiB ENC_LOCAL), p=0.95 q=0.05."""
+    """Config C3: DT random-sequential, 65536^2 (1 GiB ENC_LOCAL), p=0.95 q=0.05 (--workload
+    db4: the same lattice and rates under the DB4 scheduler)."""
     import torch
     torch.cuda.set_device(local)
     import cudakpz_b200 as kpzb
     lx = args.lx or 16
     st = torch.cuda.Stream()
-    s = kpzb.Scheduler(lx, lx, scheduler="dt", device=local)
-    s.setDtInner(args.dt_inner)
+    db4 = args.workload == "db4"
+    s = kpzb.Scheduler(lx, lx, scheduler="db4" if db4 else "dt", device=local)
+    if not db4:
+        s.setDtInner(args.dt_inner)
     s.setPQ(0.95, 0.05)
     s.supplySeed(1 + rank)
     s.setStream(st.cuda_stream)
@@ -546,23 +570,37 @@ def run_dt(args, world, rank, local):
     ms = max_over_ranks(ms, world)
     N = 1 << (2 * lx)
     value = float(N) * m * args.steps * world / (ms * 1e6)
-    launches = 4 * m * args.steps
+    launches = (2 if db4 else 4) * m * args.steps
     per_launch = ms / launches
-    alg_launch = 0.52 * N / 4  # one domain set per launch: N/4 attempts at ~0.52 B each
+    # DT: one domain set per launch, N/4 attempts reading and writing their blocks and halos
+    # (~0.52 B each); DB4: every block per launch, N/2 attempts reading and writing the whole
+    # lattice (1 B each)
+    alg_launch = 0.5 * N if db4 else 0.52 * N / 4
     peak = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()).get("hbm_gbs", 6650.0) if (
         ROOT / "MEASURED_PEAKS.json").exists() else 6650.0
     ach = alg_launch / (per_launch * 1e-3) / 1e9
     s.setStream(0)
     ok, rep = s.consitencyCheck()
     s.close()
+    lop3, _ = kpzb.probe_alu_peak(local)
+    opa = DT_ALU_OPS_PER_ATTEMPT
+    int_roofline = {"bound": "int-alu", "achieved": round(value / world * opa / 1e3, 3),
+                    "peak": round(lop3 / 1e12, 3), "unit": "Tops/s",
+                    "frac": round(value / world * opa * 1e9 / lop3, 4),
+                    "peak_source": "measured live (kpzb_probe_alu_peak, 3-input LOP3 chains)",
+                    "alu_ops_per_attempt": opa, "roofline_upd_per_ns": round(lop3 / opa / 1e9, 1)}
     return _line(value, ms / args.steps, args, world,
-                 {"workload": f"DT random-sequential {1 << lx}^2 periodic ({N // 4 >> 20} MiB ENC_LOCAL), "
-                              f"flat start, p=0.95 q=0.05, random origin + shuffled domain sets per MCS, "
-                              f"inner scheme {args.dt_inner.upper()}",
+                 {"workload": (f"DB4 random-sequential {1 << lx}^2 periodic ({N // 4 >> 20} MiB ENC_LOCAL), "
+                               "flat start, p=0.95 q=0.05, 2 launches per MCS over all 256x128 blocks, "
+                               "5-site dead border") if db4 else
+                              (f"DT random-sequential {1 << lx}^2 periodic ({N // 4 >> 20} MiB ENC_LOCAL), "
+                               f"flat start, p=0.95 q=0.05, random origin + shuffled domain sets per MCS, "
+                               f"inner scheme {args.dt_inner.upper()}"),
                   "mcs_per_step": m, "lattice": f"{1 << lx}x{1 << lx}", "parallelism": f"replicas x{world}"},
                  roofline={"bound": "hbm", "kernel": "dt_kernel", "achieved": round(ach, 1), "peak": peak,
                            "unit": "GB/s", "frac": round(ach / peak, 4), "traffic": None,
-                           "note": "integer/barrier bound; 0.52 B/attempt algorithmic"},
+                           "note": "integer/barrier bound; " + ("1 B" if db4 else "0.52 B") + "/attempt algorithmic",
+                           "slower_roofline": "int-alu", "int_roofline": int_roofline},
                  clocks=clk, gpu_launches=launches, invariants_ok=ok)
 
 
@@ -746,7 +784,8 @@ def main():
     args = parse()
     world, rank, local = dist_setup(args.gpus)
     if args.workload != "scabit" and args.impl == "ours":
-        fn = {"dt": run_dt, "batch": run_batch, "gram": run_gram, "measure": run_measure}[args.workload]
+        fn = {"dt": run_dt, "db4": run_dt, "batch": run_batch, "gram": run_gram,
+              "measure": run_measure}[args.workload]
         line = fn(args, world, rank, local)
         if rank == 0:
             print(json.dumps(line), flush=True)

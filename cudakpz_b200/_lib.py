@@ -17,7 +17,7 @@ STATUS_NAMES = {0: "KPZB_OK", 1: "KPZB_EINVAL", 2: "KPZB_ENOMEM", 3: "KPZB_ECUDA
                 4: "KPZB_ETIMEOUT", 5: "KPZB_ESTATE", 6: "KPZB_EUNSUPPORTED"}
 
 ENC_LOCAL, ENC_CBBIT = 0, 1
-DYN_SCA, DYN_SCABIT, DYN_DT = 0, 1, 2
+DYN_SCA, DYN_SCABIT, DYN_DT, DYN_DB4 = 0, 1, 2, 3
 
 
 class KpzbError(RuntimeError):
@@ -55,6 +55,7 @@ SIGNATURES = {
     "kpzb_seed": (C.c_int, [_vp, C.c_uint64, C.c_uint32]),
     "kpzb_mcs": (C.c_int, [_vp, C.c_int]),
     "kpzb_set_dt_inner": (C.c_int, [_vp, C.c_int]),
+    "kpzb_mcs_scale": (C.c_int, [_vp, C.POINTER(C.c_double)]),
     "kpzb_set_pq_class": (C.c_int, [_vp, C.c_int, C.c_double, C.c_double]),
     "kpzb_set_disorder": (C.c_int, [_vp, _vp]),
     "kpzb_mcs_disorder": (C.c_int, [_vp, C.c_int]),

@@ -73,6 +73,8 @@ struct kpzb_handle {
     DtState dt{};
     size_t words() const { return (size_t)1 << (lx + ly - 4); }
     int encoding() const { return dyn == KPZB_DYN_SCABIT ? KPZB_ENC_CBBIT : KPZB_ENC_LOCAL; }
+    // random-sequential dynamics (DT, DB4): ENC_LOCAL on the device, driven by dt_enqueue
+    bool rs() const { return dyn == KPZB_DYN_DT || dyn == KPZB_DYN_DB4; }
 };
 
 #define KPZB_CHECK_H(h)                                              \
@@ -101,7 +103,7 @@ extern "C" kpzb_status kpzb_create(kpzb_handle** out, int lx, int ly, int dynami
 {
     if (!out) return fail(KPZB_EINVAL, "null output pointer");
     *out = nullptr;
-    if (dynamics < KPZB_DYN_SCA || dynamics > KPZB_DYN_DT) return fail(KPZB_EINVAL, "bad dynamics");
+    if (dynamics < KPZB_DYN_SCA || dynamics > KPZB_DYN_DB4) return fail(KPZB_EINVAL, "bad dynamics");
     // lx >= 8: a quadrant row holds at least one 4-word Philox group; lx + ly >= 14: every
     // launch is made of whole warps (the kernels' shuffles use full-warp masks)
     if (lx < 8 || lx > 30 || ly < 2 || ly > 30 || lx + ly > 38 || lx + ly < 14)
@@ -109,6 +111,8 @@ extern "C" kpzb_status kpzb_create(kpzb_handle** out, int lx, int ly, int dynami
                     "lattice size out of range (8<=lx<=30, 2<=ly<=30, 14<=lx+ly<=38)");
     if (dynamics == KPZB_DYN_DT && (lx < 9 || ly < 8))
         return fail(KPZB_EINVAL, "DT needs lx >= 9 and ly >= 8 (one double tile of 512x256 sites)");
+    if (dynamics == KPZB_DYN_DB4 && (lx < 8 || ly < 7))
+        return fail(KPZB_EINVAL, "DB4 needs lx >= 8 and ly >= 7 (one block of 256x128 sites)");
     int dev = device;
     if (dev < 0) {
         cudaError_t e = cudaGetDevice(&dev);
@@ -136,8 +140,8 @@ extern "C" kpzb_status kpzb_create(kpzb_handle** out, int lx, int ly, int dynami
         return bail(cuda_fail(e, "cudaMalloc(counters)"));
     cudaMemsetAsync(h->d_counters, 0, 4 * sizeof(unsigned long long), h->st);
     if ((e = analysis_alloc(&h->an, ly)) != cudaSuccess) return bail(cuda_fail(e, "analysis_alloc"));
-    if (dynamics == KPZB_DYN_DT) {
-        kpzb_status s = dt_init(&h->dt, lx, ly, h->sm_count);
+    if (h->rs()) {
+        kpzb_status s = dt_init(&h->dt, lx, ly, h->sm_count, dynamics == KPZB_DYN_DB4);
         if (s != KPZB_OK) return bail(s);
     }
     kpzb_status s = kpzb_init_homogeneous(h);
@@ -170,7 +174,7 @@ extern "C" kpzb_status kpzb_init_homogeneous(kpzb_handle* h)
 {
     KPZB_CHECK_H(h);
     // SCA keeps ENC_CBBIT internally; the flat start is the same surface in both encodings
-    const int internal = h->dyn == KPZB_DYN_DT ? KPZB_ENC_LOCAL : KPZB_ENC_CBBIT;
+    const int internal = h->rs() ? KPZB_ENC_LOCAL : KPZB_ENC_CBBIT;
     KPZB_CU(init_homogeneous_dev(h->d_sys, h->lx, h->ly, internal, h->st), "init_homogeneous");
     return KPZB_OK;
 }
@@ -193,9 +197,18 @@ extern "C" kpzb_status kpzb_set_dt_inner(kpzb_handle* h, int inner)
 {
     if (!h) return fail(KPZB_EINVAL, "null handle");
     if (h->dyn != KPZB_DYN_DT) return fail(KPZB_EUNSUPPORTED, "the inner decomposition applies to DT handles");
-    if (inner != KPZB_DT_INNER_DT && inner != KPZB_DT_INNER_DBSH && inner != KPZB_DT_INNER_DB)
-        return fail(KPZB_EINVAL, "unknown DT inner scheme");
-    h->dt.scheme = inner == KPZB_DT_INNER_DBSH ? DT_SCHEME_DBSH : inner == KPZB_DT_INNER_DB ? DT_SCHEME_DB : DT_SCHEME_DT;
+    static const int scheme_of[] = {DT_SCHEME_DT, DT_SCHEME_DBSH, DT_SCHEME_DB, DT_SCHEME_DTDBSH, DT_SCHEME_DBSHREP};
+    if (inner < KPZB_DT_INNER_DT || inner > KPZB_DT_INNER_DBSHREP) return fail(KPZB_EINVAL, "unknown DT inner scheme");
+    h->dt.scheme = scheme_of[inner];
+    return KPZB_OK;
+}
+
+extern "C" kpzb_status kpzb_mcs_scale(kpzb_handle* h, double* scale)
+{
+    if (!h || !scale) return fail(KPZB_EINVAL, "null argument");
+    if (h->dyn == KPZB_DYN_DT) *scale = 1.0;
+    else if (h->dyn == KPZB_DYN_DB4) *scale = (256.0 - 5.0) * (128.0 - 5.0) / (256.0 * 128.0);
+    else *scale = h->p + h->q;
     return KPZB_OK;
 }
 
@@ -216,7 +229,7 @@ extern "C" kpzb_status kpzb_set_disorder(kpzb_handle* h, const uint32_t* local_w
     KPZB_CHECK_H(h);
     if (!local_words) return fail(KPZB_EINVAL, "null disorder words");
     if (!h->d_dis) KPZB_CU(cudaMalloc(&h->d_dis, h->words() * 4), "cudaMalloc(disorder)");
-    if (h->dyn == KPZB_DYN_DT) {
+    if (h->rs()) {
         KPZB_CU(cudaMemcpyAsync(h->d_dis, local_words, h->words() * 4, cudaMemcpyHostToDevice, h->st),
                 "disorder copy");
     } else {
@@ -252,7 +265,7 @@ static kpzb_status resolve_plan(kpzb_handle* h, Plan* plan);
 extern "C" kpzb_status kpzb_get_fusion(kpzb_handle* h, int* mcs_per_pass)
 {
     if (!h || !mcs_per_pass) return fail(KPZB_EINVAL, "null argument");
-    if (h->dyn == KPZB_DYN_DT) {
+    if (h->rs()) {
         *mcs_per_pass = 1;
         return KPZB_OK;
     }
@@ -269,7 +282,7 @@ extern "C" kpzb_status kpzb_get_plan(kpzb_handle* h, int* mcs_per_pass, int* cta
     *mcs_per_pass = 1;
     *ctas_per_sm = 0;
     *pass_kernel = KPZB_PASS_HALF_STEPS;
-    if (h->dyn == KPZB_DYN_DT) return KPZB_OK;
+    if (h->rs()) return KPZB_OK;
     Plan p;
     kpzb_status s = resolve_plan(h, &p);
     if (s != KPZB_OK) return s;
@@ -315,7 +328,7 @@ extern "C" kpzb_status kpzb_autotune(kpzb_handle* h, int* mcs_per_pass, int* cta
                                      float* ms_per_mcs)
 {
     KPZB_CHECK_H(h);
-    if (h->dyn == KPZB_DYN_DT) return fail(KPZB_EUNSUPPORTED, "the tuner covers SCA/SCABit passes");
+    if (h->rs()) return fail(KPZB_EUNSUPPORTED, "the tuner covers SCA/SCABit passes");
     Plan p;
     KPZB_CU(tune_plan(h->d_sys, h->lx, h->ly, h->seed, h->stream_id, thresh_of(h->p), thresh_of(h->q),
                       h->sm_count, reinterpret_cast<unsigned int*>(h->d_counters + 2), h->st, &p),
@@ -381,7 +394,7 @@ extern "C" kpzb_status kpzb_mcs_async(kpzb_handle* h, int n)
     if (n == 0) return KPZB_OK;
     if (h->tdev + (uint64_t)n >= (1ull << 31)) return fail(KPZB_EINVAL, "device MCS counter limit 2^31");
     kpzb_status s;
-    if (h->dyn == KPZB_DYN_DT)
+    if (h->rs())
         s = dt_enqueue(&h->dt, h->d_sys, h->lx, h->ly, h->tdev, n, h->p, h->q, h->seed, h->stream_id,
                        h->st, h->count ? h->d_counters : nullptr);
     else
@@ -397,6 +410,8 @@ extern "C" kpzb_status kpzb_mcs_disorder_async(kpzb_handle* h, int n)
 {
     KPZB_CHECK_H(h);
     if (n < 0) return fail(KPZB_EINVAL, "negative MCS count");
+    // Kpz::Scheduler::mcsDisorder2SyncRng prints "[BUG] ... not implemented" (kpz/scheduler.h:75-78)
+    if (h->dyn == KPZB_DYN_DB4) return fail(KPZB_EUNSUPPORTED, "DB4 has no disorder dynamics");
     if (!h->d_dis) return fail(KPZB_ESTATE, "no disorder set (kpzb_set_disorder)");
     if (h->tdev + (uint64_t)n >= (1ull << 31)) return fail(KPZB_EINVAL, "device MCS counter limit 2^31");
     uint64_t Tp[4], Tq[4];
@@ -405,7 +420,7 @@ extern "C" kpzb_status kpzb_mcs_disorder_async(kpzb_handle* h, int n)
         Tq[c] = thresh_of(h->qc[c]);
     }
     unsigned long long* cnt = h->count ? h->d_counters : nullptr;
-    if (h->dyn == KPZB_DYN_DT) {
+    if (h->rs()) {
         kpzb_status s = dt_enqueue(&h->dt, h->d_sys, h->lx, h->ly, h->tdev, n, h->p, h->q, h->seed, h->stream_id,
                                    h->st, cnt, h->d_dis, Tp, Tq);
         if (s != KPZB_OK) return s;
@@ -523,7 +538,7 @@ extern "C" kpzb_status kpzb_pop_device(kpzb_handle* h, uint32_t* d_words)
 // CBBIT view of the current lattice (DT keeps ENC_LOCAL and is transcoded into d_tmp).
 static kpzb_status cbbit_view(kpzb_handle* h, const uint32_t** view)
 {
-    if (h->dyn != KPZB_DYN_DT) {
+    if (!h->rs()) {
         *view = h->d_sys;
         return KPZB_OK;
     }
@@ -651,7 +666,7 @@ struct CkptTrailer {  // little-endian, written field by field
     uint64_t tdev, seed;
     uint32_t stream_id, fusion;
     double p, q;
-    uint32_t has_snap, reserved;
+    uint32_t has_snap, dt_scheme;  // dt_scheme: the DT inner scheme (0 in files of other dynamics)
     double snap_mean;
 };
 }  // namespace
@@ -687,6 +702,7 @@ extern "C" kpzb_status kpzb_save(kpzb_handle* h, const char* path, const char* m
     t.p = h->p;
     t.q = h->q;
     t.has_snap = h->has_snap ? 1u : 0u;
+    t.dt_scheme = h->dyn == KPZB_DYN_DT ? (uint32_t)h->dt.scheme : 0u;
     t.snap_mean = h->snap_mean;
     ok = ok && fwrite(CKPT_MAGIC, 1, 8, f) == 8 && fwrite(&t, sizeof t, 1, f) == 1;
     if (h->has_snap) ok = ok && fwrite(snap.data(), 4, snap.size(), f) == snap.size();
@@ -725,7 +741,7 @@ extern "C" kpzb_status kpzb_load(kpzb_handle* h, const char* path)
     const bool has_trailer = fread(magic, 1, 8, f) == 8 && memcmp(magic, CKPT_MAGIC, 8) == 0;
     if (has_trailer) {
         ok = fread(&t, sizeof t, 1, f) == 1 && t.version == 1 && t.lx == (uint32_t)h->lx &&
-             t.ly == (uint32_t)h->ly && t.dyn == (uint32_t)h->dyn;
+             t.ly == (uint32_t)h->ly && t.dyn == (uint32_t)h->dyn && t.dt_scheme <= (uint32_t)DT_SCHEME_DBSHREP;
         if (ok && t.has_snap) {
             snap.resize(h->words());
             ok = fread(snap.data(), 4, snap.size(), f) == snap.size();
@@ -744,6 +760,7 @@ extern "C" kpzb_status kpzb_load(kpzb_handle* h, const char* path)
         h->q = t.q;
         h->has_snap = t.has_snap != 0;
         h->snap_mean = t.snap_mean;
+        if (h->dyn == KPZB_DYN_DT) h->dt.scheme = (int)t.dt_scheme;
         if (h->has_snap) {
             if (!h->d_snap) KPZB_CU(cudaMalloc(&h->d_snap, h->words() * 4), "cudaMalloc(snapshot)");
             KPZB_CU(cudaMemcpyAsync(h->d_snap, snap.data(), snap.size() * 4, cudaMemcpyHostToDevice, h->st), "snapshot");

@@ -13,7 +13,14 @@
 // Geometry: 32x16 threads, thread cells of 8x8 sites (2x2 words), blocks of 256x128 sites
 // (64x32 words), shared tile 65x33 words, 64 rounds per launch (one attempt per site per
 // MCS).  All random numbers come from the counter stream (see oracle/kpz_oracle.h), so the
-// CPU emulation ko_dt_mcs reproduces every lattice bit for bit.
+// CPU emulations ko_dt_mcs* reproduce every lattice bit for bit.
+//
+// The same kernel, with the reference's other block-level decompositions (KPZ_INNER_DD,
+// kpz/kpzConst.h:26-35) as a template parameter: DTDBSH, DB, DBSH (the reference's default)
+// and DBSHRep; and the reference's DB4 scheduler (Kpz::Scheduler<Rng, LocalLayoutDB4>,
+// kpz/scheduler.cu:37-52, kpz/kpz.cu:95-117): per MCS two launches over every block from a
+// random origin in [0, block), no halo, sites within 5 of the block's far edges dead, 32
+// BaseDT rounds per launch (kpz/kpzSimulationPrimitivesTemplates.cu:74-103).
 #include <cmath>
 #include <type_traits>
 #include <cstring>
@@ -28,25 +35,88 @@ constexpr uint32_t TAG_DT_SUB = 4u;
 constexpr uint32_t TAG_DT_POS = 5u;
 constexpr uint32_t TAG_DBSH_ORIGIN = 7u;
 constexpr uint32_t TAG_DBSH_POS = 8u;
+constexpr uint32_t TAG_REP_ORIGIN = 9u;
+constexpr uint32_t TAG_REP_POS = 10u;
+constexpr uint32_t TAG_REP_U = 11u;
+constexpr uint32_t TAG_DB4_ORIGIN = 12u;
+constexpr uint32_t TAG_DB4_SUB = 13u;
+constexpr uint32_t TAG_DB4_POS = 14u;
+constexpr uint32_t TAG_DB4_U = 15u;
 constexpr int DT_TX = 32, DT_TY = 16;
+constexpr int DT_THREADS = DT_TX * DT_TY;
 constexpr int DT_BXW = 64, DT_BYW = 32;           // block in words
 constexpr int DT_BX = 4 * DT_BXW, DT_BY = 4 * DT_BYW;  // block in sites
 constexpr int DT_TW = DT_BXW + 1, DT_TH = DT_BYW + 1;  // shared tile with halo
 constexpr int DT_ROUNDS = 64;
+// DB4: sites of a block whose x >= 251 or y >= 123 (before the origin's offset inside a word)
+// are dead, so no update reaches past the block (LocalLayoutDB4::BLOCK_BORDER_WIDTH = 5,
+// kpz/LocalLayout.h:120-131)
+constexpr int DB4_BORDER = 5;
+
+__device__ __forceinline__ uint32_t pick4(const uint4& v, int i)
+{
+    return i == 0 ? v.x : i == 1 ? v.y : i == 2 ? v.z : v.w;
+}
+
+// One attempt at tile site (xt, yt) (sites counted from the tile's first word) whose flips may
+// share words with other threads' attempts of the same phase: shared-memory atomics, as the
+// reference's dead-border schemes use (fctAtomicXor).  u: the acceptance word.
+template <bool COUNT, bool DIS>
+__device__ __forceinline__ void dt_attempt_atomic(uint32_t* tile, const uint32_t* dtile, int xt, int yt, uint32_t u,
+                                                  const Thresh& tp, const Thresh& tq, const DisorderRates& dr,
+                                                  unsigned long long& ndep, unsigned long long& ndes)
+{
+    const int wi = (yt >> 2) * DT_TW + (xt >> 2);
+    const uint32_t sh = (uint32_t)(((xt & 3) << 1) | ((yt & 3) << 3));
+    const int wr = (yt >> 2) * DT_TW + ((xt + 1) >> 2);
+    const uint32_t shr = (uint32_t)((((xt + 1) & 3) << 1) | ((yt & 3) << 3));
+    const int wd = ((yt + 1) >> 2) * DT_TW + (xt >> 2);
+    const uint32_t shd = (uint32_t)(((xt & 3) << 1) | (((yt + 1) & 3) << 3) | 1);
+    const uint32_t c = (tile[wi] >> sh) & 3u, rbit = (tile[wr] >> shr) & 1u, lbit = (tile[wd] >> shd) & 1u;
+    const bool is_p = c == 0u && rbit && lbit, is_q = c == 3u && !rbit && !lbit;
+    if (!(is_p || is_q)) return;
+    int cls = 0;
+    if (DIS) cls = (int)((dtile[wi] >> sh) & 3u);
+    const Thresh& th = DIS ? (is_p ? dr.tp[cls] : dr.tq[cls]) : (is_p ? tp : tq);
+    const bool flip = th.always || (th.planes && u < th.t);
+    if (!flip) return;
+    atomicXor(&tile[wi], 3u << sh);
+    atomicXor(&tile[wr], 1u << shr);
+    atomicXor(&tile[wd], 1u << shd);
+    if (COUNT) {
+        if (is_p) ++ndep;
+        else ++ndes;
+    }
+}
 
 // DIS: quenched disorder (Disorder2SyncRng_shared, kpz/kpzSimulationPrimitivesTemplates.cu:
 // 295-382): dis holds every site's 2-bit rate class in ENC_LOCAL words, copied into a second
 // shared tile beside the lattice's; the class picks dr.tp[c] / dr.tq[c].
-// SCHEME: DT_SCHEME_DT, DT_SCHEME_DBSH or DT_SCHEME_DB (the dead-border phases without the
-// per-round cell offset).
+// SCHEME (the reference's KPZ_INNER_DD, kpz/kpzConst.h:26-35, plus its DB4 scheduler):
+//   DT_SCHEME_DT      single-hit double tiling (BaseDT)
+//   DT_SCHEME_DTDBSH  the same with a block-wide random offset of the thread cells per round
+//   DT_SCHEME_DBSH    single-hit dead border, borders delayed to later phases of the round
+//   DT_SCHEME_DB      the dead-border phases without the per-round cell offset
+//   DT_SCHEME_DBSHREP DBSH with the border hits replaced by fresh attempts after the rounds
+//   DT_SCHEME_DB4     every block of the lattice in one launch, a dead border of 5 sites, the
+//                     inner rounds of BaseDT (32 per launch, two launches per MCS)
 template <bool COUNT, bool DIS, int SCHEME>
-__global__ void __launch_bounds__(DT_TX* DT_TY)
+__global__ void __launch_bounds__(DT_THREADS)
 dt_kernel(uint32_t* __restrict__ sys, int lxw, int lyw, int lnbx, int nblocks, int ox, int oy,
           int d, uint32_t t, Key key, uint32_t stream, Thresh tp, Thresh tq,
           unsigned long long* __restrict__ counters, const uint32_t* __restrict__ dis, DisorderRates dr)
 {
+    constexpr bool DB4 = SCHEME == DT_SCHEME_DB4;
+    constexpr bool SHIFTED = SCHEME == DT_SCHEME_DTDBSH;
+    constexpr bool REP = SCHEME == DT_SCHEME_DBSHREP;
+    constexpr bool BORDER = SCHEME == DT_SCHEME_DBSH || SCHEME == DT_SCHEME_DB || REP;
+    constexpr int ROUNDS = DB4 ? DT_ROUNDS / 2 : DT_ROUNDS;
+    constexpr uint32_t T_SUB = DB4 ? TAG_DB4_SUB : TAG_DT_SUB;
+    constexpr uint32_t T_POS = DB4 ? TAG_DB4_POS : TAG_DT_POS;
+    constexpr uint32_t T_U = DB4 ? TAG_DB4_U : TAG_DT;
     __shared__ uint32_t tile[DT_TH * DT_TW];
     __shared__ uint32_t dtile[DIS ? DT_TH * DT_TW : 1];
+    __shared__ uint32_t rep_hits[REP ? DT_THREADS / 32 + 1 : 1];
     // Site geometry of every (sub-cell s, in-cell position pb) pair, relative to a thread's cell:
     // the origin's offset inside a word (ox & 3, oy & 3) is the same for every block and thread
     // of the launch, so the word offsets and bit shifts of the site, its right neighbour and its
@@ -57,17 +127,18 @@ dt_kernel(uint32_t* __restrict__ sys, int lxw, int lyw, int lnbx, int nblocks, i
     __shared__ uint32_t lut[64];
     const int tid = threadIdx.y * DT_TX + threadIdx.x;
     const uint32_t Wx = 1u << lxw, Wy = 1u << lyw;
+    const int ax = ox & 3, ay = oy & 3;
     bool need_u = !(tp.always || tp.planes == 0) || !(tq.always || tq.planes == 0);
     if (DIS) need_u = dr.planes > 0;
     unsigned long long ndep = 0, ndes = 0;
     if (tid < 64) {
         const int sc = tid >> 4, pb = tid & 15;
-        const int ax = (ox & 3) + (pb & 3), ay = (oy & 3) + (pb >> 2);
-        const int col = (sc & 1) + (ax >> 2), row = (sc >> 1) + (ay >> 2);
-        const int xb = ax & 3, yb = ay & 3;
+        const int axx = ax + (pb & 3), ayy = ay + (pb >> 2);
+        const int col = (sc & 1) + (axx >> 2), row = (sc >> 1) + (ayy >> 2);
+        const int xb = axx & 3, yb = ayy & 3;
         const uint32_t sh = (uint32_t)((xb << 1) | (yb << 3));
-        const uint32_t shr = (uint32_t)((((ax + 1) & 3) << 1) | (yb << 3));
-        const uint32_t shd = (uint32_t)((xb << 1) | (((ay + 1) & 3) << 3) | 1);
+        const uint32_t shr = (uint32_t)((((axx + 1) & 3) << 1) | (yb << 3));
+        const uint32_t shd = (uint32_t)((xb << 1) | (((ayy + 1) & 3) << 3) | 1);
         lut[tid] = (uint32_t)(row * DT_TW + col) | (sh << 8) | (shr << 13) | (shd << 18) |
                    ((xb == 3 ? 1u : 0u) << 23) | ((yb == 3 ? 1u : 0u) << 24);
     }
@@ -75,31 +146,36 @@ dt_kernel(uint32_t* __restrict__ sys, int lxw, int lyw, int lnbx, int nblocks, i
 
     for (int b = blockIdx.x; b < nblocks; b += gridDim.x) {
         const int bx = b & ((1 << lnbx) - 1), by = b >> lnbx;
-        const uint32_t X0 = (uint32_t)ox + (uint32_t)(2 * bx + (d & 1)) * DT_BX;
-        const uint32_t Y0 = (uint32_t)oy + (uint32_t)(2 * by + (d >> 1)) * DT_BY;
+        const uint32_t X0 = (uint32_t)ox + (uint32_t)(DB4 ? bx : 2 * bx + (d & 1)) * DT_BX;
+        const uint32_t Y0 = (uint32_t)oy + (uint32_t)(DB4 ? by : 2 * by + (d >> 1)) * DT_BY;
         const uint32_t wx0 = X0 >> 2, wy0 = Y0 >> 2;
-        for (int i = tid; i < DT_TH * DT_TW; i += DT_TX * DT_TY) {
+        for (int i = tid; i < DT_TH * DT_TW; i += DT_THREADS) {
             const uint32_t r = i / DT_TW, c = i - r * DT_TW;
+            // DB4 blocks tile the lattice without halo: the dead border keeps every update,
+            // its right and its lower neighbour inside the block's 64x32 words
+            if (DB4 && (r == DT_BYW || c == DT_BXW)) continue;
             const size_t gi = (size_t)((wy0 + r) & (Wy - 1)) * Wx + ((wx0 + c) & (Wx - 1));
             tile[i] = sys[gi];
             if (DIS) dtile[i] = dis[gi];
         }
         // block-wide sub-cell sequence: 2 bits per round (every thread derives the same words)
         const uint4 sub = philox4x32_10(
-            make_uint4((uint32_t)b, t, (TAG_DT_SUB << 24) | ((uint32_t)d << 16), stream), key);
-        const uint32_t cid = (uint32_t)b * (DT_TX * DT_TY) + (uint32_t)tid;
+            make_uint4((uint32_t)b, t, (T_SUB << 24) | ((uint32_t)d << 16), stream), key);
+        const uint32_t cid = (uint32_t)b * DT_THREADS + (uint32_t)tid;
         __syncthreads();
-        uint4 pos = make_uint4(0, 0, 0, 0), uu = make_uint4(0, 0, 0, 0);
-        constexpr bool DBSH = SCHEME != DT_SCHEME_DT;
-        if (DBSH) {
+        uint4 pos = make_uint4(0, 0, 0, 0), uu = make_uint4(0, 0, 0, 0), ow = make_uint4(0, 0, 0, 0);
+        if (BORDER) {
             // the reference's default inner scheme (BaseDTInnerDBSH::systemLoopDC,
             // kpz/kpzSimulationPrimitivesTemplates_BaseInnerDB.cu:110-163): per round one
             // block-wide offset shifts every thread cell, each thread picks a site of its shifted
             // cell, and sites on a cell's last column/row wait for phases 1 (off the corner) and
-            // 2 (the corner); the flips use shared-memory atomics as the reference's do
-            const int ax = ox & 3, ay = oy & 3;
+            // 2 (the corner); the flips use shared-memory atomics as the reference's do.
+            // REP (BaseDTInnerDBSHRep, :175-268): a border hit is not done in its round but
+            // counted, and after the 64 rounds the block makes that many fresh attempts, 512 per
+            // repetition round, each again in the three phases.
+            uint32_t hits = 0;
             for (int rb = 0; rb < DT_ROUNDS; rb += 16) {
-                const uint4 ow = philox4x32_10(
+                ow = philox4x32_10(
                     make_uint4((uint32_t)b, t, (TAG_DBSH_ORIGIN << 24) | ((uint32_t)d << 16) | (uint32_t)(rb >> 4),
                                stream), key);
                 const uint4 pw = philox4x32_10(
@@ -111,107 +187,156 @@ dt_kernel(uint32_t* __restrict__ sys, int lxw, int lyw, int lnbx, int nblocks, i
                     if (need_u && (j & 3) == 0)
                         uu = philox4x32_10(
                             make_uint4(cid, t, (TAG_DT << 24) | ((uint32_t)d << 16) | (uint32_t)(r >> 2), stream), key);
-                    const uint32_t owd = (j >> 2) == 0 ? ow.x : (j >> 2) == 1 ? ow.y : (j >> 2) == 2 ? ow.z : ow.w;
-                    const uint32_t pwd = (j >> 2) == 0 ? pw.x : (j >> 2) == 1 ? pw.y : (j >> 2) == 2 ? pw.z : pw.w;
-                    const uint32_t ob = (owd >> (8 * (j & 3))) & 0xFFu, pb = (pwd >> (8 * (j & 3))) & 0xFFu;
+                    const uint32_t ob = (pick4(ow, j >> 2) >> (8 * (j & 3))) & 0xFFu;
+                    const uint32_t pb = (pick4(pw, j >> 2) >> (8 * (j & 3))) & 0xFFu;
                     const int px = (int)(pb & 7u), py = (int)((pb >> 3) & 7u);
                     const int ph = (px == 7 && py == 7) ? 2 : (px == 7 || py == 7) ? 1 : 0;
                     const int orx = SCHEME == DT_SCHEME_DB ? 0 : (int)(ob & 7u);
                     const int ory = SCHEME == DT_SCHEME_DB ? 0 : (int)((ob >> 3) & 7u);
                     const int xt = (threadIdx.x * 8 + ax + px + orx) & (DT_BX - 1);
                     const int yt = (threadIdx.y * 8 + ay + py + ory) & (DT_BY - 1);
-                    const int wi = (yt >> 2) * DT_TW + (xt >> 2);
-                    const uint32_t sh = (uint32_t)(((xt & 3) << 1) | ((yt & 3) << 3));
-                    const int wr = (yt >> 2) * DT_TW + ((xt + 1) >> 2);
-                    const uint32_t shr = (uint32_t)((((xt + 1) & 3) << 1) | ((yt & 3) << 3));
-                    const int wd = ((yt + 1) >> 2) * DT_TW + (xt >> 2);
-                    const uint32_t shd = (uint32_t)(((xt & 3) << 1) | (((yt + 1) & 3) << 3) | 1);
-                    const uint32_t u = (j & 3) == 0 ? uu.x : (j & 3) == 1 ? uu.y : (j & 3) == 2 ? uu.z : uu.w;
-                    for (int phase = 0; phase < 3; ++phase) {
-                        if (ph == phase) {
-                            const uint32_t c = (tile[wi] >> sh) & 3u, rbit = (tile[wr] >> shr) & 1u,
-                                           lbit = (tile[wd] >> shd) & 1u;
-                            const bool is_p = c == 0u && rbit && lbit, is_q = c == 3u && !rbit && !lbit;
-                            bool flip = false;
-                            if (is_p || is_q) {
-                                int cls = 0;
-                                if (DIS) cls = (int)((dtile[wi] >> sh) & 3u);
-                                const Thresh& th = DIS ? (is_p ? dr.tp[cls] : dr.tq[cls]) : (is_p ? tp : tq);
-                                if (th.always) flip = true;
-                                else if (th.planes) flip = u < th.t;
-                            }
-                            if (flip) {
-                                atomicXor(&tile[wi], 3u << sh);
-                                atomicXor(&tile[wr], 1u << shr);
-                                atomicXor(&tile[wd], 1u << shd);
-                                if (COUNT) {
-                                    if (is_p) ++ndep;
-                                    else ++ndes;
-                                }
-                            }
+                    const uint32_t u = pick4(uu, j & 3);
+                    if (REP) {
+                        if (ph == 0) dt_attempt_atomic<COUNT, DIS>(tile, dtile, xt, yt, u, tp, tq, dr, ndep, ndes);
+                        else ++hits;
+                        __syncthreads();
+                    } else {
+                        for (int phase = 0; phase < 3; ++phase) {
+                            if (ph == phase)
+                                dt_attempt_atomic<COUNT, DIS>(tile, dtile, xt, yt, u, tp, tq, dr, ndep, ndes);
+                            __syncthreads();
                         }
+                    }
+                }
+            }
+            if (REP) {
+                // The block's count as the reference's reduction forms it (:214-227): thread 0's
+                // own hits plus the warp sums of warps 1.. -- the hits of warp 0's lanes 1-31 are
+                // not repeated there, nor here.
+                uint32_t ws = hits;
+                for (int o = 16; o > 0; o >>= 1) ws += __shfl_xor_sync(0xffffffffu, ws, o);
+                if ((tid & 31) == 0) rep_hits[1 + (tid >> 5)] = ws;
+                if (tid == 0) rep_hits[0] = hits;
+                __syncthreads();
+                uint32_t total = rep_hits[0];
+                for (int w = 1; w < DT_THREADS / 32; ++w) total += rep_hits[1 + w];
+                uint4 rpw = make_uint4(0, 0, 0, 0), ruu = make_uint4(0, 0, 0, 0);
+                for (int k = 0; k * DT_THREADS < (int)total; ++k) {
+                    const bool active = k * DT_THREADS + tid < (int)total;
+                    if ((k & 15) == 0) {
+                        ow = philox4x32_10(make_uint4((uint32_t)b, t,
+                                                      (TAG_REP_ORIGIN << 24) | ((uint32_t)d << 16) | (uint32_t)(k >> 4),
+                                                      stream), key);
+                        if (active)
+                            rpw = philox4x32_10(
+                                make_uint4(cid, t, (TAG_REP_POS << 24) | ((uint32_t)d << 16) | (uint32_t)(k >> 4),
+                                           stream), key);
+                    }
+                    if (active && need_u && (k & 3) == 0)
+                        ruu = philox4x32_10(
+                            make_uint4(cid, t, (TAG_REP_U << 24) | ((uint32_t)d << 16) | (uint32_t)(k >> 2), stream),
+                            key);
+                    const uint32_t ob = (pick4(ow, (k & 15) >> 2) >> (8 * (k & 3))) & 0xFFu;
+                    const uint32_t pb = (pick4(rpw, (k & 15) >> 2) >> (8 * (k & 3))) & 0xFFu;
+                    const int px = (int)(pb & 7u), py = (int)((pb >> 3) & 7u);
+                    const int ph = !active ? 3 : (px == 7 && py == 7) ? 2 : (px == 7 || py == 7) ? 1 : 0;
+                    const int xt = (threadIdx.x * 8 + ax + px + (int)(ob & 7u)) & (DT_BX - 1);
+                    const int yt = (threadIdx.y * 8 + ay + py + (int)((ob >> 3) & 7u)) & (DT_BY - 1);
+                    const uint32_t u = pick4(ruu, k & 3);
+                    for (int phase = 0; phase < 3; ++phase) {
+                        if (ph == phase)
+                            dt_attempt_atomic<COUNT, DIS>(tile, dtile, xt, yt, u, tp, tq, dr, ndep, ndes);
                         __syncthreads();
                     }
                 }
             }
         }
-        for (int rb = 0; !DBSH && rb < DT_ROUNDS; rb += 8) {
+        for (int rb = 0; !BORDER && rb < ROUNDS; rb += 8) {
             if ((rb & 31) == 0)
                 pos = philox4x32_10(
-                    make_uint4(cid, t, (TAG_DT_POS << 24) | ((uint32_t)d << 16) | (uint32_t)(rb >> 5), stream),
-                    key);
-            const uint32_t sw = (rb < 16) ? sub.x : (rb < 32) ? sub.y : (rb < 48) ? sub.z : sub.w;
-            const int pq = (rb & 31) >> 3;
-            const uint32_t pw = pq == 0 ? pos.x : pq == 1 ? pos.y : pq == 2 ? pos.z : pos.w;
+                    make_uint4(cid, t, (T_POS << 24) | ((uint32_t)d << 16) | (uint32_t)(rb >> 5), stream), key);
+            if (SHIFTED && (rb & 15) == 0)
+                ow = philox4x32_10(
+                    make_uint4((uint32_t)b, t, (TAG_DBSH_ORIGIN << 24) | ((uint32_t)d << 16) | (uint32_t)(rb >> 4),
+                               stream), key);
+            const uint32_t sw = pick4(sub, rb >> 4);
+            const uint32_t pw = pick4(pos, (rb & 31) >> 3);
 #pragma unroll
             for (int j = 0; j < 8; ++j) {
                 const int r = rb + j;
                 if (need_u && (j & 3) == 0)
                     uu = philox4x32_10(
-                        make_uint4(cid, t, (TAG_DT << 24) | ((uint32_t)d << 16) | (uint32_t)(r >> 2), stream), key);
+                        make_uint4(cid, t, (T_U << 24) | ((uint32_t)d << 16) | (uint32_t)(r >> 2), stream), key);
                 const uint32_t sc = (sw >> (2 * (r & 15))) & 3u;
                 const uint32_t pb = (pw >> (4 * j)) & 15u;
-                const uint32_t e = lut[sc * 16u + pb];
-                const int w = tbase + (int)(e & 255u);
-                const uint32_t sh = (e >> 8) & 31u, shr = (e >> 13) & 31u, shd = (e >> 18) & 31u;
-                const bool dxr = (e >> 23) & 1u, dyd = (e >> 24) & 1u;
-                uint32_t cw = tile[w];
-                uint32_t rw = dxr ? tile[w + 1] : cw;
-                uint32_t dw = dyd ? tile[w + DT_TW] : cw;
-                const uint32_t c = (cw >> sh) & 3u, rbit = (rw >> shr) & 1u, lbit = (dw >> shd) & 1u;
-                const bool is_p = c == 0u && rbit && lbit;      // local minimum (config 12)
-                const bool is_q = c == 3u && !rbit && !lbit;    // local maximum (config 3)
-                bool flip = false;
-                if (is_p || is_q) {
-                    int cls = 0;
-                    if (DIS) cls = (int)((dtile[w] >> sh) & 3u);
-                    const Thresh& th = DIS ? (is_p ? dr.tp[cls] : dr.tq[cls]) : (is_p ? tp : tq);
-                    if (th.always) flip = true;
-                    else if (th.planes) {
-                        const uint32_t u = (j & 3) == 0 ? uu.x : (j & 3) == 1 ? uu.y : (j & 3) == 2 ? uu.z : uu.w;
-                        flip = u < th.t;
-                    }
+                int w;
+                uint32_t sh, shr, shd;
+                bool dxr, dyd, live = true;
+                if (SHIFTED) {
+                    // BaseDTInnerDTDBSH (kpz/kpzSimulationPrimitivesTemplates_BaseInnerDTr.cu:
+                    // 30-85): the quadrant and a block-wide offset in [0,8)^2 per round, the
+                    // site wrapped inside the block before the origin's in-word offset is added;
+                    // neighbouring threads' sites stay 4 or more sites apart, so no two share a word
+                    const uint32_t ob = (pick4(ow, (r & 15) >> 2) >> (8 * (r & 3))) & 0xFFu;
+                    const int xt = ((threadIdx.x * 8 + 4 * (int)(sc & 1u) + (int)(pb & 3u) + (int)(ob & 7u)) &
+                                    (DT_BX - 1)) + ax;
+                    const int yt = ((threadIdx.y * 8 + 2 * (int)(sc & 2u) + (int)(pb >> 2) + (int)((ob >> 3) & 7u)) &
+                                    (DT_BY - 1)) + ay;
+                    w = (yt >> 2) * DT_TW + (xt >> 2);
+                    sh = (uint32_t)(((xt & 3) << 1) | ((yt & 3) << 3));
+                    shr = (uint32_t)((((xt + 1) & 3) << 1) | ((yt & 3) << 3));
+                    shd = (uint32_t)(((xt & 3) << 1) | (((yt + 1) & 3) << 3) | 1);
+                    dxr = (xt & 3) == 3;
+                    dyd = (yt & 3) == 3;
+                } else {
+                    const uint32_t e = lut[sc * 16u + pb];
+                    w = tbase + (int)(e & 255u);
+                    sh = (e >> 8) & 31u;
+                    shr = (e >> 13) & 31u;
+                    shd = (e >> 18) & 31u;
+                    dxr = (e >> 23) & 1u;
+                    dyd = (e >> 24) & 1u;
+                    if (DB4)
+                        live = threadIdx.x * 8 + 4 * (int)(sc & 1u) + (int)(pb & 3u) < DT_BX - DB4_BORDER &&
+                               threadIdx.y * 8 + 2 * (int)(sc & 2u) + (int)(pb >> 2) < DT_BY - DB4_BORDER;
                 }
-                if (flip) {
-                    // the words of this round's site and neighbours belong to this thread alone
-                    cw ^= 3u << sh;
-                    if (dxr) rw ^= 1u << shr;
-                    else cw ^= 1u << shr;
-                    if (dyd) dw ^= 1u << shd;
-                    else cw ^= 1u << shd;
-                    tile[w] = cw;
-                    if (dxr) tile[w + 1] = rw;
-                    if (dyd) tile[w + DT_TW] = dw;
-                    if (COUNT) {
-                        if (is_p) ++ndep;
-                        else ++ndes;
+                if (live) {
+                    uint32_t cw = tile[w];
+                    uint32_t rw = dxr ? tile[w + 1] : cw;
+                    uint32_t dw = dyd ? tile[w + DT_TW] : cw;
+                    const uint32_t c = (cw >> sh) & 3u, rbit = (rw >> shr) & 1u, lbit = (dw >> shd) & 1u;
+                    const bool is_p = c == 0u && rbit && lbit;      // local minimum (config 12)
+                    const bool is_q = c == 3u && !rbit && !lbit;    // local maximum (config 3)
+                    bool flip = false;
+                    if (is_p || is_q) {
+                        int cls = 0;
+                        if (DIS) cls = (int)((dtile[w] >> sh) & 3u);
+                        const Thresh& th = DIS ? (is_p ? dr.tp[cls] : dr.tq[cls]) : (is_p ? tp : tq);
+                        if (th.always) flip = true;
+                        else if (th.planes) flip = pick4(uu, j & 3) < th.t;
+                    }
+                    if (flip) {
+                        // the words of this round's site and neighbours belong to this thread alone
+                        cw ^= 3u << sh;
+                        if (dxr) rw ^= 1u << shr;
+                        else cw ^= 1u << shr;
+                        if (dyd) dw ^= 1u << shd;
+                        else cw ^= 1u << shd;
+                        tile[w] = cw;
+                        if (dxr) tile[w + 1] = rw;
+                        if (dyd) tile[w + DT_TW] = dw;
+                        if (COUNT) {
+                            if (is_p) ++ndep;
+                            else ++ndes;
+                        }
                     }
                 }
                 __syncthreads();
             }
         }
-        for (int i = tid; i < DT_TH * DT_TW; i += DT_TX * DT_TY) {
+        for (int i = tid; i < DT_TH * DT_TW; i += DT_THREADS) {
             const uint32_t r = i / DT_TW, c = i - r * DT_TW;
+            if (DB4 && (r == DT_BYW || c == DT_BXW)) continue;
             sys[(size_t)((wy0 + r) & (Wy - 1)) * Wx + ((wx0 + c) & (Wx - 1))] = tile[i];
         }
         __syncthreads();
@@ -271,12 +396,15 @@ static void dt_plan(uint64_t seed, uint32_t stream, uint32_t t, int* ox, int* oy
     }
 }
 
-kpzb_status dt_init(DtState* s, int lx, int ly, int sm_count)
+kpzb_status dt_init(DtState* s, int lx, int ly, int sm_count, bool db4)
 {
-    if (lx < 9 || ly < 8) return fail(KPZB_EINVAL, "DT needs lx >= 9 and ly >= 8 (one 512x256 double tile)");
-    const int nblocks = (1 << (lx - 9)) * (1 << (ly - 8));
+    if (db4 && (lx < 8 || ly < 7)) return fail(KPZB_EINVAL, "DB4 needs lx >= 8 and ly >= 7 (one 256x128 block)");
+    if (!db4 && (lx < 9 || ly < 8))
+        return fail(KPZB_EINVAL, "DT needs lx >= 9 and ly >= 8 (one 512x256 double tile)");
+    const int nblocks = db4 ? (1 << (lx - 8)) * (1 << (ly - 7)) : (1 << (lx - 9)) * (1 << (ly - 8));
     // 2048 threads per SM / 512 per CTA: 4 resident CTAs per SM
     s->grid = nblocks < sm_count * 4 ? nblocks : sm_count * 4;
+    if (db4) s->scheme = DT_SCHEME_DB4;
     s->ready = true;
     return KPZB_OK;
 }
@@ -299,30 +427,48 @@ kpzb_status dt_enqueue(DtState* s, uint32_t* d_local, int lx, int ly, uint64_t t
     if (!s->ready) return fail(KPZB_ESTATE, "DT state not initialised");
     const Key key = make_key(seed);
     const Thresh tp = make_thresh(thresh_dt(p)), tq = make_thresh(thresh_dt(q));
-    const int lnbx = lx - 9;
-    const int nblocks = (1 << lnbx) * (1 << (ly - 8));
+    const bool db4 = s->scheme == DT_SCHEME_DB4;
+    const int lnbx = db4 ? lx - 8 : lx - 9;
+    const int nblocks = (1 << lnbx) * (1 << (db4 ? ly - 7 : ly - 8));
     const dim3 block(DT_TX, DT_TY);
     const DisorderRates dr = dis ? make_disorder_rates(dis_Tp, dis_Tq) : DisorderRates{};
+    const bool c = d_counters != nullptr, ds = dis != nullptr;
+    auto launch = [&](int ox, int oy, int d, uint32_t t) {
+        auto go = [&](auto kern) {
+            kern<<<s->grid, block, 0, st>>>(d_local, lx - 2, ly - 2, lnbx, nblocks, ox, oy, d, t, key, stream, tp,
+                                             tq, d_counters, dis, dr);
+        };
+        auto pick = [&](auto scheme_tag) {
+            constexpr int S = decltype(scheme_tag)::value;
+            if (c && ds) go(dt_kernel<true, true, S>);
+            else if (c) go(dt_kernel<true, false, S>);
+            else if (ds) go(dt_kernel<false, true, S>);
+            else go(dt_kernel<false, false, S>);
+        };
+        switch (s->scheme) {
+        case DT_SCHEME_DBSH: pick(std::integral_constant<int, DT_SCHEME_DBSH>{}); break;
+        case DT_SCHEME_DB: pick(std::integral_constant<int, DT_SCHEME_DB>{}); break;
+        case DT_SCHEME_DTDBSH: pick(std::integral_constant<int, DT_SCHEME_DTDBSH>{}); break;
+        case DT_SCHEME_DBSHREP: pick(std::integral_constant<int, DT_SCHEME_DBSHREP>{}); break;
+        case DT_SCHEME_DB4: pick(std::integral_constant<int, DT_SCHEME_DB4>{}); break;
+        default: pick(std::integral_constant<int, DT_SCHEME_DT>{}); break;
+        }
+    };
     for (int i = 0; i < n; ++i) {
         const uint32_t t = (uint32_t)(t0 + (uint64_t)i);
-        int ox, oy, order[4];
-        dt_plan(seed, stream, t, &ox, &oy, order);
-        for (int a = 0; a < 4; ++a) {
-            auto go = [&](auto kern) {
-                kern<<<s->grid, block, 0, st>>>(d_local, lx - 2, ly - 2, lnbx, nblocks, ox, oy, order[a], t, key,
-                                                 stream, tp, tq, d_counters, dis, dr);
-            };
-            const bool c = d_counters != nullptr, ds = dis != nullptr;
-            auto pick = [&](auto scheme_tag) {
-                constexpr int S = decltype(scheme_tag)::value;
-                if (c && ds) go(dt_kernel<true, true, S>);
-                else if (c) go(dt_kernel<true, false, S>);
-                else if (ds) go(dt_kernel<false, true, S>);
-                else go(dt_kernel<false, false, S>);
-            };
-            if (s->scheme == DT_SCHEME_DBSH) pick(std::integral_constant<int, DT_SCHEME_DBSH>{});
-            else if (s->scheme == DT_SCHEME_DB) pick(std::integral_constant<int, DT_SCHEME_DB>{});
-            else pick(std::integral_constant<int, DT_SCHEME_DT>{});
+        if (db4) {
+            // Scheduler::doMcs (kpz/scheduler.cu:37-52): 2^L_MCS_DIV = 2 launches per MCS, each
+            // over every block from a random origin in [0, block) sites
+            for (int a = 0; a < 2; ++a) {
+                const uint32_t ctr[4] = {(uint32_t)a, t, TAG_DB4_ORIGIN << 24, stream};
+                uint32_t r[4];
+                philox_host(ctr, seed, r);
+                launch((int)(r[0] & (uint32_t)(DT_BX - 1)), (int)(r[1] & (uint32_t)(DT_BY - 1)), a, t);
+            }
+        } else {
+            int ox, oy, order[4];
+            dt_plan(seed, stream, t, &ox, &oy, order);
+            for (int a = 0; a < 4; ++a) launch(ox, oy, order[a], t);
         }
         const cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess) return cuda_fail(e, "dt_kernel");

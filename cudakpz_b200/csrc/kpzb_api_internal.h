@@ -40,13 +40,22 @@ cudaError_t tune_plan(uint32_t* d_src, int lx, int ly, uint64_t seed, uint32_t s
 void philox_host(const uint32_t ctr[4], uint64_t seed, uint32_t out[4]);
 
 // Double-tiling random-sequential scheduler state (dt.cu).
-enum DtScheme { DT_SCHEME_DT = 0, DT_SCHEME_DBSH = 1, DT_SCHEME_DB = 2 };
+// DT_SCHEME_DB4 is not an inner scheme of DT but the reference's DB4 scheduler
+// (Kpz::Scheduler<Rng, LocalLayoutDB4>): every block at once behind a dead border.
+enum DtScheme {
+    DT_SCHEME_DT = 0,
+    DT_SCHEME_DBSH = 1,
+    DT_SCHEME_DB = 2,
+    DT_SCHEME_DTDBSH = 3,
+    DT_SCHEME_DBSHREP = 4,
+    DT_SCHEME_DB4 = 5
+};
 struct DtState {
     int grid = 0;
     bool ready = false;
     int scheme = DT_SCHEME_DT;  // inner decomposition of a block
 };
-kpzb_status dt_init(DtState* s, int lx, int ly, int sm_count);
+kpzb_status dt_init(DtState* s, int lx, int ly, int sm_count, bool db4 = false);
 void dt_free(DtState* s);
 // dis (optional): ENC_LOCAL rate-class words; dis_Tp / dis_Tq: the four classes' thresholds
 kpzb_status dt_enqueue(DtState* s, uint32_t* d_local, int lx, int ly, uint64_t t0, int n,

@@ -22,10 +22,13 @@ ENC_LOCAL = _lib.ENC_LOCAL
 ENC_CBBIT = _lib.ENC_CBBIT
 
 # --scheduler names of kpz/kpzFrontend.cpp:355-403
-_DYN = {"sca": _lib.DYN_SCA, "scaBit": _lib.DYN_SCABIT, "dt": _lib.DYN_DT}
+_DYN = {"sca": _lib.DYN_SCA, "scaBit": _lib.DYN_SCABIT, "dt": _lib.DYN_DT, "db4": _lib.DYN_DB4}
 # setPQDefault of each scheduler (kpz/schedulerSCA.h:37-39, kpz/schedulerSCABit.h:35-37);
-# the DT scheduler's mcs() runs the p=1, q=0 SyncRng core (kpz/kpz.cu:208-216)
-_DEFAULT_PQ = {_lib.DYN_SCA: (0.95, 0.0), _lib.DYN_SCABIT: (0.5, 0.0), _lib.DYN_DT: (1.0, 0.0)}
+# the DT and DB4 schedulers' mcs() run the p=1, q=0 SyncRng core (kpz/kpz.cu:157-162,208-216)
+_DEFAULT_PQ = {_lib.DYN_SCA: (0.95, 0.0), _lib.DYN_SCABIT: (0.5, 0.0), _lib.DYN_DT: (1.0, 0.0),
+               _lib.DYN_DB4: (1.0, 0.0)}
+# KPZ_INNER_DD of the reference (kpz/kpzConst.h:26-35) -> kpzb_set_dt_inner
+_DT_INNER = {"dt": 0, "dbsh": 1, "db": 2, "dtdbsh": 3, "dbshrep": 4}
 
 
 @dataclass
@@ -44,7 +47,8 @@ class Roughness:
 
 
 class Scheduler:
-    """One lattice on one GPU.  ``scheduler`` is one of ``"sca"``, ``"scaBit"``, ``"dt"``."""
+    """One lattice on one GPU.  ``scheduler`` is one of ``"sca"``, ``"scaBit"``, ``"dt"``,
+    ``"db4"``."""
 
     def __init__(self, lx: int, ly: Optional[int] = None, scheduler: str = "scaBit",
                  device: int = 0):
@@ -107,8 +111,18 @@ class Scheduler:
 
     def setDtInner(self, inner: str) -> None:
         """DT handles: "dt" (single-hit double tiling, default), "dbsh" (the reference's
-        default single-hit dead border inner decomposition) or "db" (dead border, no offset)."""
-        check(lib.kpzb_set_dt_inner(self._h, {"dt": 0, "dbsh": 1, "db": 2}[inner]), "kpzb_set_dt_inner")
+        default single-hit dead border inner decomposition), "db" (dead border, no offset),
+        "dtdbsh" (double tiling with a per-round cell offset) or "dbshrep" (DBSH with the
+        border hits replaced after the rounds)."""
+        if inner not in _DT_INNER:
+            raise ValueError(f"unknown DT inner scheme {inner!r}; expected one of {sorted(_DT_INNER)}")
+        check(lib.kpzb_set_dt_inner(self._h, _DT_INNER[inner]), "kpzb_set_dt_inner")
+
+    def mcsScale(self) -> float:
+        """SchedulerService::mcsScale (kpz/schedulerService.h:241)."""
+        s = C.c_double()
+        check(lib.kpzb_mcs_scale(self._h, C.byref(s)), "kpzb_mcs_scale")
+        return s.value
 
     def setDisorder(self, words: np.ndarray) -> None:
         """Quenched disorder classes, ENC_LOCAL words (SchedulerService::m_disorder)."""

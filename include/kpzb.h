@@ -45,7 +45,9 @@ enum { KPZB_ENC_LOCAL = 0, KPZB_ENC_CBBIT = 1 };
 enum {
     KPZB_DYN_SCA = 0,    /* Kpz::SchedulerSCA: checkerboard SCA, ENC_LOCAL push/pop      */
     KPZB_DYN_SCABIT = 1, /* Kpz::SchedulerSCABit: bit-vectorised SCA, ENC_CBBIT push/pop */
-    KPZB_DYN_DT = 2      /* Kpz::SchedulerDT: double-tiling random-sequential, ENC_LOCAL */
+    KPZB_DYN_DT = 2,     /* Kpz::SchedulerDT: double-tiling random-sequential, ENC_LOCAL */
+    KPZB_DYN_DB4 = 3     /* Kpz::Scheduler<Rng, LocalLayoutDB4> ("db4", kpz/scheduler.cu): all
+                            256x128-site blocks at once behind a 5-site dead border, ENC_LOCAL */
 };
 
 typedef struct kpzb_handle kpzb_handle;
@@ -65,7 +67,8 @@ kpzb_status kpzb_probe_alu_peak(int device, double* lop3_per_s, double* iadd3_pe
  * Replaces SchedulerSCA/SchedulerSCABit/SchedulerDT constructors + SchedulerBase::initCUDA
  * (kpz/schedulerSCABit.cu:84-88, kpz/schedulerBase.cu:65-74, kpz/schedulerDT.cu:93-118).
  * Limits: 8 <= lx <= 30, 2 <= ly <= 30, 14 <= lx + ly <= 38; DT also needs lx >= 9 and
- * ly >= 8 (one double tile of 512x256 sites).  The lattice starts flat. */
+ * ly >= 8 (one double tile of 512x256 sites), DB4 ly >= 7 (one block of 256x128 sites).
+ * The lattice starts flat. */
 kpzb_status kpzb_create(kpzb_handle** h, int lx, int ly, int dynamics, int device);
 kpzb_status kpzb_destroy(kpzb_handle* h);
 
@@ -82,10 +85,26 @@ kpzb_status kpzb_seed(kpzb_handle* h, uint64_t seed, uint32_t stream);
 /* DT only: the inner decomposition of a block, the reference's compile-time KPZ_INNER_DD
  * (kpz/param.h, kpz/kpzConst.h:26-35): KPZB_DT_INNER_DT (single-hit double tiling, the
  * default here), KPZB_DT_INNER_DBSH (single-hit dead border, the reference's default:
- * BaseDTInnerDBSH, kpz/kpzSimulationPrimitivesTemplates_BaseInnerDB.cu:110-163) or
- * KPZB_DT_INNER_DB (dead border without the per-round cell offset: BaseDTInnerDB, :30-74). */
-enum { KPZB_DT_INNER_DT = 0, KPZB_DT_INNER_DBSH = 1, KPZB_DT_INNER_DB = 2 };
+ * BaseDTInnerDBSH, kpz/kpzSimulationPrimitivesTemplates_BaseInnerDB.cu:110-163),
+ * KPZB_DT_INNER_DB (dead border without the per-round cell offset: BaseDTInnerDB, :30-74),
+ * KPZB_DT_INNER_DTDBSH (double tiling with a random per-round cell offset:
+ * BaseDTInnerDTDBSH, kpz/kpzSimulationPrimitivesTemplates_BaseInnerDTr.cu:30-85) or
+ * KPZB_DT_INNER_DBSHREP (DBSH with border hits replaced by fresh attempts after the rounds:
+ * BaseDTInnerDBSHRep, kpz/kpzSimulationPrimitivesTemplates_BaseInnerDB.cu:165-268).  The
+ * scheme is saved in checkpoints. */
+enum {
+    KPZB_DT_INNER_DT = 0,
+    KPZB_DT_INNER_DBSH = 1,
+    KPZB_DT_INNER_DB = 2,
+    KPZB_DT_INNER_DTDBSH = 3,
+    KPZB_DT_INNER_DBSHREP = 4
+};
 kpzb_status kpzb_set_dt_inner(kpzb_handle* h, int inner);
+/* SchedulerService::mcsScale (kpz/schedulerService.h:241): the factor the frontend reports
+ * beside MCS counts -- p + q of rate class 0 for SCA/SCABit (kpz/schedulerSCA.cu:36-39,
+ * kpz/schedulerSCABit.cu:39-42), the active fraction (256-5)(128-5)/(256*128) of a block for
+ * DB4 (kpz/scheduler.cu:57-65), 1 for DT. */
+kpzb_status kpzb_mcs_scale(kpzb_handle* h, double* scale);
 /* SchedulerService::setPQ(p, q, n) for rate class n = 0..3 (kpz/schedulerService.h:186-192):
  * the rates a site of disorder class n uses in kpzb_mcs_disorder; class 0 is kpzb_set_pq's.
  * Classes never set follow class 0. */

@@ -35,7 +35,7 @@ struct Roughness {
 class Scheduler {
 public:
     enum Encoding { ENC_LOCAL = KPZB_ENC_LOCAL, ENC_CBBIT = KPZB_ENC_CBBIT };
-    enum Dynamics { SCA = KPZB_DYN_SCA, SCABIT = KPZB_DYN_SCABIT, DT = KPZB_DYN_DT };
+    enum Dynamics { SCA = KPZB_DYN_SCA, SCABIT = KPZB_DYN_SCABIT, DT = KPZB_DYN_DT, DB4 = KPZB_DYN_DB4 };
 
     Scheduler(int lx, int ly, Dynamics dyn = SCABIT, int device = -1) : dyn_(dyn)
     {
@@ -67,6 +67,15 @@ public:
     {
         if (words.size() != sizeW()) throw Error(KPZB_EINVAL, "setDisorder: one word per lattice word");
         check(kpzb_set_disorder(h_, words.data()), "kpzb_set_disorder");
+    }
+    // DT: the block-level decomposition (KPZB_DT_INNER_*; the reference's KPZ_INNER_DD)
+    void setDtInner(int inner) { check(kpzb_set_dt_inner(h_, inner), "kpzb_set_dt_inner"); }
+    // SchedulerService::mcsScale (kpz/schedulerService.h:241)
+    double mcsScale() const
+    {
+        double s = 1.0;
+        check(kpzb_mcs_scale(h_, &s), "kpzb_mcs_scale");
+        return s;
     }
     double rateP() const { return p_; }
     double rateQ() const { return q_; }
@@ -181,7 +190,7 @@ public:
 
 private:
     // setPQDefault of each scheduler (kpz/schedulerSCA.h:37-39, kpz/schedulerSCABit.h:35-37);
-    // SchedulerDT::mcs runs the p=1, q=0 core (kpz/kpz.cu:208-216)
+    // SchedulerDT::mcs and Scheduler (DB4)::mcs run the p=1, q=0 core (kpz/kpz.cu:157-162,208-216)
     void setPQDefault()
     {
         if (dyn_ == SCA) setPQ(0.95, 0.0);

@@ -155,6 +155,11 @@ def patch_gpu(work: Path) -> None:
     t = (t[:a] + "\ttemplate class SchedulerDT<SLCG64, SchedulerDT_LocalLayoutDis>;\n"
          "\ttemplate class SchedulerDT<TinyMT32, SchedulerDT_LocalLayoutDis>;\n" + t[b:])
     di.write_text(t)
+    # BaseDTInnerDBSHRep's warp reduction uses the pre-CUDA-9 __shfl_xor, which does not exist
+    # for sm_70 and later; the full-warp __shfl_xor_sync is the same butterfly
+    ib = work / "kpz/kpzSimulationPrimitivesTemplates_BaseInnerDB.cu"
+    t = ib.read_text()
+    ib.write_text(t.replace("__shfl_xor(borderHits, a, 32)", "__shfl_xor_sync(0xffffffffu, borderHits, a, 32)"))
 
 
 def build_gpu(cpu_objs: list[str]) -> None:
@@ -181,14 +186,14 @@ def build_gpu(cpu_objs: list[str]) -> None:
     subprocess.run([NVCC, "-gencode", "arch=compute_100a,code=sm_100a", "-o", str(OUT / "kpz_ref_gpu"),
                     str(drv), *objs, *cpu, "-Xcompiler", "-pthread", "-lcudart"], check=True)
     print(f"built {OUT / 'kpz_ref_gpu'}")
-    # second build with the reference's single-hit double-tiling inner scheme (KPZ_INNER_DT,
-    # kpz/kpzConst.h:26) instead of its default DBSH (kpz/param.h), the scheme the DT kernel
-    # here follows: a like-for-like statistical comparison of the two DT implementations
     # further builds with the other inner schemes the DT kernel here implements: single-hit
-    # double tiling (KPZ_INNER_DT) and dead border (KPZ_INNER_DB), kpz/kpzConst.h:26-35
+    # double tiling (KPZ_INNER_DT), dead border (KPZ_INNER_DB), double tiling with a random cell
+    # offset (KPZ_INNER_DTDBSH) and DBSH with replaced borders (KPZ_INNER_DBSHREP),
+    # kpz/kpzConst.h:26-35
     param = WORK / "kpz/param.h"
     t = param.read_text()
-    for tag, dd in (("innerdt", "KPZ_INNER_DT"), ("innerdb", "KPZ_INNER_DB")):
+    for tag, dd in (("innerdt", "KPZ_INNER_DT"), ("innerdb", "KPZ_INNER_DB"), ("innerdtdbsh", "KPZ_INNER_DTDBSH"),
+                    ("innerdbshrep", "KPZ_INNER_DBSHREP")):
         param.write_text(t.replace("#define KPZ_INNER_DD KPZ_INNER_DBSH", f"#define KPZ_INNER_DD {dd}"))
         objs2 = []
         for src in GPU_SOURCES:
@@ -200,6 +205,23 @@ def build_gpu(cpu_objs: list[str]) -> None:
                         str(drv), *objs2, *cpu, "-Xcompiler", "-pthread", "-lcudart"], check=True)
         print(f"built {OUT / f'kpz_ref_gpu_{tag}'}")
     param.write_text(t)
+
+
+def build_adapter(cpu_objs: list[str], flags: list[str]) -> None:
+    """tests/cpp/scheduler_b200_adapter.cpp -- a SchedulerService subclass forwarding to this
+    library's C ABI -- against the reference's headers and CPU objects, into
+    oracle/_ref/kpz_ref_adapter (needs cudakpz_b200/libkpzb200.so, built first)."""
+    lib = HERE.parent / "cudakpz_b200" / "libkpzb200.so"
+    if not lib.exists():
+        print("libkpzb200.so not built; skipping the adapter", file=sys.stderr)
+        return
+    src = HERE.parent / "tests" / "cpp" / "scheduler_b200_adapter.cpp"
+    obj = WORK / "scheduler_b200_adapter.o"
+    subprocess.run(["g++", *flags, f"-I{HERE.parent / 'include'}", "-c", str(src), "-o", str(obj)], check=True)
+    cpu = [o for o in cpu_objs if not o.endswith("ref_driver.o")]
+    subprocess.run(["g++", "-pthread", "-o", str(OUT / "kpz_ref_adapter"), str(obj), *cpu,
+                    f"-L{lib.parent}", "-lkpzb200", f"-Wl,-rpath,{lib.parent}"], check=True)
+    print(f"built {OUT / 'kpz_ref_adapter'}")
 
 
 def main() -> int:
@@ -227,6 +249,7 @@ def main() -> int:
     subprocess.run(["g++", *flags, "-c", str(HERE / "ref_driver.cpp"), "-o", str(drv)], check=True)
     subprocess.run(["g++", "-pthread", "-o", str(OUT / "kpz_ref"), str(drv), *objs], check=True)
     print(f"built {OUT / 'kpz_ref'}")
+    build_adapter(objs, flags)
     build_gpu(objs)
     return 0
 

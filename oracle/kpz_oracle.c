@@ -584,6 +584,218 @@ static void dt_mcs_border(uint32_t* w, int lx, int ly, uint64_t seed, uint32_t s
     if (des) *des += nr;
 }
 
+/* Single-hit double tiling with a block-wide random offset of the thread cells per round
+ * (BaseDTInnerDTDBSH::systemLoopDC, kpz/kpzSimulationPrimitivesTemplates_BaseInnerDTr.cu:
+ * 56-83): per round the DT sub-cell (as ko_dt_mcs_dis) and an offset (ox_r, oy_r) in [0,8)^2
+ * (the DBSH offset byte of dt_mcs_border); the site's in-block coordinates wrap modulo the
+ * block before the origin's in-word offset (X0 & 3) is added; positions and acceptance words
+ * as ko_dt_mcs_dis. */
+void ko_dt_mcs_dtdbsh(uint32_t* w, int lx, int ly, uint64_t seed, uint32_t stream, uint64_t t0, int n,
+                      const double p[4], const double q[4], const uint32_t* dis, int64_t* dep, int64_t* des)
+{
+    const int L = 1 << lx, M = 1 << ly;
+    const int BX = 256, BY = 128;
+    const int nbx = L / (2 * BX), nby = M / (2 * BY);
+    uint64_t Tpc[4], Tqc[4];
+    for (int c = 0; c < 4; ++c) {
+        Tpc[c] = ko_threshold(p[c]);
+        Tqc[c] = ko_threshold(q[c]);
+    }
+    int64_t nd = 0, nr = 0;
+    for (int i = 0; i < n; ++i) {
+        const uint64_t t = t0 + (uint64_t)i;
+        int ox, oy, order[4];
+        ko_dt_plan(seed, stream, t, &ox, &oy, order);
+        for (int a = 0; a < 4; ++a) {
+            const int d = order[a];
+            for (int b = 0; b < nbx * nby; ++b) {
+                const int bx = b % nbx, by = b / nbx;
+                const int X0 = ox + (2 * bx + (d & 1)) * BX;
+                const int Y0 = oy + (2 * by + (d >> 1)) * BY;
+                uint32_t sub[4];
+                philox_u32(seed, (uint32_t)b, (uint32_t)t, (KO_TAG_DT_SUB << 24) | ((uint32_t)d << 16), stream, sub);
+                for (int r = 0; r < 64; ++r) {
+                    const int s = (int)((sub[r >> 4] >> (2 * (r & 15))) & 3u);
+                    uint32_t ow[4];
+                    philox_u32(seed, (uint32_t)b, (uint32_t)t,
+                               (KO_TAG_DBSH_ORIGIN << 24) | ((uint32_t)d << 16) | (uint32_t)(r >> 4), stream, ow);
+                    const uint32_t ob = (ow[(r & 15) >> 2] >> (8 * (r & 3))) & 0xFFu;
+                    const int orx = (int)(ob & 7u), ory = (int)((ob >> 3) & 7u);
+                    for (int cell = 0; cell < 512; ++cell) {
+                        const int tx = cell & 31, ty = cell >> 5;
+                        const uint32_t cid = (uint32_t)b * 512u + (uint32_t)cell;
+                        uint32_t pw[4], uw[4];
+                        philox_u32(seed, cid, (uint32_t)t,
+                                   (KO_TAG_DT_POS << 24) | ((uint32_t)d << 16) | (uint32_t)(r >> 5), stream, pw);
+                        const int pos = (int)((pw[(r & 31) >> 3] >> (4 * (r & 7))) & 15u);
+                        const int xt = ((tx * 8 + (s & 1) * 4 + (pos & 3) + orx) & (BX - 1)) + (X0 & 3);
+                        const int yt = ((ty * 8 + (s >> 1) * 4 + (pos >> 2) + ory) & (BY - 1)) + (Y0 & 3);
+                        const int x = ((X0 & ~3) + xt) & (L - 1);
+                        const int y = ((Y0 & ~3) + yt) & (M - 1);
+                        philox_u32(seed, cid, (uint32_t)t, (KO_TAG_DT << 24) | ((uint32_t)d << 16) | (uint32_t)(r >> 2),
+                                   stream, uw);
+                        dt_attempt(w, lx, ly, x, y, Tpc, Tqc, dis, uw[r & 3], &nd, &nr);
+                    }
+                }
+            }
+        }
+    }
+    if (dep) *dep += nd;
+    if (des) *des += nr;
+}
+
+/* DBSH with out-of-sequence replaced borders (BaseDTInnerDBSHRep::systemLoopDC,
+ * kpz/kpzSimulationPrimitivesTemplates_BaseInnerDB.cu:184-268): the 64 rounds of
+ * dt_mcs_border, but a site on its shifted cell's last column or row is not updated; each
+ * thread counts such hits.  The block then makes R fresh attempts, where R is formed as the
+ * reference's reduction forms it (:214-227): thread 0's own count plus the counts of threads
+ * 32..511 (the hits of threads 1..31 are not repeated).  Repetition round k (512 attempts,
+ * thread c active while 512k + c < R) draws a new block offset, a new position per active
+ * thread and runs the three phases of dt_mcs_border.  Counter stream of the repetition:
+ * offset byte k&15 of Philox(ctr=(block, t, TAG_REP_ORIGIN<<24 | d<<16 | k>>4, stream)),
+ * position byte k&15 of (cell, t, TAG_REP_POS<<24 | d<<16 | k>>4), acceptance word k&3 of
+ * (cell, t, TAG_REP_U<<24 | d<<16 | k>>2). */
+void ko_dt_mcs_dbshrep(uint32_t* w, int lx, int ly, uint64_t seed, uint32_t stream, uint64_t t0, int n,
+                       const double p[4], const double q[4], const uint32_t* dis, int64_t* dep, int64_t* des)
+{
+    const int L = 1 << lx, M = 1 << ly;
+    const int BX = 256, BY = 128;
+    const int nbx = L / (2 * BX), nby = M / (2 * BY);
+    uint64_t Tpc[4], Tqc[4];
+    for (int c = 0; c < 4; ++c) {
+        Tpc[c] = ko_threshold(p[c]);
+        Tqc[c] = ko_threshold(q[c]);
+    }
+    int64_t nd = 0, nr = 0;
+    uint32_t hits[512];
+    for (int i = 0; i < n; ++i) {
+        const uint64_t t = t0 + (uint64_t)i;
+        int ox, oy, order[4];
+        ko_dt_plan(seed, stream, t, &ox, &oy, order);
+        for (int a = 0; a < 4; ++a) {
+            const int d = order[a];
+            for (int b = 0; b < nbx * nby; ++b) {
+                const int bx = b % nbx, by = b / nbx;
+                const int X0 = ox + (2 * bx + (d & 1)) * BX;
+                const int Y0 = oy + (2 * by + (d >> 1)) * BY;
+                for (int c = 0; c < 512; ++c) hits[c] = 0;
+                for (int r = 0; r < 64; ++r) {
+                    uint32_t ow[4];
+                    philox_u32(seed, (uint32_t)b, (uint32_t)t,
+                               (KO_TAG_DBSH_ORIGIN << 24) | ((uint32_t)d << 16) | (uint32_t)(r >> 4), stream, ow);
+                    const uint32_t ob = (ow[(r & 15) >> 2] >> (8 * (r & 3))) & 0xFFu;
+                    for (int cell = 0; cell < 512; ++cell) {
+                        const int tx = cell & 31, ty = cell >> 5;
+                        const uint32_t cid = (uint32_t)b * 512u + (uint32_t)cell;
+                        uint32_t pw[4], uw[4];
+                        philox_u32(seed, cid, (uint32_t)t,
+                                   (KO_TAG_DBSH_POS << 24) | ((uint32_t)d << 16) | (uint32_t)(r >> 4), stream, pw);
+                        const uint32_t pb = (pw[(r & 15) >> 2] >> (8 * (r & 3))) & 0xFFu;
+                        const int px = (int)(pb & 7u), py = (int)((pb >> 3) & 7u);
+                        if (px == 7 || py == 7) {
+                            ++hits[cell];
+                            continue;
+                        }
+                        const int xt = (tx * 8 + (X0 & 3) + px + (int)(ob & 7u)) & (BX - 1);
+                        const int yt = (ty * 8 + (Y0 & 3) + py + (int)((ob >> 3) & 7u)) & (BY - 1);
+                        philox_u32(seed, cid, (uint32_t)t, (KO_TAG_DT << 24) | ((uint32_t)d << 16) | (uint32_t)(r >> 2),
+                                   stream, uw);
+                        dt_attempt(w, lx, ly, ((X0 & ~3) + xt) & (L - 1), ((Y0 & ~3) + yt) & (M - 1), Tpc, Tqc, dis,
+                                   uw[r & 3], &nd, &nr);
+                    }
+                }
+                uint32_t R = hits[0];
+                for (int c = 32; c < 512; ++c) R += hits[c];
+                for (int k = 0; k * 512 < (int)R; ++k) {
+                    uint32_t ow[4];
+                    philox_u32(seed, (uint32_t)b, (uint32_t)t,
+                               (KO_TAG_REP_ORIGIN << 24) | ((uint32_t)d << 16) | (uint32_t)(k >> 4), stream, ow);
+                    const uint32_t ob = (ow[(k & 15) >> 2] >> (8 * (k & 3))) & 0xFFu;
+                    for (int phase = 0; phase < 3; ++phase)
+                        for (int cell = 0; cell < 512 && k * 512 + cell < (int)R; ++cell) {
+                            const int tx = cell & 31, ty = cell >> 5;
+                            const uint32_t cid = (uint32_t)b * 512u + (uint32_t)cell;
+                            uint32_t pw[4], uw[4];
+                            philox_u32(seed, cid, (uint32_t)t,
+                                       (KO_TAG_REP_POS << 24) | ((uint32_t)d << 16) | (uint32_t)(k >> 4), stream, pw);
+                            const uint32_t pb = (pw[(k & 15) >> 2] >> (8 * (k & 3))) & 0xFFu;
+                            const int px = (int)(pb & 7u), py = (int)((pb >> 3) & 7u);
+                            const int ph = (px == 7 && py == 7) ? 2 : (px == 7 || py == 7) ? 1 : 0;
+                            if (ph != phase) continue;
+                            const int xt = (tx * 8 + (X0 & 3) + px + (int)(ob & 7u)) & (BX - 1);
+                            const int yt = (ty * 8 + (Y0 & 3) + py + (int)((ob >> 3) & 7u)) & (BY - 1);
+                            philox_u32(seed, cid, (uint32_t)t,
+                                       (KO_TAG_REP_U << 24) | ((uint32_t)d << 16) | (uint32_t)(k >> 2), stream, uw);
+                            dt_attempt(w, lx, ly, ((X0 & ~3) + xt) & (L - 1), ((Y0 & ~3) + yt) & (M - 1), Tpc, Tqc,
+                                       dis, uw[k & 3], &nd, &nr);
+                        }
+                }
+            }
+        }
+    }
+    if (dep) *dep += nd;
+    if (des) *des += nr;
+}
+
+/* The DB4 scheduler (Kpz::Scheduler<Rng, LocalLayoutDB4>::doMcs, kpz/scheduler.cu:37-52;
+ * kpzKernelTemplate, kpz/kpz.cu:95-117; Base::systemLoopDC,
+ * kpz/kpzSimulationPrimitivesTemplates.cu:74-103): per MCS two launches a = 0, 1, each from a
+ * random origin (ox, oy) in [0,256) x [0,128) sites over every 256x128 block of the lattice
+ * (block (bx, by) starts at site (ox + 256 bx, oy + 128 by)); per launch 32 BaseDT rounds (a
+ * block-wide sub-cell, a position per thread cell in that quadrant), an attempt whose
+ * in-block position (before the origin's in-word offset) has x >= 251 or y >= 123 is skipped
+ * (LocalLayoutDB4::BLOCK_BORDER_WIDTH = 5, kpz/LocalLayout.h:120-131).  Counter stream:
+ *   origin       : Philox(ctr=(a, t, TAG_DB4_ORIGIN<<24, stream)) words 0, 1
+ *   sub-cells    : Philox(ctr=(block, t, TAG_DB4_SUB<<24 | a<<16, stream)), 2 bits per round
+ *   positions    : Philox(ctr=(cell, t, TAG_DB4_POS<<24 | a<<16 | r>>5, stream)), 4 bits/round
+ *   acceptance u : Philox(ctr=(cell, t, TAG_DB4_U<<24 | a<<16 | r>>2, stream)), word r&3 */
+void ko_db4_mcs(uint32_t* w, int lx, int ly, uint64_t seed, uint32_t stream, uint64_t t0, int n, double p,
+                double q, int64_t* dep, int64_t* des)
+{
+    const int L = 1 << lx, M = 1 << ly;
+    const int BX = 256, BY = 128;
+    const int nbx = L / BX, nby = M / BY;
+    uint64_t Tpc[4], Tqc[4];
+    for (int c = 0; c < 4; ++c) {
+        Tpc[c] = ko_threshold(p);
+        Tqc[c] = ko_threshold(q);
+    }
+    int64_t nd = 0, nr = 0;
+    for (int i = 0; i < n; ++i) {
+        const uint64_t t = t0 + (uint64_t)i;
+        for (int a = 0; a < 2; ++a) {
+            uint32_t o[4];
+            philox_u32(seed, (uint32_t)a, (uint32_t)t, KO_TAG_DB4_ORIGIN << 24, stream, o);
+            const int ox = (int)(o[0] & (uint32_t)(BX - 1)), oy = (int)(o[1] & (uint32_t)(BY - 1));
+            for (int b = 0; b < nbx * nby; ++b) {
+                const int bx = b % nbx, by = b / nbx;
+                const int X0 = ox + bx * BX, Y0 = oy + by * BY;
+                uint32_t sub[4];
+                philox_u32(seed, (uint32_t)b, (uint32_t)t, (KO_TAG_DB4_SUB << 24) | ((uint32_t)a << 16), stream, sub);
+                for (int r = 0; r < 32; ++r) {
+                    const int s = (int)((sub[r >> 4] >> (2 * (r & 15))) & 3u);
+                    for (int cell = 0; cell < 512; ++cell) {
+                        const int tx = cell & 31, ty = cell >> 5;
+                        const uint32_t cid = (uint32_t)b * 512u + (uint32_t)cell;
+                        uint32_t pw[4], uw[4];
+                        philox_u32(seed, cid, (uint32_t)t,
+                                   (KO_TAG_DB4_POS << 24) | ((uint32_t)a << 16) | (uint32_t)(r >> 5), stream, pw);
+                        const int pos = (int)((pw[(r & 31) >> 3] >> (4 * (r & 7))) & 15u);
+                        const int xl = tx * 8 + (s & 1) * 4 + (pos & 3), yl = ty * 8 + (s >> 1) * 4 + (pos >> 2);
+                        if (xl >= BX - 5 || yl >= BY - 5) continue;
+                        philox_u32(seed, cid, (uint32_t)t,
+                                   (KO_TAG_DB4_U << 24) | ((uint32_t)a << 16) | (uint32_t)(r >> 2), stream, uw);
+                        dt_attempt(w, lx, ly, (X0 + xl) & (L - 1), (Y0 + yl) & (M - 1), Tpc, Tqc, NULL, uw[r & 3],
+                                   &nd, &nr);
+                    }
+                }
+            }
+        }
+    }
+    if (dep) *dep += nd;
+    if (des) *des += nr;
+}
+
 /* ------------------------------------------------------------------------ */
 /* dSFMT-19937 (vendored BSD third-party code in the reference,             */
 /* inc/dSFMT/dSFMT.{h,cpp}, parameters inc/dSFMT/dSFMT-params19937.h;       */

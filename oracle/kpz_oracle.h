@@ -122,6 +122,23 @@ void ko_dt_mcs_dbsh(uint32_t* w, int lx, int ly, uint64_t seed, uint32_t stream,
 /* the dead-border scheme without the per-round cell offset (DB) */
 void ko_dt_mcs_db(uint32_t* w, int lx, int ly, uint64_t seed, uint32_t stream, uint64_t t0, int n,
                   const double p[4], const double q[4], const uint32_t* dis, int64_t* dep, int64_t* des);
+/* double tiling with a per-round block-wide offset of the thread cells (DTDBSH) */
+void ko_dt_mcs_dtdbsh(uint32_t* w, int lx, int ly, uint64_t seed, uint32_t stream, uint64_t t0, int n,
+                      const double p[4], const double q[4], const uint32_t* dis, int64_t* dep, int64_t* des);
+/* DBSH with border hits replaced by fresh attempts after the rounds (DBSHRep) */
+#define KO_TAG_REP_ORIGIN 9u
+#define KO_TAG_REP_POS 10u
+#define KO_TAG_REP_U 11u
+void ko_dt_mcs_dbshrep(uint32_t* w, int lx, int ly, uint64_t seed, uint32_t stream, uint64_t t0, int n,
+                       const double p[4], const double q[4], const uint32_t* dis, int64_t* dep, int64_t* des);
+/* the DB4 scheduler: all 256x128 blocks per launch behind a 5-site dead border, 2 launches
+ * of 32 BaseDT rounds per MCS; ENC_LOCAL lattice, lx >= 8, ly >= 7 */
+#define KO_TAG_DB4_ORIGIN 12u
+#define KO_TAG_DB4_SUB 13u
+#define KO_TAG_DB4_POS 14u
+#define KO_TAG_DB4_U 15u
+void ko_db4_mcs(uint32_t* w, int lx, int ly, uint64_t seed, uint32_t stream, uint64_t t0, int n, double p,
+                double q, int64_t* dep, int64_t* des);
 /* the per-MCS origin (sites) and domain-set order used by ko_dt_mcs */
 void ko_dt_plan(uint64_t seed, uint32_t stream, uint64_t t, int* ox, int* oy, int order[4]);
 

@@ -68,6 +68,12 @@ def _load():
                                   dblp, dblp, u32p, i64p, i64p]),
         "ko_dt_mcs_db": (None, [u32p, C.c_int, C.c_int, C.c_uint64, C.c_uint32, C.c_uint64, C.c_int,
                                 dblp, dblp, u32p, i64p, i64p]),
+        "ko_dt_mcs_dtdbsh": (None, [u32p, C.c_int, C.c_int, C.c_uint64, C.c_uint32, C.c_uint64, C.c_int,
+                                    dblp, dblp, u32p, i64p, i64p]),
+        "ko_dt_mcs_dbshrep": (None, [u32p, C.c_int, C.c_int, C.c_uint64, C.c_uint32, C.c_uint64, C.c_int,
+                                     dblp, dblp, u32p, i64p, i64p]),
+        "ko_db4_mcs": (None, [u32p, C.c_int, C.c_int, C.c_uint64, C.c_uint32, C.c_uint64, C.c_int,
+                              C.c_double, C.c_double, i64p, i64p]),
         "ko_generate_disorder2": (None, [u32p, C.c_int, C.c_int, C.c_void_p, C.c_double]),
         "ko_rs_mcs_dis": (None, [u32p, C.c_int, C.c_int, C.c_void_p, C.c_int, dblp, dblp, u32p, i64p,
                                  i64p]),
@@ -171,6 +177,27 @@ def dt_mcs_dbsh(w: np.ndarray, lx: int, ly: int, seed: int, stream: int, t0: int
     qq = q if isinstance(q, (list, tuple)) else [q]
     fn = lib.ko_dt_mcs_dbsh if shift else lib.ko_dt_mcs_db
     fn(_u32(w), lx, ly, seed, stream, t0, n, _rates4(pp), _rates4(qq), d, C.byref(dep), C.byref(des))
+    return dep.value, des.value
+
+
+def dt_mcs_inner(w: np.ndarray, lx: int, ly: int, seed: int, stream: int, t0: int, n: int, p, q,
+                 inner: str, dis: np.ndarray = None):
+    """DT with inner scheme "dt", "dbsh", "db", "dtdbsh" or "dbshrep", ENC_LOCAL, in place;
+    returns (#dep, #des)."""
+    fn = {"dt": lib.ko_dt_mcs_dis, "dbsh": lib.ko_dt_mcs_dbsh, "db": lib.ko_dt_mcs_db,
+          "dtdbsh": lib.ko_dt_mcs_dtdbsh, "dbshrep": lib.ko_dt_mcs_dbshrep}[inner]
+    dep, des = C.c_int64(0), C.c_int64(0)
+    d = None if dis is None else _u32(dis)
+    pp = p if isinstance(p, (list, tuple)) else [p]
+    qq = q if isinstance(q, (list, tuple)) else [q]
+    fn(_u32(w), lx, ly, seed, stream, t0, n, _rates4(pp), _rates4(qq), d, C.byref(dep), C.byref(des))
+    return dep.value, des.value
+
+
+def db4_mcs(w: np.ndarray, lx: int, ly: int, seed: int, stream: int, t0: int, n: int, p: float, q: float):
+    """The DB4 scheduler's MCS, ENC_LOCAL, in place; returns (#dep, #des)."""
+    dep, des = C.c_int64(0), C.c_int64(0)
+    lib.ko_db4_mcs(_u32(w), lx, ly, seed, stream, t0, n, p, q, C.byref(dep), C.byref(des))
     return dep.value, des.value
 
 

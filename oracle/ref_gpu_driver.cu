@@ -7,12 +7,16 @@
 // supplySeed, randomize, initHomogeneous, setPQ, mcsPQSyncRng, popSystem.
 //
 // and SchedulerDT<SLCG64, SchedulerDT_LocalLayoutDis> (kpz/schedulerDT.cu, kpz/kpz.cu, the
-// default DBSH inner decomposition of kpz/param.h) the same way.
+// default DBSH inner decomposition of kpz/param.h) and the DB4 scheduler
+// Scheduler<SLCG64, Scheduler_LocalLayoutDefault> (kpz/scheduler.cu, --scheduler db4 of
+// kpz/kpzFrontend.cpp:368-371) the same way.
 //
 // usage:
 //   kpz_ref_gpu scabit LX P Q WARMUP MCS   warm-up MCS, then MCS timed; prints
 //   kpz_ref_gpu dt LX P Q WARMUP MCS       "<attempted updates/ns> <seconds> <W2>"
+//   kpz_ref_gpu db4 LX P Q WARMUP MCS
 //   kpz_ref_gpu dtcurve LX P Q SEED T1 T2 ...      supplySeed(1, SEED); "<t> <W2> <h>" per time
+//   kpz_ref_gpu db4curve LX P Q SEED T1 T2 ...
 //   kpz_ref_gpu scabitcurve LX P Q SEED T1 T2 ...
 //   kpz_ref_gpu scabitdump LX P Q N FILE          lattice words after N MCS (flat start)
 #include <chrono>
@@ -25,6 +29,7 @@
 
 #include "GPURandom.h"
 #include "correlator.h"
+#include "scheduler.h"
 #include "schedulerDT.h"
 #include "schedulerSCABit.h"
 
@@ -97,12 +102,15 @@ int main(int argc, char** argv)
         return 2;
     }
     const std::string cmd = argv[1];
-    if ((cmd == "scabit" || cmd == "dt") && argc >= 7) {
+    if ((cmd == "scabit" || cmd == "dt" || cmd == "db4") && argc >= 7) {
         const int lx = std::atoi(argv[2]);
         const double p = std::atof(argv[3]), q = std::atof(argv[4]);
         const int warm = std::atoi(argv[5]), n = std::atoi(argv[6]);
         if (cmd == "scabit")
             return run<Kpz::SchedulerSCABit<SLCG64>>(lx, p, q, warm, n, Kpz::SchedulerService::ENC_CBBIT);
+        if (cmd == "db4")
+            return run<Kpz::Scheduler<SLCG64, Kpz::Scheduler_LocalLayoutDefault>>(lx, p, q, warm, n,
+                                                                               Kpz::SchedulerService::ENC_LOCAL);
         return run<Kpz::SchedulerDT<SLCG64, Kpz::SchedulerDT_LocalLayoutDis>>(lx, p, q, warm, n,
                                                                            Kpz::SchedulerService::ENC_LOCAL);
     }
@@ -129,13 +137,16 @@ int main(int argc, char** argv)
         std::fclose(f);
         return ok ? 0 : 3;
     }
-    if ((cmd == "dtcurve" || cmd == "scabitcurve") && argc >= 7) {
+    if ((cmd == "dtcurve" || cmd == "scabitcurve" || cmd == "db4curve") && argc >= 7) {
         const int lx = std::atoi(argv[2]);
         const double p = std::atof(argv[3]), q = std::atof(argv[4]);
         const int seed = std::atoi(argv[5]);
         if (cmd == "scabitcurve")
             return curve<Kpz::SchedulerSCABit<SLCG64>>(lx, p, q, seed, argv + 6, argc - 6,
                                                        Kpz::SchedulerService::ENC_CBBIT);
+        if (cmd == "db4curve")
+            return curve<Kpz::Scheduler<SLCG64, Kpz::Scheduler_LocalLayoutDefault>>(
+                lx, p, q, seed, argv + 6, argc - 6, Kpz::SchedulerService::ENC_LOCAL);
         return curve<Kpz::SchedulerDT<SLCG64, Kpz::SchedulerDT_LocalLayoutDis>>(lx, p, q, seed, argv + 6, argc - 6,
                                                                               Kpz::SchedulerService::ENC_LOCAL);
     }

@@ -160,3 +160,86 @@ def test_dbsh_with_disorder_and_stream(kpzb, oracle):
     got = s.popSystem()
     s.close()
     assert np.array_equal(got, ref)
+
+
+@pytest.mark.parametrize("inner", ["dtdbsh", "dbshrep"])
+@pytest.mark.parametrize("p,q", [(1.0, 0.0), (0.95, 0.05), (0.5, 0.5), (1.0, 1.0)])
+@pytest.mark.parametrize("lx,ly", [(9, 8), (10, 9)])
+def test_dtdbsh_dbshrep_bit_exact(kpzb, oracle, lx, ly, p, q, inner):
+    """The reference's other block-level decompositions -- double tiling with a per-round
+    cell offset (DTDBSH, plain read-modify-write: neighbouring sites of a round stay 4 sites
+    apart) and DBSH with replaced borders (DBSHRep, a data-dependent number of repetition
+    rounds) -- against their CPU emulations, word for word, with counters."""
+    n = 3
+    ref = oracle.homogeneous(lx, ly, oracle.ENC_LOCAL)
+    rc = oracle.dt_mcs_inner(ref, lx, ly, 42, 0, 0, n, p, q, inner)
+    s = kpzb.Scheduler(lx, ly, scheduler="dt")
+    s.setDtInner(inner)
+    s.setPQ(p, q)
+    s.supplySeed(42)
+    s.enableCounters(True)
+    s.mcsPQSyncRng(n)
+    got = s.popSystem()
+    cnt = s.counters()
+    s.close()
+    assert np.array_equal(got, ref)
+    assert cnt == rc
+
+
+@pytest.mark.parametrize("inner", ["dtdbsh", "dbshrep"])
+def test_dtdbsh_dbshrep_disorder_random_start(kpzb, oracle, inner):
+    lx, ly = 10, 9
+    dis = oracle.generate_disorder2(lx, ly, oracle.DSFMT(6), 0.4)
+    init = oracle.cbbit_to_local(oracle.random_lattice(lx, ly, oracle.ENC_CBBIT, seed=4, mcs=6), lx, ly)
+    ref = init.copy()
+    oracle.dt_mcs_inner(ref, lx, ly, 9, 2, 0, 3, [0.9, 0.4], [0.1, 0.5], inner, dis)
+    s = kpzb.Scheduler(lx, ly, scheduler="dt")
+    s.setDtInner(inner)
+    s.pushSystem(init)
+    s.setPQ(0.9, 0.1)
+    s.setPQ(0.4, 0.5, 1)
+    s.supplySeed(9, 2)
+    s.setDisorder(dis)
+    s.mcsDisorder2SyncRng(3)
+    got = s.popSystem()
+    s.close()
+    assert np.array_equal(got, ref)
+
+
+@pytest.mark.parametrize("p,q", [(1.0, 0.0), (0.95, 0.05), (0.5, 0.5), (1.0, 1.0)])
+@pytest.mark.parametrize("lx,ly", [(8, 7), (9, 9), (11, 10)])
+def test_db4_bit_exact(kpzb, oracle, lx, ly, p, q):
+    """The DB4 scheduler (all blocks per launch behind a 5-site dead border, no halo) against
+    its CPU emulation, word for word, with counters; a race between neighbouring blocks or an
+    update reaching the dead border would show as a differing word."""
+    n = 3
+    ref = oracle.homogeneous(lx, ly, oracle.ENC_LOCAL)
+    rc = oracle.db4_mcs(ref, lx, ly, 42, 0, 0, n, p, q)
+    s = kpzb.Scheduler(lx, ly, scheduler="db4")
+    s.setPQ(p, q)
+    s.supplySeed(42)
+    s.enableCounters(True)
+    s.mcsPQSyncRng(n)
+    got = s.popSystem()
+    cnt = s.counters()
+    assert s.mcsScale() == pytest.approx(251 * 123 / 32768)
+    s.close()
+    assert np.array_equal(got, ref)
+    assert cnt == rc
+
+
+def test_db4_random_start_stream_and_invariants(kpzb, oracle):
+    lx, ly = 10, 10
+    init = oracle.cbbit_to_local(oracle.random_lattice(lx, ly, oracle.ENC_CBBIT, seed=5, mcs=6), lx, ly)
+    ref = init.copy()
+    oracle.db4_mcs(ref, lx, ly, 7, 3, 0, 5, 0.9, 0.2)
+    s = kpzb.Scheduler(lx, ly, scheduler="db4")
+    s.pushSystem(init)
+    s.setPQ(0.9, 0.2)
+    s.supplySeed(7, 3)
+    s.mcsPQSyncRng(5)
+    assert np.array_equal(s.popSystem(), ref)
+    s.mcsPQSyncRng(20)
+    ok, rep = s.consitencyCheck()
+    assert ok, rep
+    s.close()

@@ -27,25 +27,34 @@ def beta_of(w2):
 REF_DBSH = REF.parent / "kpz_ref_gpu"
 
 
-@pytest.mark.parametrize("inner,binary", [("dt", REF), ("dbsh", REF_DBSH),
-                                          ("db", REF.parent / "kpz_ref_gpu_innerdb")])
-def test_dt_statistics_match_reference_gpu_dt(kpzb, inner, binary):
+@pytest.mark.parametrize("sched,inner,binary,cmd", [
+    ("dt", "dt", REF, "dtcurve"),
+    ("dt", "dbsh", REF_DBSH, "dtcurve"),
+    ("dt", "db", REF.parent / "kpz_ref_gpu_innerdb", "dtcurve"),
+    ("dt", "dtdbsh", REF.parent / "kpz_ref_gpu_innerdtdbsh", "dtcurve"),
+    ("dt", "dbshrep", REF.parent / "kpz_ref_gpu_innerdbshrep", "dtcurve"),
+    ("db4", None, REF_DBSH, "db4curve"),
+])
+def test_dt_statistics_match_reference_gpu_dt(kpzb, sched, inner, binary, cmd):
     """inner "dt": the reference built with KPZ_INNER_DT; "dbsh": its default build
-    (KPZ_INNER_DBSH, kpz/param.h); "db": built with KPZ_INNER_DB -- each against this
-    library's DT kernel with the same inner scheme."""
+    (KPZ_INNER_DBSH, kpz/param.h); "db", "dtdbsh", "dbshrep": built with KPZ_INNER_DB,
+    KPZ_INNER_DTDBSH, KPZ_INNER_DBSHREP -- each against this library's DT kernel with the same
+    inner scheme; "db4": the reference's DB4 scheduler (Scheduler<SLCG64, LocalLayoutDB4>,
+    --scheduler db4) against this library's."""
     if not binary.exists():
         pytest.skip("reference GPU DT not built (needs the CudaKpz sources)")
     ref = []
     for s in range(1, SEEDS + 1):
-        r = subprocess.run([str(binary), "dtcurve", str(LX), str(P), str(Q), str(s)] + [str(t) for t in TS],
+        r = subprocess.run([str(binary), cmd, str(LX), str(P), str(Q), str(s)] + [str(t) for t in TS],
                            capture_output=True, text=True, check=True, timeout=600)
         rows = [ln.split() for ln in r.stdout.splitlines() if ln and not ln.startswith("#")]
         assert [int(x[0]) for x in rows] == TS
         ref.append([float(x[1]) for x in rows])
     ours = []
     for s in range(1, SEEDS + 1):
-        h = kpzb.Scheduler(LX, LX, scheduler="dt")
-        h.setDtInner(inner)
+        h = kpzb.Scheduler(LX, LX, scheduler=sched)
+        if inner:
+            h.setDtInner(inner)
         h.setPQ(P, Q)
         h.supplySeed(1000 + s)
         t, cur = 0, []

@@ -101,7 +101,7 @@ __device__ __forceinline__ void dt_attempt_atomic(uint32_t* tile, const uint32_t
 //   DT_SCHEME_DB4     every block of the lattice in one launch, a dead border of 5 sites, the
 //                     inner rounds of BaseDT (32 per launch, two launches per MCS)
 template <bool COUNT, bool DIS, int SCHEME>
-__global__ void __launch_bounds__(DT_THREADS)
+__global__ void __launch_bounds__(DT_THREADS, 4)
 dt_kernel(uint32_t* __restrict__ sys, int lxw, int lyw, int lnbx, int nblocks, int ox, int oy,
           int d, uint32_t t, Key key, uint32_t stream, Thresh tp, Thresh tq,
           unsigned long long* __restrict__ counters, const uint32_t* __restrict__ dis, DisorderRates dr)
@@ -119,17 +119,24 @@ dt_kernel(uint32_t* __restrict__ sys, int lxw, int lyw, int lnbx, int nblocks, i
     __shared__ uint32_t rep_hits[REP ? DT_THREADS / 32 + 1 : 1];
     // Site geometry of every (sub-cell s, in-cell position pb) pair, relative to a thread's cell:
     // the origin's offset inside a word (ox & 3, oy & 3) is the same for every block and thread
-    // of the launch, so the word offsets and bit shifts of the site, its right neighbour and its
-    // lower neighbour form one 64-entry table:
-    //   bits 0-7 word offset, 8-12 site shift, 13-17 right-neighbour x-slope shift,
-    //   18-22 lower-neighbour y-slope shift, 23 right neighbour in the next word,
-    //   24 lower neighbour in the next word row.
-    __shared__ uint32_t lut[64];
+    // of the launch, so the tile words of the site, its right and its lower neighbour and the
+    // bit positions form one 64-entry table {w, w_right, w_down, rot}:
+    //   rot bits 0-7: the site's shift sh (its two slope bits rotate down to bits 0-1),
+    //   8-15: (shr - 2) mod 32 (the right neighbour's x-slope bit rotates to bit 2),
+    //   16-23: (shd - 3) mod 32 (the lower neighbour's y-slope bit rotates to bit 3),
+    //   24 / 25: the site lies at in-cell x >= 3 / y >= 3 (DB4's dead border for the last
+    //   thread column / row).
+    // A funnel shift uses its amount modulo 32, so each field needs no mask.
+    __shared__ uint4 lut[64];
     const int tid = threadIdx.y * DT_TX + threadIdx.x;
     const uint32_t Wx = 1u << lxw, Wy = 1u << lyw;
     const int ax = ox & 3, ay = oy & 3;
     bool need_u = !(tp.always || tp.planes == 0) || !(tq.always || tq.planes == 0);
     if (DIS) need_u = dr.planes > 0;
+    // the rule's candidates and acceptance limits: a site with configuration cfg_p (12, or an
+    // impossible 16 when p = 0) flips when u <= lim_p = T_p - 1; likewise q (cfg 3)
+    const uint32_t cfg_p = (tp.always || tp.planes) ? 12u : 16u, cfg_q = (tq.always || tq.planes) ? 3u : 16u;
+    const uint32_t lim_p = tp.always ? 0xFFFFFFFFu : tp.t - 1u, lim_q = tq.always ? 0xFFFFFFFFu : tq.t - 1u;
     unsigned long long ndep = 0, ndes = 0;
     if (tid < 64) {
         const int sc = tid >> 4, pb = tid & 15;
@@ -139,9 +146,15 @@ dt_kernel(uint32_t* __restrict__ sys, int lxw, int lyw, int lnbx, int nblocks, i
         const uint32_t sh = (uint32_t)((xb << 1) | (yb << 3));
         const uint32_t shr = (uint32_t)((((axx + 1) & 3) << 1) | (yb << 3));
         const uint32_t shd = (uint32_t)((xb << 1) | (((ayy + 1) & 3) << 3) | 1);
-        lut[tid] = (uint32_t)(row * DT_TW + col) | (sh << 8) | (shr << 13) | (shd << 18) |
-                   ((xb == 3 ? 1u : 0u) << 23) | ((yb == 3 ? 1u : 0u) << 24);
+        const int w = row * DT_TW + col;
+        // the last cell of a row starts 8 sites before the block's edge
+        const uint32_t fx = 4 * (sc & 1) + (pb & 3) >= 8 - DB4_BORDER ? 1u : 0u;
+        const uint32_t fy = 4 * (sc >> 1) + (pb >> 2) >= 8 - DB4_BORDER ? 1u : 0u;
+        lut[tid] = make_uint4((uint32_t)w, (uint32_t)(w + (xb == 3 ? 1 : 0)), (uint32_t)(w + (yb == 3 ? DT_TW : 0)),
+                              sh | (((shr - 2u) & 31u) << 8) | (((shd - 3u) & 31u) << 16) | (fx << 24) | (fy << 25));
     }
+    // DB4: the last thread column / row owns the block's dead border
+    const uint32_t dead_mask = (threadIdx.x == DT_TX - 1 ? 1u << 24 : 0u) | (threadIdx.y == DT_TY - 1 ? 1u << 25 : 0u);
     const int tbase = 2 * threadIdx.y * DT_TW + 2 * threadIdx.x;
 
     for (int b = blockIdx.x; b < nblocks; b += gridDim.x) {
@@ -269,9 +282,7 @@ dt_kernel(uint32_t* __restrict__ sys, int lxw, int lyw, int lnbx, int nblocks, i
                         make_uint4(cid, t, (T_U << 24) | ((uint32_t)d << 16) | (uint32_t)(r >> 2), stream), key);
                 const uint32_t sc = (sw >> (2 * (r & 15))) & 3u;
                 const uint32_t pb = (pw >> (4 * j)) & 15u;
-                int w;
-                uint32_t sh, shr, shd;
-                bool dxr, dyd, live = true;
+                const uint32_t u = pick4(uu, j & 3);
                 if (SHIFTED) {
                     // BaseDTInnerDTDBSH (kpz/kpzSimulationPrimitivesTemplates_BaseInnerDTr.cu:
                     // 30-85): the quadrant and a block-wide offset in [0,8)^2 per round, the
@@ -282,52 +293,40 @@ dt_kernel(uint32_t* __restrict__ sys, int lxw, int lyw, int lnbx, int nblocks, i
                                     (DT_BX - 1)) + ax;
                     const int yt = ((threadIdx.y * 8 + 2 * (int)(sc & 2u) + (int)(pb >> 2) + (int)((ob >> 3) & 7u)) &
                                     (DT_BY - 1)) + ay;
-                    w = (yt >> 2) * DT_TW + (xt >> 2);
-                    sh = (uint32_t)(((xt & 3) << 1) | ((yt & 3) << 3));
-                    shr = (uint32_t)((((xt + 1) & 3) << 1) | ((yt & 3) << 3));
-                    shd = (uint32_t)(((xt & 3) << 1) | (((yt + 1) & 3) << 3) | 1);
-                    dxr = (xt & 3) == 3;
-                    dyd = (yt & 3) == 3;
+                    dt_attempt_atomic<COUNT, DIS>(tile, dtile, xt, yt, u, tp, tq, dr, ndep, ndes);
                 } else {
-                    const uint32_t e = lut[sc * 16u + pb];
-                    w = tbase + (int)(e & 255u);
-                    sh = (e >> 8) & 31u;
-                    shr = (e >> 13) & 31u;
-                    shd = (e >> 18) & 31u;
-                    dxr = (e >> 23) & 1u;
-                    dyd = (e >> 24) & 1u;
-                    if (DB4)
-                        live = threadIdx.x * 8 + 4 * (int)(sc & 1u) + (int)(pb & 3u) < DT_BX - DB4_BORDER &&
-                               threadIdx.y * 8 + 2 * (int)(sc & 2u) + (int)(pb >> 2) < DT_BY - DB4_BORDER;
-                }
-                if (live) {
-                    uint32_t cw = tile[w];
-                    uint32_t rw = dxr ? tile[w + 1] : cw;
-                    uint32_t dw = dyd ? tile[w + DT_TW] : cw;
-                    const uint32_t c = (cw >> sh) & 3u, rbit = (rw >> shr) & 1u, lbit = (dw >> shd) & 1u;
-                    const bool is_p = c == 0u && rbit && lbit;      // local minimum (config 12)
-                    const bool is_q = c == 3u && !rbit && !lbit;    // local maximum (config 3)
-                    bool flip = false;
-                    if (is_p || is_q) {
-                        int cls = 0;
-                        if (DIS) cls = (int)((dtile[w] >> sh) & 3u);
-                        const Thresh& th = DIS ? (is_p ? dr.tp[cls] : dr.tq[cls]) : (is_p ? tp : tq);
-                        if (th.always) flip = true;
-                        else if (th.planes) flip = pick4(uu, j & 3) < th.t;
-                    }
-                    if (flip) {
-                        // the words of this round's site and neighbours belong to this thread alone
-                        cw ^= 3u << sh;
-                        if (dxr) rw ^= 1u << shr;
-                        else cw ^= 1u << shr;
-                        if (dyd) dw ^= 1u << shd;
-                        else cw ^= 1u << shd;
-                        tile[w] = cw;
-                        if (dxr) tile[w + 1] = rw;
-                        if (dyd) tile[w + DT_TW] = dw;
-                        if (COUNT) {
-                            if (is_p) ++ndep;
-                            else ++ndes;
+                    const uint4 e = lut[sc * 16u + pb];
+                    if (!DB4 || (e.w & dead_mask) == 0u) {
+                        const int w = tbase + (int)e.x, wr = tbase + (int)e.y, wd = tbase + (int)e.z;
+                        const uint32_t cw = tile[w], rw = tile[wr], dw = tile[wd];
+                        // configuration c | s_x(x+1)<<2 | s_y(y+1)<<3 (kpz/kpzSimulationPrimitivesTemplates.cu:
+                        // 258-260): three rotations by the table's amounts, one mask each
+                        const uint32_t cfg = (__funnelshift_r(cw, cw, e.w) & 3u) |
+                                             (__funnelshift_r(rw, rw, e.w >> 8) & 4u) |
+                                             (__funnelshift_r(dw, dw, e.w >> 16) & 8u);
+                        bool flip, is_p;
+                        if (DIS) {
+                            is_p = cfg == 12u;
+                            flip = false;
+                            if (is_p || cfg == 3u) {
+                                const int cls = (int)(__funnelshift_r(dtile[w], dtile[w], e.w) & 3u);
+                                const Thresh& th = is_p ? dr.tp[cls] : dr.tq[cls];
+                                flip = th.always || (th.planes && u < th.t);
+                            }
+                        } else {
+                            is_p = cfg == cfg_p;
+                            flip = (is_p || cfg == cfg_q) && u <= (is_p ? lim_p : lim_q);
+                        }
+                        if (flip) {
+                            // single hit: these words are this thread's alone in this round; the
+                            // atomics only serialise the three flips when two of them share a word
+                            atomicXor(&tile[w], 3u << (e.w & 31u));
+                            atomicXor(&tile[wr], __funnelshift_l(4u, 4u, e.w >> 8));
+                            atomicXor(&tile[wd], __funnelshift_l(8u, 8u, e.w >> 16));
+                            if (COUNT) {
+                                if (is_p) ++ndep;
+                                else ++ndes;
+                            }
                         }
                     }
                 }

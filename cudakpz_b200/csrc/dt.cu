@@ -89,6 +89,72 @@ __device__ __forceinline__ void dt_attempt_atomic(uint32_t* tile, const uint32_t
     }
 }
 
+// The rule's candidates and acceptance limits for the plain rates: a site of configuration
+// cfg_p (12, or an impossible 16 when p = 0) flips when its acceptance word u <= lim_p =
+// T_p - 1; likewise cfg_q (3).
+struct DtRule {
+    uint32_t cfg_p, cfg_q, lim_p, lim_q;
+};
+
+// One attempt of the random-sequential rule (PQSyncRng::update,
+// kpz/kpzSimulationPrimitivesTemplates.cu:250-281) at tile word w, its right neighbour's word
+// wr and its lower neighbour's word wd, with a site-table entry's rotate amounts (rot).
+template <bool COUNT, bool DIS>
+__device__ __forceinline__ void dt_attempt_at(uint32_t* tile, const uint32_t* dtile, int w, int wr, int wd,
+                                              uint32_t rot, uint32_t u, const DtRule rule, const DisorderRates& dr,
+                                              unsigned long long& ndep, unsigned long long& ndes)
+{
+    const uint32_t cw = tile[w], rw = tile[wr], dw = tile[wd];
+    // configuration c | s_x(x+1)<<2 | s_y(y+1)<<3 (kpz/kpzSimulationPrimitivesTemplates.cu:
+    // 258-260): three rotations by the table's amounts, one mask each
+    const uint32_t cfg = (__funnelshift_r(cw, cw, rot) & 3u) | (__funnelshift_r(rw, rw, rot >> 8) & 4u) |
+                         (__funnelshift_r(dw, dw, rot >> 16) & 8u);
+    bool flip, is_p;
+    if (DIS) {
+        is_p = cfg == 12u;
+        flip = false;
+        if (is_p || cfg == 3u) {
+            const int cls = (int)(__funnelshift_r(dtile[w], dtile[w], rot) & 3u);
+            const Thresh& th = is_p ? dr.tp[cls] : dr.tq[cls];
+            flip = th.always || (th.planes && u < th.t);
+        }
+    } else {
+        is_p = cfg == rule.cfg_p;
+        flip = (is_p || cfg == rule.cfg_q) && u <= (is_p ? rule.lim_p : rule.lim_q);
+    }
+    if (flip) {
+        // shared atomics: under the single-hit schemes only this thread touches these words in
+        // this round (the atomics merely order its own three flips when two share a word);
+        // under the dead-border schemes other threads' flips of the same phase may share them
+        // (the reference's fctAtomicXor)
+        atomicXor(&tile[w], 3u << (rot & 31u));
+        atomicXor(&tile[wr], __funnelshift_l(4u, 4u, rot >> 8));
+        atomicXor(&tile[wd], __funnelshift_l(8u, 8u, rot >> 16));
+        if (COUNT) {
+            if (is_p) ++ndep;
+            else ++ndes;
+        }
+    }
+}
+
+// Site-table entry of the site (vx, vy) sites right of and below a word (a thread cell's first
+// word, or the tile's): the tile words of the site, its right neighbour and its lower neighbour
+// relative to that word, and the rotate amounts
+//   bits 0-7: the site's shift sh (its two slope bits rotate down to bits 0-1),
+//   8-15: (shr - 2) mod 32 (the right neighbour's x-slope bit rotates to bit 2),
+//   16-23: (shd - 3) mod 32 (the lower neighbour's y-slope bit rotates to bit 3);
+// a funnel shift uses its amount modulo 32, so no field needs a mask.
+__device__ __forceinline__ uint4 site_entry(int vx, int vy)
+{
+    const uint32_t sh = (uint32_t)(((vx & 3) << 1) | ((vy & 3) << 3));
+    const uint32_t shr = (uint32_t)((((vx + 1) & 3) << 1) | ((vy & 3) << 3));
+    const uint32_t shd = (uint32_t)(((vx & 3) << 1) | (((vy + 1) & 3) << 3) | 1);
+    return make_uint4((uint32_t)((vy >> 2) * DT_TW + (vx >> 2)), (uint32_t)((vy >> 2) * DT_TW + ((vx + 1) >> 2)),
+                      (uint32_t)(((vy + 1) >> 2) * DT_TW + (vx >> 2)),
+                      sh | (((shr - 2u) & 31u) << 8) | (((shd - 3u) & 31u) << 16));
+}
+constexpr int DT_VSPAN = 18;  // in-cell offsets of the shifted schemes: up to 3 + 7 + 7 (or 4 + 3 + 7 + 3)
+
 // DIS: quenched disorder (Disorder2SyncRng_shared, kpz/kpzSimulationPrimitivesTemplates.cu:
 // 295-382): dis holds every site's 2-bit rate class in ENC_LOCAL words, copied into a second
 // shared tile beside the lattice's; the class picks dr.tp[c] / dr.tq[c].
@@ -110,6 +176,11 @@ dt_kernel(uint32_t* __restrict__ sys, int lxw, int lyw, int lnbx, int nblocks, i
     constexpr bool SHIFTED = SCHEME == DT_SCHEME_DTDBSH;
     constexpr bool REP = SCHEME == DT_SCHEME_DBSHREP;
     constexpr bool BORDER = SCHEME == DT_SCHEME_DBSH || SCHEME == DT_SCHEME_DB || REP;
+    // DT and DB4 index a 64-entry table by (quadrant, position): the origin's offset inside a
+    // word (ox & 3, oy & 3) is the launch's, so it is folded in.  DTDBSH, which shifts the cells
+    // per round, indexes an 18 x 18 table by the in-cell offset instead; the dead-border schemes
+    // compute their site's entry directly, once per round before the phases.
+    constexpr int NLUT = SHIFTED ? DT_VSPAN * DT_VSPAN : 64;
     constexpr int ROUNDS = DB4 ? DT_ROUNDS / 2 : DT_ROUNDS;
     constexpr uint32_t T_SUB = DB4 ? TAG_DB4_SUB : TAG_DT_SUB;
     constexpr uint32_t T_POS = DB4 ? TAG_DB4_POS : TAG_DT_POS;
@@ -117,45 +188,40 @@ dt_kernel(uint32_t* __restrict__ sys, int lxw, int lyw, int lnbx, int nblocks, i
     __shared__ uint32_t tile[DT_TH * DT_TW];
     __shared__ uint32_t dtile[DIS ? DT_TH * DT_TW : 1];
     __shared__ uint32_t rep_hits[REP ? DT_THREADS / 32 + 1 : 1];
-    // Site geometry of every (sub-cell s, in-cell position pb) pair, relative to a thread's cell:
-    // the origin's offset inside a word (ox & 3, oy & 3) is the same for every block and thread
-    // of the launch, so the tile words of the site, its right and its lower neighbour and the
-    // bit positions form one 64-entry table {w, w_right, w_down, rot}:
-    //   rot bits 0-7: the site's shift sh (its two slope bits rotate down to bits 0-1),
-    //   8-15: (shr - 2) mod 32 (the right neighbour's x-slope bit rotates to bit 2),
-    //   16-23: (shd - 3) mod 32 (the lower neighbour's y-slope bit rotates to bit 3),
-    //   24 / 25: the site lies at in-cell x >= 3 / y >= 3 (DB4's dead border for the last
-    //   thread column / row).
-    // A funnel shift uses its amount modulo 32, so each field needs no mask.
-    __shared__ uint4 lut[64];
+    __shared__ uint4 lut[NLUT];
     const int tid = threadIdx.y * DT_TX + threadIdx.x;
     const uint32_t Wx = 1u << lxw, Wy = 1u << lyw;
     const int ax = ox & 3, ay = oy & 3;
     bool need_u = !(tp.always || tp.planes == 0) || !(tq.always || tq.planes == 0);
     if (DIS) need_u = dr.planes > 0;
     // the rule's candidates and acceptance limits: a site with configuration cfg_p (12, or an
-    // impossible 16 when p = 0) flips when u <= lim_p = T_p - 1; likewise q (cfg 3)
+    // impossible 16 when p = 0) flips when u <= lim_p = T_p - 1; likewise q (configuration 3)
     const uint32_t cfg_p = (tp.always || tp.planes) ? 12u : 16u, cfg_q = (tq.always || tq.planes) ? 3u : 16u;
     const uint32_t lim_p = tp.always ? 0xFFFFFFFFu : tp.t - 1u, lim_q = tq.always ? 0xFFFFFFFFu : tq.t - 1u;
+    const DtRule rule{cfg_p, cfg_q, lim_p, lim_q};
     unsigned long long ndep = 0, ndes = 0;
-    if (tid < 64) {
-        const int sc = tid >> 4, pb = tid & 15;
-        const int axx = ax + (pb & 3), ayy = ay + (pb >> 2);
-        const int col = (sc & 1) + (axx >> 2), row = (sc >> 1) + (ayy >> 2);
-        const int xb = axx & 3, yb = ayy & 3;
-        const uint32_t sh = (uint32_t)((xb << 1) | (yb << 3));
-        const uint32_t shr = (uint32_t)((((axx + 1) & 3) << 1) | (yb << 3));
-        const uint32_t shd = (uint32_t)((xb << 1) | (((ayy + 1) & 3) << 3) | 1);
-        const int w = row * DT_TW + col;
-        // the last cell of a row starts 8 sites before the block's edge
-        const uint32_t fx = 4 * (sc & 1) + (pb & 3) >= 8 - DB4_BORDER ? 1u : 0u;
-        const uint32_t fy = 4 * (sc >> 1) + (pb >> 2) >= 8 - DB4_BORDER ? 1u : 0u;
-        lut[tid] = make_uint4((uint32_t)w, (uint32_t)(w + (xb == 3 ? 1 : 0)), (uint32_t)(w + (yb == 3 ? DT_TW : 0)),
-                              sh | (((shr - 2u) & 31u) << 8) | (((shd - 3u) & 31u) << 16) | (fx << 24) | (fy << 25));
+    if (NLUT == 64) {
+        if (tid < 64) {
+            // bits 24 / 25: the site lies at in-cell x / y >= 3, DB4's dead border when the cell
+            // is the block's last in its row / column (it starts 8 sites before the block's edge)
+            const int sc = tid >> 4, pb = tid & 15;
+            const int ux = 4 * (sc & 1) + (pb & 3), uy = 4 * (sc >> 1) + (pb >> 2);
+            uint4 e = site_entry(ux + ax, uy + ay);
+            e.w |= (ux >= 8 - DB4_BORDER ? 1u << 24 : 0u) | (uy >= 8 - DB4_BORDER ? 1u << 25 : 0u);
+            lut[tid] = e;
+        }
+    } else {
+        for (int i = tid; i < NLUT; i += DT_THREADS) lut[i] = site_entry(i % DT_VSPAN, i / DT_VSPAN);
     }
     // DB4: the last thread column / row owns the block's dead border
     const uint32_t dead_mask = (threadIdx.x == DT_TX - 1 ? 1u << 24 : 0u) | (threadIdx.y == DT_TY - 1 ? 1u << 25 : 0u);
     const int tbase = 2 * threadIdx.y * DT_TW + 2 * threadIdx.x;
+    // a shifted cell whose site passes the block's right / lower edge wraps to its left / upper
+    // edge (the reference masks coordinates with M_BLOCK_DIM): the cell's words move back by
+    // a block's width / height
+    auto wrapped_base = [&](int ex, int ey) {
+        return tbase - (threadIdx.x * 8 + ex >= DT_BX ? DT_BXW : 0) - (threadIdx.y * 8 + ey >= DT_BY ? DT_BYW * DT_TW : 0);
+    };
 
     for (int b = blockIdx.x; b < nblocks; b += gridDim.x) {
         const int bx = b & ((1 << lnbx) - 1), by = b >> lnbx;
@@ -182,7 +248,8 @@ dt_kernel(uint32_t* __restrict__ sys, int lxw, int lyw, int lnbx, int nblocks, i
             // kpz/kpzSimulationPrimitivesTemplates_BaseInnerDB.cu:110-163): per round one
             // block-wide offset shifts every thread cell, each thread picks a site of its shifted
             // cell, and sites on a cell's last column/row wait for phases 1 (off the corner) and
-            // 2 (the corner); the flips use shared-memory atomics as the reference's do.
+            // 2 (the corner); the flips use shared-memory atomics as the reference's do.  The
+            // site's words and rotations are found once per round, before the phases.
             // REP (BaseDTInnerDBSHRep, :175-268): a border hit is not done in its round but
             // counted, and after the 64 rounds the block makes that many fresh attempts, 512 per
             // repetition round, each again in the three phases.
@@ -204,19 +271,23 @@ dt_kernel(uint32_t* __restrict__ sys, int lxw, int lyw, int lnbx, int nblocks, i
                     const uint32_t pb = (pick4(pw, j >> 2) >> (8 * (j & 3))) & 0xFFu;
                     const int px = (int)(pb & 7u), py = (int)((pb >> 3) & 7u);
                     const int ph = (px == 7 && py == 7) ? 2 : (px == 7 || py == 7) ? 1 : 0;
-                    const int orx = SCHEME == DT_SCHEME_DB ? 0 : (int)(ob & 7u);
-                    const int ory = SCHEME == DT_SCHEME_DB ? 0 : (int)((ob >> 3) & 7u);
-                    const int xt = (threadIdx.x * 8 + ax + px + orx) & (DT_BX - 1);
-                    const int yt = (threadIdx.y * 8 + ay + py + ory) & (DT_BY - 1);
+                    const int xt = (threadIdx.x * 8 + ax + px + (SCHEME == DT_SCHEME_DB ? 0 : (int)(ob & 7u))) &
+                                   (DT_BX - 1);
+                    const int yt = (threadIdx.y * 8 + ay + py + (SCHEME == DT_SCHEME_DB ? 0 : (int)((ob >> 3) & 7u))) &
+                                   (DT_BY - 1);
                     const uint32_t u = pick4(uu, j & 3);
                     if (REP) {
+                        // one phase: the site's geometry is only needed inside it
                         if (ph == 0) dt_attempt_atomic<COUNT, DIS>(tile, dtile, xt, yt, u, tp, tq, dr, ndep, ndes);
                         else ++hits;
                         __syncthreads();
                     } else {
+                        // three phases: the site's words and rotations once, before them
+                        const uint4 e = site_entry(xt, yt);
                         for (int phase = 0; phase < 3; ++phase) {
                             if (ph == phase)
-                                dt_attempt_atomic<COUNT, DIS>(tile, dtile, xt, yt, u, tp, tq, dr, ndep, ndes);
+                                dt_attempt_at<COUNT, DIS>(tile, dtile, (int)e.x, (int)e.y, (int)e.z, e.w, u, rule, dr,
+                                                          ndep, ndes);
                             __syncthreads();
                         }
                     }
@@ -255,10 +326,12 @@ dt_kernel(uint32_t* __restrict__ sys, int lxw, int lyw, int lnbx, int nblocks, i
                     const int ph = !active ? 3 : (px == 7 && py == 7) ? 2 : (px == 7 || py == 7) ? 1 : 0;
                     const int xt = (threadIdx.x * 8 + ax + px + (int)(ob & 7u)) & (DT_BX - 1);
                     const int yt = (threadIdx.y * 8 + ay + py + (int)((ob >> 3) & 7u)) & (DT_BY - 1);
+                    const uint4 e = site_entry(xt, yt);
                     const uint32_t u = pick4(ruu, k & 3);
                     for (int phase = 0; phase < 3; ++phase) {
                         if (ph == phase)
-                            dt_attempt_atomic<COUNT, DIS>(tile, dtile, xt, yt, u, tp, tq, dr, ndep, ndes);
+                            dt_attempt_at<COUNT, DIS>(tile, dtile, (int)e.x, (int)e.y, (int)e.z, e.w, u, rule, dr, ndep,
+                                                      ndes);
                         __syncthreads();
                     }
                 }
@@ -289,18 +362,17 @@ dt_kernel(uint32_t* __restrict__ sys, int lxw, int lyw, int lnbx, int nblocks, i
                     // site wrapped inside the block before the origin's in-word offset is added;
                     // neighbouring threads' sites stay 4 or more sites apart, so no two share a word
                     const uint32_t ob = (pick4(ow, (r & 15) >> 2) >> (8 * (r & 3))) & 0xFFu;
-                    const int xt = ((threadIdx.x * 8 + 4 * (int)(sc & 1u) + (int)(pb & 3u) + (int)(ob & 7u)) &
-                                    (DT_BX - 1)) + ax;
-                    const int yt = ((threadIdx.y * 8 + 2 * (int)(sc & 2u) + (int)(pb >> 2) + (int)((ob >> 3) & 7u)) &
-                                    (DT_BY - 1)) + ay;
-                    dt_attempt_atomic<COUNT, DIS>(tile, dtile, xt, yt, u, tp, tq, dr, ndep, ndes);
+                    const int ux = 4 * (int)(sc & 1u) + (int)(pb & 3u) + (int)(ob & 7u);
+                    const int uy = 2 * (int)(sc & 2u) + (int)(pb >> 2) + (int)((ob >> 3) & 7u);
+                    const uint4 e = lut[(uy + ay) * DT_VSPAN + ux + ax];
+                    const int base = wrapped_base(ux, uy);
+                    dt_attempt_at<COUNT, DIS>(tile, dtile, base + (int)e.x, base + (int)e.y, base + (int)e.z, e.w, u,
+                                              rule, dr, ndep, ndes);
                 } else {
                     const uint4 e = lut[sc * 16u + pb];
                     if (!DB4 || (e.w & dead_mask) == 0u) {
                         const int w = tbase + (int)e.x, wr = tbase + (int)e.y, wd = tbase + (int)e.z;
                         const uint32_t cw = tile[w], rw = tile[wr], dw = tile[wd];
-                        // configuration c | s_x(x+1)<<2 | s_y(y+1)<<3 (kpz/kpzSimulationPrimitivesTemplates.cu:
-                        // 258-260): three rotations by the table's amounts, one mask each
                         const uint32_t cfg = (__funnelshift_r(cw, cw, e.w) & 3u) |
                                              (__funnelshift_r(rw, rw, e.w >> 8) & 4u) |
                                              (__funnelshift_r(dw, dw, e.w >> 16) & 8u);
@@ -318,8 +390,6 @@ dt_kernel(uint32_t* __restrict__ sys, int lxw, int lyw, int lnbx, int nblocks, i
                             flip = (is_p || cfg == cfg_q) && u <= (is_p ? lim_p : lim_q);
                         }
                         if (flip) {
-                            // single hit: these words are this thread's alone in this round; the
-                            // atomics only serialise the three flips when two of them share a word
                             atomicXor(&tile[w], 3u << (e.w & 31u));
                             atomicXor(&tile[wr], __funnelshift_l(4u, 4u, e.w >> 8));
                             atomicXor(&tile[wd], __funnelshift_l(8u, 8u, e.w >> 16));

@@ -98,23 +98,26 @@ struct DtRule {
 
 // One attempt of the random-sequential rule (PQSyncRng::update,
 // kpz/kpzSimulationPrimitivesTemplates.cu:250-281) at tile word w, its right neighbour's word
-// wr and its lower neighbour's word wd, with a site-table entry's rotate amounts (rot).
+// wr and its lower neighbour's word wd.  r1, r2, r3: rotate amounts (used modulo 32) that
+// bring the site's two slope bits to bits 0-1, the right neighbour's x-slope bit to bit 2 and
+// the lower neighbour's y-slope bit to bit 3.
 template <bool COUNT, bool DIS>
 __device__ __forceinline__ void dt_attempt_at(uint32_t* tile, const uint32_t* dtile, int w, int wr, int wd,
-                                              uint32_t rot, uint32_t u, const DtRule rule, const DisorderRates& dr,
-                                              unsigned long long& ndep, unsigned long long& ndes)
+                                              uint32_t r1, uint32_t r2, uint32_t r3, uint32_t u, const DtRule rule,
+                                              const DisorderRates& dr, unsigned long long& ndep,
+                                              unsigned long long& ndes)
 {
     const uint32_t cw = tile[w], rw = tile[wr], dw = tile[wd];
     // configuration c | s_x(x+1)<<2 | s_y(y+1)<<3 (kpz/kpzSimulationPrimitivesTemplates.cu:
-    // 258-260): three rotations by the table's amounts, one mask each
-    const uint32_t cfg = (__funnelshift_r(cw, cw, rot) & 3u) | (__funnelshift_r(rw, rw, rot >> 8) & 4u) |
-                         (__funnelshift_r(dw, dw, rot >> 16) & 8u);
+    // 258-260): three rotations, one mask each
+    const uint32_t cfg = (__funnelshift_r(cw, cw, r1) & 3u) | (__funnelshift_r(rw, rw, r2) & 4u) |
+                         (__funnelshift_r(dw, dw, r3) & 8u);
     bool flip, is_p;
     if (DIS) {
         is_p = cfg == 12u;
         flip = false;
         if (is_p || cfg == 3u) {
-            const int cls = (int)(__funnelshift_r(dtile[w], dtile[w], rot) & 3u);
+            const int cls = (int)(__funnelshift_r(dtile[w], dtile[w], r1) & 3u);
             const Thresh& th = is_p ? dr.tp[cls] : dr.tq[cls];
             flip = th.always || (th.planes && u < th.t);
         }
@@ -127,9 +130,9 @@ __device__ __forceinline__ void dt_attempt_at(uint32_t* tile, const uint32_t* dt
         // this round (the atomics merely order its own three flips when two share a word);
         // under the dead-border schemes other threads' flips of the same phase may share them
         // (the reference's fctAtomicXor)
-        atomicXor(&tile[w], 3u << (rot & 31u));
-        atomicXor(&tile[wr], __funnelshift_l(4u, 4u, rot >> 8));
-        atomicXor(&tile[wd], __funnelshift_l(8u, 8u, rot >> 16));
+        atomicXor(&tile[w], __funnelshift_l(3u, 3u, r1));
+        atomicXor(&tile[wr], __funnelshift_l(4u, 4u, r2));
+        atomicXor(&tile[wd], __funnelshift_l(8u, 8u, r3));
         if (COUNT) {
             if (is_p) ++ndep;
             else ++ndes;
@@ -154,6 +157,18 @@ __device__ __forceinline__ uint4 site_entry(int vx, int vy)
                       sh | (((shr - 2u) & 31u) << 8) | (((shd - 3u) & 31u) << 16));
 }
 constexpr int DT_VSPAN = 18;  // in-cell offsets of the shifted schemes: up to 3 + 7 + 7 (or 4 + 3 + 7 + 3)
+// Row stride of the DTDBSH table: a round's 16 entries (4 x 4 in-cell offsets around one
+// corner) then lie in 32 distinct banks, 8 bytes each
+constexpr int DT_VROW = 20;
+
+// An 8-byte table entry in shared memory: x = w | w_right << 16, y = w_down | sh << 10 |
+// (shr - 2) << 15 | (shd - 3) << 20 (the rotate amounts of site_entry, each read by shifting
+// y right and used modulo 32); bits 25-26 are left for flags.
+__device__ __forceinline__ uint2 pack_entry(const uint4 e)
+{
+    return make_uint2(e.x | (e.y << 16),
+                      e.z | ((e.w & 31u) << 10) | (((e.w >> 8) & 31u) << 15) | (((e.w >> 16) & 31u) << 20));
+}
 
 // DIS: quenched disorder (Disorder2SyncRng_shared, kpz/kpzSimulationPrimitivesTemplates.cu:
 // 295-382): dis holds every site's 2-bit rate class in ENC_LOCAL words, copied into a second
@@ -180,7 +195,7 @@ dt_kernel(uint32_t* __restrict__ sys, int lxw, int lyw, int lnbx, int nblocks, i
     // word (ox & 3, oy & 3) is the launch's, so it is folded in.  DTDBSH, which shifts the cells
     // per round, indexes an 18 x 18 table by the in-cell offset instead; the dead-border schemes
     // compute their site's entry directly, once per round before the phases.
-    constexpr int NLUT = SHIFTED ? DT_VSPAN * DT_VSPAN : 64;
+    constexpr int NLUT = SHIFTED ? DT_VSPAN * DT_VROW : 64;
     constexpr int ROUNDS = DB4 ? DT_ROUNDS / 2 : DT_ROUNDS;
     constexpr uint32_t T_SUB = DB4 ? TAG_DB4_SUB : TAG_DT_SUB;
     constexpr uint32_t T_POS = DB4 ? TAG_DB4_POS : TAG_DT_POS;
@@ -188,7 +203,7 @@ dt_kernel(uint32_t* __restrict__ sys, int lxw, int lyw, int lnbx, int nblocks, i
     __shared__ uint32_t tile[DT_TH * DT_TW];
     __shared__ uint32_t dtile[DIS ? DT_TH * DT_TW : 1];
     __shared__ uint32_t rep_hits[REP ? DT_THREADS / 32 + 1 : 1];
-    __shared__ uint4 lut[NLUT];
+    __shared__ uint2 lut[NLUT];
     const int tid = threadIdx.y * DT_TX + threadIdx.x;
     const uint32_t Wx = 1u << lxw, Wy = 1u << lyw;
     const int ax = ox & 3, ay = oy & 3;
@@ -202,19 +217,19 @@ dt_kernel(uint32_t* __restrict__ sys, int lxw, int lyw, int lnbx, int nblocks, i
     unsigned long long ndep = 0, ndes = 0;
     if (NLUT == 64) {
         if (tid < 64) {
-            // bits 24 / 25: the site lies at in-cell x / y >= 3, DB4's dead border when the cell
+            // bits 25 / 26 of y: the site lies at in-cell x / y >= 3, DB4's dead border when the cell
             // is the block's last in its row / column (it starts 8 sites before the block's edge)
             const int sc = tid >> 4, pb = tid & 15;
             const int ux = 4 * (sc & 1) + (pb & 3), uy = 4 * (sc >> 1) + (pb >> 2);
-            uint4 e = site_entry(ux + ax, uy + ay);
-            e.w |= (ux >= 8 - DB4_BORDER ? 1u << 24 : 0u) | (uy >= 8 - DB4_BORDER ? 1u << 25 : 0u);
+            uint2 e = pack_entry(site_entry(ux + ax, uy + ay));
+            e.y |= (ux >= 8 - DB4_BORDER ? 1u << 25 : 0u) | (uy >= 8 - DB4_BORDER ? 1u << 26 : 0u);
             lut[tid] = e;
         }
     } else {
-        for (int i = tid; i < NLUT; i += DT_THREADS) lut[i] = site_entry(i % DT_VSPAN, i / DT_VSPAN);
+        for (int i = tid; i < NLUT; i += DT_THREADS) lut[i] = pack_entry(site_entry(i % DT_VROW, i / DT_VROW));
     }
     // DB4: the last thread column / row owns the block's dead border
-    const uint32_t dead_mask = (threadIdx.x == DT_TX - 1 ? 1u << 24 : 0u) | (threadIdx.y == DT_TY - 1 ? 1u << 25 : 0u);
+    const uint32_t dead_mask = (threadIdx.x == DT_TX - 1 ? 1u << 25 : 0u) | (threadIdx.y == DT_TY - 1 ? 1u << 26 : 0u);
     const int tbase = 2 * threadIdx.y * DT_TW + 2 * threadIdx.x;
     // a shifted cell whose site passes the block's right / lower edge wraps to its left / upper
     // edge (the reference masks coordinates with M_BLOCK_DIM): the cell's words move back by
@@ -286,8 +301,8 @@ dt_kernel(uint32_t* __restrict__ sys, int lxw, int lyw, int lnbx, int nblocks, i
                         const uint4 e = site_entry(xt, yt);
                         for (int phase = 0; phase < 3; ++phase) {
                             if (ph == phase)
-                                dt_attempt_at<COUNT, DIS>(tile, dtile, (int)e.x, (int)e.y, (int)e.z, e.w, u, rule, dr,
-                                                          ndep, ndes);
+                                dt_attempt_at<COUNT, DIS>(tile, dtile, (int)e.x, (int)e.y, (int)e.z, e.w, e.w >> 8,
+                                                          e.w >> 16, u, rule, dr, ndep, ndes);
                             __syncthreads();
                         }
                     }
@@ -330,8 +345,8 @@ dt_kernel(uint32_t* __restrict__ sys, int lxw, int lyw, int lnbx, int nblocks, i
                     const uint32_t u = pick4(ruu, k & 3);
                     for (int phase = 0; phase < 3; ++phase) {
                         if (ph == phase)
-                            dt_attempt_at<COUNT, DIS>(tile, dtile, (int)e.x, (int)e.y, (int)e.z, e.w, u, rule, dr, ndep,
-                                                      ndes);
+                            dt_attempt_at<COUNT, DIS>(tile, dtile, (int)e.x, (int)e.y, (int)e.z, e.w, e.w >> 8,
+                                                      e.w >> 16, u, rule, dr, ndep, ndes);
                         __syncthreads();
                     }
                 }
@@ -364,24 +379,26 @@ dt_kernel(uint32_t* __restrict__ sys, int lxw, int lyw, int lnbx, int nblocks, i
                     const uint32_t ob = (pick4(ow, (r & 15) >> 2) >> (8 * (r & 3))) & 0xFFu;
                     const int ux = 4 * (int)(sc & 1u) + (int)(pb & 3u) + (int)(ob & 7u);
                     const int uy = 2 * (int)(sc & 2u) + (int)(pb >> 2) + (int)((ob >> 3) & 7u);
-                    const uint4 e = lut[(uy + ay) * DT_VSPAN + ux + ax];
+                    const uint2 e = lut[(uy + ay) * DT_VROW + ux + ax];
                     const int base = wrapped_base(ux, uy);
-                    dt_attempt_at<COUNT, DIS>(tile, dtile, base + (int)e.x, base + (int)e.y, base + (int)e.z, e.w, u,
-                                              rule, dr, ndep, ndes);
+                    dt_attempt_at<COUNT, DIS>(tile, dtile, base + (int)(e.x & 0xFFFFu), base + (int)(e.x >> 16),
+                                              base + (int)(e.y & 1023u), e.y >> 10, e.y >> 15, e.y >> 20, u, rule, dr,
+                                              ndep, ndes);
                 } else {
-                    const uint4 e = lut[sc * 16u + pb];
-                    if (!DB4 || (e.w & dead_mask) == 0u) {
-                        const int w = tbase + (int)e.x, wr = tbase + (int)e.y, wd = tbase + (int)e.z;
+                    const uint2 e = lut[sc * 16u + pb];
+                    if (!DB4 || (e.y & dead_mask) == 0u) {
+                        const int w = tbase + (int)(e.x & 0xFFFFu), wr = tbase + (int)(e.x >> 16);
+                        const int wd = tbase + (int)(e.y & 1023u);
+                        const uint32_t r1 = e.y >> 10, r2 = e.y >> 15, r3 = e.y >> 20;
                         const uint32_t cw = tile[w], rw = tile[wr], dw = tile[wd];
-                        const uint32_t cfg = (__funnelshift_r(cw, cw, e.w) & 3u) |
-                                             (__funnelshift_r(rw, rw, e.w >> 8) & 4u) |
-                                             (__funnelshift_r(dw, dw, e.w >> 16) & 8u);
+                        const uint32_t cfg = (__funnelshift_r(cw, cw, r1) & 3u) | (__funnelshift_r(rw, rw, r2) & 4u) |
+                                             (__funnelshift_r(dw, dw, r3) & 8u);
                         bool flip, is_p;
                         if (DIS) {
                             is_p = cfg == 12u;
                             flip = false;
                             if (is_p || cfg == 3u) {
-                                const int cls = (int)(__funnelshift_r(dtile[w], dtile[w], e.w) & 3u);
+                                const int cls = (int)(__funnelshift_r(dtile[w], dtile[w], r1) & 3u);
                                 const Thresh& th = is_p ? dr.tp[cls] : dr.tq[cls];
                                 flip = th.always || (th.planes && u < th.t);
                             }
@@ -390,9 +407,9 @@ dt_kernel(uint32_t* __restrict__ sys, int lxw, int lyw, int lnbx, int nblocks, i
                             flip = (is_p || cfg == cfg_q) && u <= (is_p ? lim_p : lim_q);
                         }
                         if (flip) {
-                            atomicXor(&tile[w], 3u << (e.w & 31u));
-                            atomicXor(&tile[wr], __funnelshift_l(4u, 4u, e.w >> 8));
-                            atomicXor(&tile[wd], __funnelshift_l(8u, 8u, e.w >> 16));
+                            atomicXor(&tile[w], __funnelshift_l(3u, 3u, r1));
+                            atomicXor(&tile[wr], __funnelshift_l(4u, 4u, r2));
+                            atomicXor(&tile[wd], __funnelshift_l(8u, 8u, r3));
                             if (COUNT) {
                                 if (is_p) ++ndep;
                                 else ++ndes;

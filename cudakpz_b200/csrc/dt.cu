@@ -58,37 +58,6 @@ __device__ __forceinline__ uint32_t pick4(const uint4& v, int i)
     return i == 0 ? v.x : i == 1 ? v.y : i == 2 ? v.z : v.w;
 }
 
-// One attempt at tile site (xt, yt) (sites counted from the tile's first word) whose flips may
-// share words with other threads' attempts of the same phase: shared-memory atomics, as the
-// reference's dead-border schemes use (fctAtomicXor).  u: the acceptance word.
-template <bool COUNT, bool DIS>
-__device__ __forceinline__ void dt_attempt_atomic(uint32_t* tile, const uint32_t* dtile, int xt, int yt, uint32_t u,
-                                                  const Thresh& tp, const Thresh& tq, const DisorderRates& dr,
-                                                  unsigned long long& ndep, unsigned long long& ndes)
-{
-    const int wi = (yt >> 2) * DT_TW + (xt >> 2);
-    const uint32_t sh = (uint32_t)(((xt & 3) << 1) | ((yt & 3) << 3));
-    const int wr = (yt >> 2) * DT_TW + ((xt + 1) >> 2);
-    const uint32_t shr = (uint32_t)((((xt + 1) & 3) << 1) | ((yt & 3) << 3));
-    const int wd = ((yt + 1) >> 2) * DT_TW + (xt >> 2);
-    const uint32_t shd = (uint32_t)(((xt & 3) << 1) | (((yt + 1) & 3) << 3) | 1);
-    const uint32_t c = (tile[wi] >> sh) & 3u, rbit = (tile[wr] >> shr) & 1u, lbit = (tile[wd] >> shd) & 1u;
-    const bool is_p = c == 0u && rbit && lbit, is_q = c == 3u && !rbit && !lbit;
-    if (!(is_p || is_q)) return;
-    int cls = 0;
-    if (DIS) cls = (int)((dtile[wi] >> sh) & 3u);
-    const Thresh& th = DIS ? (is_p ? dr.tp[cls] : dr.tq[cls]) : (is_p ? tp : tq);
-    const bool flip = th.always || (th.planes && u < th.t);
-    if (!flip) return;
-    atomicXor(&tile[wi], 3u << sh);
-    atomicXor(&tile[wr], 1u << shr);
-    atomicXor(&tile[wd], 1u << shd);
-    if (COUNT) {
-        if (is_p) ++ndep;
-        else ++ndes;
-    }
-}
-
 // The rule's candidates and acceptance limits for the plain rates: a site of configuration
 // cfg_p (12, or an impossible 16 when p = 0) flips when its acceptance word u <= lim_p =
 // T_p - 1; likewise cfg_q (3).
@@ -192,10 +161,10 @@ dt_kernel(uint32_t* __restrict__ sys, int lxw, int lyw, int lnbx, int nblocks, i
     constexpr bool REP = SCHEME == DT_SCHEME_DBSHREP;
     constexpr bool BORDER = SCHEME == DT_SCHEME_DBSH || SCHEME == DT_SCHEME_DB || REP;
     // DT and DB4 index a 64-entry table by (quadrant, position): the origin's offset inside a
-    // word (ox & 3, oy & 3) is the launch's, so it is folded in.  DTDBSH, which shifts the cells
-    // per round, indexes an 18 x 18 table by the in-cell offset instead; the dead-border schemes
-    // compute their site's entry directly, once per round before the phases.
-    constexpr int NLUT = SHIFTED ? DT_VSPAN * DT_VROW : 64;
+    // word (ox & 3, oy & 3) is the launch's, so it is folded in.  The schemes that shift the
+    // cells per round (DTDBSH and the dead-border schemes) index an 18 x 18 table by the
+    // in-cell offset instead.
+    constexpr int NLUT = (SHIFTED || BORDER) ? DT_VSPAN * DT_VROW : 64;
     constexpr int ROUNDS = DB4 ? DT_ROUNDS / 2 : DT_ROUNDS;
     constexpr uint32_t T_SUB = DB4 ? TAG_DB4_SUB : TAG_DT_SUB;
     constexpr uint32_t T_POS = DB4 ? TAG_DB4_POS : TAG_DT_POS;
@@ -276,7 +245,7 @@ dt_kernel(uint32_t* __restrict__ sys, int lxw, int lyw, int lnbx, int nblocks, i
                 const uint4 pw = philox4x32_10(
                     make_uint4(cid, t, (TAG_DBSH_POS << 24) | ((uint32_t)d << 16) | (uint32_t)(rb >> 4), stream),
                     key);
-#pragma unroll 4
+#pragma unroll
                 for (int j = 0; j < 16; ++j) {
                     const int r = rb + j;
                     if (need_u && (j & 3) == 0)
@@ -286,23 +255,26 @@ dt_kernel(uint32_t* __restrict__ sys, int lxw, int lyw, int lnbx, int nblocks, i
                     const uint32_t pb = (pick4(pw, j >> 2) >> (8 * (j & 3))) & 0xFFu;
                     const int px = (int)(pb & 7u), py = (int)((pb >> 3) & 7u);
                     const int ph = (px == 7 && py == 7) ? 2 : (px == 7 || py == 7) ? 1 : 0;
-                    const int xt = (threadIdx.x * 8 + ax + px + (SCHEME == DT_SCHEME_DB ? 0 : (int)(ob & 7u))) &
-                                   (DT_BX - 1);
-                    const int yt = (threadIdx.y * 8 + ay + py + (SCHEME == DT_SCHEME_DB ? 0 : (int)((ob >> 3) & 7u))) &
-                                   (DT_BY - 1);
+                    // the site at in-cell offset (vx, vy) from the cell's first word; the table gives
+                    // its words and rotations, once per round, before the phases
+                    const int vx = ax + px + (SCHEME == DT_SCHEME_DB ? 0 : (int)(ob & 7u));
+                    const int vy = ay + py + (SCHEME == DT_SCHEME_DB ? 0 : (int)((ob >> 3) & 7u));
+                    const uint2 e = lut[vy * DT_VROW + vx];
+                    const int base = wrapped_base(vx, vy);
+                    const int w = base + (int)(e.x & 0xFFFFu), wr = base + (int)(e.x >> 16);
+                    const int wd = base + (int)(e.y & 1023u);
                     const uint32_t u = pick4(uu, j & 3);
                     if (REP) {
-                        // one phase: the site's geometry is only needed inside it
-                        if (ph == 0) dt_attempt_atomic<COUNT, DIS>(tile, dtile, xt, yt, u, tp, tq, dr, ndep, ndes);
+                        if (ph == 0)
+                            dt_attempt_at<COUNT, DIS>(tile, dtile, w, wr, wd, e.y >> 10, e.y >> 15, e.y >> 20, u, rule,
+                                                      dr, ndep, ndes);
                         else ++hits;
                         __syncthreads();
                     } else {
-                        // three phases: the site's words and rotations once, before them
-                        const uint4 e = site_entry(xt, yt);
                         for (int phase = 0; phase < 3; ++phase) {
                             if (ph == phase)
-                                dt_attempt_at<COUNT, DIS>(tile, dtile, (int)e.x, (int)e.y, (int)e.z, e.w, e.w >> 8,
-                                                          e.w >> 16, u, rule, dr, ndep, ndes);
+                                dt_attempt_at<COUNT, DIS>(tile, dtile, w, wr, wd, e.y >> 10, e.y >> 15, e.y >> 20, u,
+                                                          rule, dr, ndep, ndes);
                             __syncthreads();
                         }
                     }
@@ -339,14 +311,16 @@ dt_kernel(uint32_t* __restrict__ sys, int lxw, int lyw, int lnbx, int nblocks, i
                     const uint32_t pb = (pick4(rpw, (k & 15) >> 2) >> (8 * (k & 3))) & 0xFFu;
                     const int px = (int)(pb & 7u), py = (int)((pb >> 3) & 7u);
                     const int ph = !active ? 3 : (px == 7 && py == 7) ? 2 : (px == 7 || py == 7) ? 1 : 0;
-                    const int xt = (threadIdx.x * 8 + ax + px + (int)(ob & 7u)) & (DT_BX - 1);
-                    const int yt = (threadIdx.y * 8 + ay + py + (int)((ob >> 3) & 7u)) & (DT_BY - 1);
-                    const uint4 e = site_entry(xt, yt);
+                    const int vx = ax + px + (int)(ob & 7u), vy = ay + py + (int)((ob >> 3) & 7u);
+                    const uint2 e = lut[vy * DT_VROW + vx];
+                    const int base = wrapped_base(vx, vy);
+                    const int w = base + (int)(e.x & 0xFFFFu), wr = base + (int)(e.x >> 16);
+                    const int wd = base + (int)(e.y & 1023u);
                     const uint32_t u = pick4(ruu, k & 3);
                     for (int phase = 0; phase < 3; ++phase) {
                         if (ph == phase)
-                            dt_attempt_at<COUNT, DIS>(tile, dtile, (int)e.x, (int)e.y, (int)e.z, e.w, e.w >> 8,
-                                                      e.w >> 16, u, rule, dr, ndep, ndes);
+                            dt_attempt_at<COUNT, DIS>(tile, dtile, w, wr, wd, e.y >> 10, e.y >> 15, e.y >> 20, u, rule,
+                                                      dr, ndep, ndes);
                         __syncthreads();
                     }
                 }

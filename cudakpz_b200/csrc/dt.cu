@@ -291,37 +291,41 @@ dt_kernel(uint32_t* __restrict__ sys, int lxw, int lyw, int lnbx, int nblocks, i
                 __syncthreads();
                 uint32_t total = rep_hits[0];
                 for (int w = 1; w < DT_THREADS / 32; ++w) total += rep_hits[1 + w];
-                uint4 rpw = make_uint4(0, 0, 0, 0), ruu = make_uint4(0, 0, 0, 0);
-                for (int k = 0; k * DT_THREADS < (int)total; ++k) {
-                    const bool active = k * DT_THREADS + tid < (int)total;
-                    if ((k & 15) == 0) {
-                        ow = philox4x32_10(make_uint4((uint32_t)b, t,
-                                                      (TAG_REP_ORIGIN << 24) | ((uint32_t)d << 16) | (uint32_t)(k >> 4),
-                                                      stream), key);
-                        if (active)
-                            rpw = philox4x32_10(
-                                make_uint4(cid, t, (TAG_REP_POS << 24) | ((uint32_t)d << 16) | (uint32_t)(k >> 4),
-                                           stream), key);
-                    }
-                    if (active && need_u && (k & 3) == 0)
-                        ruu = philox4x32_10(
-                            make_uint4(cid, t, (TAG_REP_U << 24) | ((uint32_t)d << 16) | (uint32_t)(k >> 2), stream),
-                            key);
-                    const uint32_t ob = (pick4(ow, (k & 15) >> 2) >> (8 * (k & 3))) & 0xFFu;
-                    const uint32_t pb = (pick4(rpw, (k & 15) >> 2) >> (8 * (k & 3))) & 0xFFu;
-                    const int px = (int)(pb & 7u), py = (int)((pb >> 3) & 7u);
-                    const int ph = !active ? 3 : (px == 7 && py == 7) ? 2 : (px == 7 || py == 7) ? 1 : 0;
-                    const int vx = ax + px + (int)(ob & 7u), vy = ay + py + (int)((ob >> 3) & 7u);
-                    const uint2 e = lut[vy * DT_VROW + vx];
-                    const int base = wrapped_base(vx, vy);
-                    const int w = base + (int)(e.x & 0xFFFFu), wr = base + (int)(e.x >> 16);
-                    const int wd = base + (int)(e.y & 1023u);
-                    const uint32_t u = pick4(ruu, k & 3);
-                    for (int phase = 0; phase < 3; ++phase) {
-                        if (ph == phase)
-                            dt_attempt_at<COUNT, DIS>(tile, dtile, w, wr, wd, e.y >> 10, e.y >> 15, e.y >> 20, u, rule,
-                                                      dr, ndep, ndes);
-                        __syncthreads();
+                // repetition rounds in groups of 16, unrolled like the main rounds (the offset and
+                // position words serve 16 rounds, the acceptance words 4)
+                for (int kb = 0; kb * DT_THREADS < (int)total; kb += 16) {
+                    ow = philox4x32_10(make_uint4((uint32_t)b, t,
+                                                  (TAG_REP_ORIGIN << 24) | ((uint32_t)d << 16) | (uint32_t)(kb >> 4),
+                                                  stream), key);
+                    const uint4 rpw = philox4x32_10(
+                        make_uint4(cid, t, (TAG_REP_POS << 24) | ((uint32_t)d << 16) | (uint32_t)(kb >> 4), stream),
+                        key);
+                    uint4 ruu = make_uint4(0, 0, 0, 0);
+#pragma unroll
+                    for (int j = 0; j < 16; ++j) {
+                        const int k = kb + j;
+                        if (k * DT_THREADS >= (int)total) break;
+                        const bool active = k * DT_THREADS + tid < (int)total;
+                        if (need_u && (j & 3) == 0)
+                            ruu = philox4x32_10(
+                                make_uint4(cid, t, (TAG_REP_U << 24) | ((uint32_t)d << 16) | (uint32_t)(k >> 2), stream),
+                                key);
+                        const uint32_t ob = (pick4(ow, j >> 2) >> (8 * (j & 3))) & 0xFFu;
+                        const uint32_t pb = (pick4(rpw, j >> 2) >> (8 * (j & 3))) & 0xFFu;
+                        const int px = (int)(pb & 7u), py = (int)((pb >> 3) & 7u);
+                        const int ph = !active ? 3 : (px == 7 && py == 7) ? 2 : (px == 7 || py == 7) ? 1 : 0;
+                        const int vx = ax + px + (int)(ob & 7u), vy = ay + py + (int)((ob >> 3) & 7u);
+                        const uint2 e = lut[vy * DT_VROW + vx];
+                        const int base = wrapped_base(vx, vy);
+                        const int w = base + (int)(e.x & 0xFFFFu), wr = base + (int)(e.x >> 16);
+                        const int wd = base + (int)(e.y & 1023u);
+                        const uint32_t u = pick4(ruu, j & 3);
+                        for (int phase = 0; phase < 3; ++phase) {
+                            if (ph == phase)
+                                dt_attempt_at<COUNT, DIS>(tile, dtile, w, wr, wd, e.y >> 10, e.y >> 15, e.y >> 20, u, rule,
+                                                          dr, ndep, ndes);
+                            __syncthreads();
+                        }
                     }
                 }
             }

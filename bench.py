@@ -345,8 +345,11 @@ def alu_ops_per_word(p, q):
 
 def run_e2e(args, torch, kpzb, scheds, N, M, world):
     """Public API with host buffers: push (pinned H2D) -> mcs -> pop (D2H) -> roughness, every
-    step, both lattices, through the asynchronous push/pop entry points; each step's W^2 is
-    read while the other lattice's step runs."""
+    step, both lattices, through the asynchronous push/pop entry points.  Each lattice runs on
+    its own stream and its MCS waits for the other lattice's MCS to finish, so the lattices take
+    turns on the SMs and one lattice's copies and W^2 read overlap the other's MCS (two MCS
+    passes sharing the SMs would finish together and leave the copies exposed); each step's
+    W^2 is read while the other lattice's step runs."""
     import numpy as np
     nw = scheds[0].size_words()
     host = [torch.empty(nw, dtype=torch.int32).pin_memory() for _ in scheds]
@@ -358,21 +361,27 @@ def run_e2e(args, torch, kpzb, scheds, N, M, world):
     steps = max(3, args.steps // 4)
     for s in scheds:
         s.mcsPQSyncRng(M)  # warm-up through the same path
+    streams = [torch.cuda.Stream() for _ in scheds]
+    for s, st in zip(scheds, streams):
+        s.setStream(st.cuda_stream)
     torch.cuda.synchronize()
     barrier(world)
     t0 = time.perf_counter()
     L = len(scheds)
     unread = [False] * L
+    mcs_done = [None] * L
     for _ in range(steps):
-        # each lattice on its own stream; after enqueueing one lattice's step (push, MCS, pop)
-        # the host reads the previous lattice's W^2 while this one runs, so copies and reads
-        # overlap the other lattice's MCS across step boundaries too
         for j, (h, o, s) in enumerate(zip(host, outs, scheds)):
             s.pushSystemAsync(h.numpy().view(np.uint32))
+            prev = (j - 1) % L  # with one lattice: itself
+            if mcs_done[prev] is not None and prev != j:
+                streams[j].wait_event(mcs_done[prev])
             s.mcsPQSyncRngAsync(M)
+            ev = torch.cuda.Event()
+            ev.record(streams[j])
+            mcs_done[j] = ev
             s.popSystemAsync(o.numpy().view(np.uint32))
             unread[j] = True
-            prev = (j - 1) % L  # with one lattice: itself, read at once
             if unread[prev]:
                 scheds[prev].join()
                 scheds[prev].roughness()
@@ -384,6 +393,8 @@ def run_e2e(args, torch, kpzb, scheds, N, M, world):
     torch.cuda.synchronize()
     dt = time.perf_counter() - t0
     dt = max_over_ranks(dt, world)
+    for s in scheds:
+        s.setStream(0)
     updates = float(N) * M * len(scheds) * steps * world
     return {"value": round(updates / (dt * 1e9), 3), "unit": UNIT,
             "h2d_bytes_per_step": nw * 4 * len(scheds),

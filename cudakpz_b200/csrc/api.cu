@@ -289,7 +289,7 @@ extern "C" kpzb_status kpzb_get_plan(kpzb_handle* h, int* mcs_per_pass, int* cta
     if (p.k > 1 && plan_shape_ok(p, h->lx, h->ly, h->sm_count)) {
         *mcs_per_pass = p.k;
         *ctas_per_sm = p.kind == PASS_STREAM && p.cps == 0 ? 1 : p.cps;
-        *pass_kernel = p.kind == PASS_STREAM ? KPZB_PASS_STREAM : KPZB_PASS_BAND;
+        *pass_kernel = p.kind == PASS_STREAM ? KPZB_PASS_STREAM : p.kind == PASS_WAVE ? KPZB_PASS_WAVE : KPZB_PASS_BAND;
     }
     return KPZB_OK;
 }
@@ -305,7 +305,7 @@ static uint64_t thresh_of(double p)
 
 // The pass shape used for the current rates: the caller's choice, else the tuner's cached
 // or freshly measured choice (KPZB_AUTOTUNE=0 disables measuring), else the heuristic.
-static kpzb_status resolve_plan(kpzb_handle* h, Plan* plan)
+static kpzb_status resolve_plan_raw(kpzb_handle* h, Plan* plan)
 {
     if (h->fusion > 0) {
         *plan = explicit_plan(h->lx, h->ly, h->fusion, h->sm_count);
@@ -321,6 +321,22 @@ static kpzb_status resolve_plan(kpzb_handle* h, Plan* plan)
     KPZB_CU(tune_plan(h->d_sys, h->lx, h->ly, h->seed, h->stream_id, Tp, Tq, h->sm_count,
                       reinterpret_cast<unsigned int*>(h->d_counters + 2), h->st, plan),
             "autotune");
+    return KPZB_OK;
+}
+
+static kpzb_status resolve_plan(kpzb_handle* h, Plan* plan)
+{
+    kpzb_status s = resolve_plan_raw(h, plan);
+    if (s != KPZB_OK) return s;
+    // the register-wavefront kernel covers rates of at most one random plane; other rates
+    // run the same depth as band passes
+    if (plan->kind == PASS_WAVE) {
+        const int mode = dec_mode(make_thresh(thresh_of(h->p)), make_thresh(thresh_of(h->q)));
+        if (!scabit_wave_shape(h->lx, h->ly, plan->k, h->sm_count, plan->cps, mode).ok) {
+            plan->kind = PASS_BAND;
+            plan->cps = 0;
+        }
+    }
     return KPZB_OK;
 }
 
@@ -348,7 +364,21 @@ static kpzb_status enqueue_sca(kpzb_handle* h, int n)
     kpzb_status ps = resolve_plan(h, &plan);
     if (ps != KPZB_OK) return ps;
     const int k = plan.k;
-    if (k > 1 && plan.kind == PASS_STREAM) {
+    const int mode = dec_mode(make_thresh(Tp), make_thresh(Tq));
+    const WaveShape ws = plan.kind == PASS_WAVE ? scabit_wave_shape(h->lx, h->ly, k, h->sm_count, plan.cps, mode)
+                                                : WaveShape{};
+    if (k > 1 && plan.kind == PASS_WAVE && ws.ok) {
+        kpzb_status s = ensure_tmp(h);
+        if (s != KPZB_OK) return s;
+        while (n - done >= k) {
+            KPZB_CU(scabit_wave(h->d_sys, h->d_tmp, h->lx, h->ly, (uint32_t)(h->tdev + done), h->seed,
+                                h->stream_id, Tp, Tq, ws, cnt, reinterpret_cast<unsigned int*>(h->d_counters + 2),
+                                h->st),
+                    "scabit_wave");
+            std::swap(h->d_sys, h->d_tmp);
+            done += k;
+        }
+    } else if (k > 1 && plan.kind == PASS_STREAM) {
         const StreamShape ss = scabit_stream_shape(h->lx, h->ly, k, h->sm_count, plan.cps ? plan.cps : 1);
         if (ss.ok) {
             kpzb_status s = ensure_tmp(h);

@@ -16,8 +16,8 @@ int auto_fusion(int lx, int ly);
 
 // SCABit pass shape: k MCS per HBM pass (1 = one launch per half-step), cps CTAs per SM
 // (0 = shape heuristic), the measured cost when it came from the tuner, and the pass kernel
-// (band: scabit_fused_kernel, stream: scabit_stream_kernel).
-enum PassKernel { PASS_BAND = 0, PASS_STREAM = 1 };
+// (band: scabit_fused_kernel, stream: scabit_stream_kernel, wave: scabit_wave_kernel).
+enum PassKernel { PASS_BAND = 0, PASS_STREAM = 1, PASS_WAVE = 2 };
 struct Plan {
     int k;
     int cps;
@@ -26,8 +26,9 @@ struct Plan {
     int kind;
 };
 // Pass kernel and CTAs per SM for an explicitly set fusion depth: the streaming kernel with one
-// chunk per SM, unless the environment variable KPZB_PASS_KERNEL says "band" or "stream2" (two
-// chunks per SM), or the streaming shape does not fit.
+// chunk per SM, unless the environment variable KPZB_PASS_KERNEL says "band", "stream2" (two
+// chunks per SM) or "wave" / "wave1".."wave4" (the register-wavefront kernel, 2 or the given
+// CTAs per SM), or that shape does not fit.
 Plan explicit_plan(int lx, int ly, int k, int sm_count);
 bool plan_shape_ok(const Plan& p, int lx, int ly, int sm_count);
 bool lookup_plan(int lx, int ly, uint64_t Tp, uint64_t Tq, int sm_count, Plan* out);

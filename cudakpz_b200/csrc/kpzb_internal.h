@@ -55,6 +55,22 @@ cudaError_t scabit_stream(const uint32_t* d_src, uint32_t* d_dst, int lx, int ly
                           const StreamShape& sh, unsigned long long* d_counters, unsigned int* d_err,
                           cudaStream_t st);
 
+// Register-wavefront temporal blocking (scabit_wave.cu): k MCS per HBM pass, one CTA per band
+// of rows spanning the full quadrant-row width, the half-steps in registers.
+struct WaveShape {
+    int mcs;       // MCS per pass (2, 4, 6 or 8)
+    int threads;   // threads per CTA = words per quadrant row
+    int band;      // output rows per CTA
+    int grid;      // bands (CTAs)
+    size_t smem;   // dynamic shared memory bytes
+    bool ok;
+};
+// mode: the DecMode of the rates (the kernel covers DEC_NONE and DEC_ONE)
+WaveShape scabit_wave_shape(int lx, int ly, int mcs_per_pass, int sm_count, int ctas_per_sm, int mode);
+cudaError_t scabit_wave(const uint32_t* d_src, uint32_t* d_dst, int lx, int ly, uint32_t t0, uint64_t seed,
+                        uint32_t stream_id, uint64_t Tp, uint64_t Tq, const WaveShape& sh,
+                        unsigned long long* d_counters, unsigned int* d_err, cudaStream_t st);
+
 // codec / init
 cudaError_t init_homogeneous_dev(uint32_t* d, int lx, int ly, int encoding, cudaStream_t st);
 cudaError_t local_to_cbbit_dev(const uint32_t* local, uint32_t* cbbit, int lx, int ly, cudaStream_t st);

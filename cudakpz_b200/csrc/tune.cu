@@ -87,6 +87,11 @@ Plan explicit_plan(int lx, int ly, int k, int sm_count)
     const char* env = getenv("KPZB_PASS_KERNEL");
     const std::string v = env ? env : "";
     if (k <= 1 || v == "band") return Plan{k, 0, 0.f, false, PASS_BAND};
+    if (v.compare(0, 4, "wave") == 0) {
+        const int cps = v.size() > 4 ? v[4] - '0' : 2;
+        if (scabit_wave_shape(lx, ly, k, sm_count, cps, DEC_NONE).ok) return Plan{k, cps, 0.f, false, PASS_WAVE};
+        return Plan{k, 0, 0.f, false, PASS_BAND};
+    }
     const int cps = v == "stream2" ? 2 : 1;
     if (scabit_stream_shape(lx, ly, k, sm_count, cps).ok) return Plan{k, cps, 0.f, false, PASS_STREAM};
     return Plan{k, 0, 0.f, false, PASS_BAND};
@@ -96,6 +101,7 @@ bool plan_shape_ok(const Plan& p, int lx, int ly, int sm_count)
 {
     if (p.k <= 1) return true;
     if (p.kind == PASS_STREAM) return scabit_stream_shape(lx, ly, p.k, sm_count, p.cps ? p.cps : 1).ok;
+    if (p.kind == PASS_WAVE) return scabit_wave_shape(lx, ly, p.k, sm_count, p.cps, DEC_NONE).ok;
     return scabit_fused_shape_cps(lx, ly, p.k, p.cps, 0).ok;
 }
 
@@ -119,12 +125,14 @@ cudaError_t tune_plan(uint32_t* d_src, int lx, int ly, uint64_t seed, uint32_t s
     struct Cand {
         int k, cps, kind;
     };
+    const int mode = dec_mode(make_thresh(Tp), make_thresh(Tq));
     std::vector<Cand> cands{{1, 0, PASS_BAND}};
     for (int k = 2; k <= 8; ++k)
         for (int cps = 1; cps <= 3; ++cps) {
             FusedShape f = scabit_fused_shape_cps(lx, ly, k, cps, 0);
             if (f.ok && f.band >= 2) cands.push_back({k, cps, PASS_BAND});
             if (cps <= 2 && scabit_stream_shape(lx, ly, k, sm_count, cps).ok) cands.push_back({k, cps, PASS_STREAM});
+            if (scabit_wave_shape(lx, ly, k, sm_count, cps, mode).ok) cands.push_back({k, cps, PASS_WAVE});
         }
     Plan best{1, 0, 1e30f, true, PASS_BAND};
     const ScabitShape hs = scabit_shape(lx, ly, sm_count);
@@ -143,11 +151,15 @@ cudaError_t tune_plan(uint32_t* d_src, int lx, int ly, uint64_t seed, uint32_t s
             }
             const FusedShape f = scabit_fused_shape_cps(lx, ly, c.k, c.cps, 0);
             const StreamShape ss = scabit_stream_shape(lx, ly, c.k, sm_count, c.cps);
+            const WaveShape ws = scabit_wave_shape(lx, ly, c.k, sm_count, c.cps, mode);
             uint32_t *s = a, *d = b;
             for (int m = 0; m + c.k <= mcs; m += c.k) {
                 cudaError_t r = c.kind == PASS_STREAM
                                     ? scabit_stream(s, d, lx, ly, (uint32_t)m, seed, stream_id, Tp, Tq, ss,
                                                     nullptr, d_err, st)
+                                : c.kind == PASS_WAVE
+                                    ? scabit_wave(s, d, lx, ly, (uint32_t)m, seed, stream_id, Tp, Tq, ws, nullptr,
+                                                  d_err, st)
                                     : scabit_fused(s, d, lx, ly, (uint32_t)m, seed, stream_id, Tp, Tq, f,
                                                    nullptr, d_err, st);
                 if (r != cudaSuccess) return r;
@@ -166,7 +178,7 @@ cudaError_t tune_plan(uint32_t* d_src, int lx, int ly, uint64_t seed, uint32_t s
         const float per = ms / (float)mcs;
         if (getenv("KPZB_TUNE_VERBOSE"))
             fprintf(stderr, "kpzb tune lx=%d ly=%d %s k=%d cps=%d: %.4f ms/MCS, %.1f upd/ns\n", lx, ly,
-                    c.kind == PASS_STREAM ? "stream" : "band", c.k, c.cps, per,
+                    c.kind == PASS_STREAM ? "stream" : c.kind == PASS_WAVE ? "wave" : "band", c.k, c.cps, per,
                     (double)(1ull << (lx + ly)) / (per * 1e6));
         if (per < best.ms_per_mcs) best = Plan{c.k, c.cps, per, true, c.kind};
     }

@@ -92,6 +92,42 @@ def test_stream_kernel_edges(kpzb, oracle, monkeypatch, lx, ly, k, p, q, kernel)
     assert first_diff(got, ref) is None, first_diff(got, ref)
 
 
+@pytest.mark.parametrize("kernel", ["wave1", "wave2", "wave3"])
+@pytest.mark.parametrize("lx,ly,k,p,q", [
+    (11, 7, 2, 1.0, 0.0),   # one warp per row (the cross-warp carry goes through its own lane 0)
+    (11, 3, 8, 0.5, 0.5),   # 8 rows, deepest pass: every band's halo wraps the lattice
+    (12, 8, 4, 0.5, 0.5),   # two warps per row
+    (12, 6, 6, 1.0, 1.0),   # every candidate flips, maxima too
+    (13, 7, 8, 0.5, 0.0),   # one random plane, no maxima
+    (13, 5, 4, 0.0, 1.0),   # only maxima
+    (14, 6, 2, 1.0, 0.0),   # the headline width: eight warps per row
+    (14, 5, 6, 0.5, 0.5),
+    (14, 4, 4, 0.9, 0.1),   # generic rates: the wave kernel does not cover them, band fallback
+])
+def test_wave_kernel_bit_exact(kpzb, oracle, monkeypatch, lx, ly, k, p, q, kernel):
+    """The register-wavefront pass kernel, word for word, with counters: bands of few rows,
+    halos that wrap, one to eight warps per row, one to three CTAs per SM."""
+    monkeypatch.setenv("KPZB_PASS_KERNEL", kernel)
+    n = 2 * k + 1
+    init = oracle.random_lattice(lx, ly, oracle.ENC_CBBIT, seed=17, mcs=2)
+    ref = init.copy()
+    rc = oracle.sca_mcs(ref, lx, ly, oracle.ENC_CBBIT, 9, 3, 0, n, p, q)
+    s = kpzb.Scheduler(lx, ly)
+    s.pushSystem(init)
+    s.setPQ(p, q)
+    s.supplySeed(9, 3)
+    s.setFusion(k)
+    s.enableCounters(True)
+    s.mcsPQSyncRng(n)
+    got = s.popSystem()
+    cnt = s.counters()
+    kind = s.plan()[2]
+    s.close()
+    assert kind == ("band" if (p, q) == (0.9, 0.1) else "wave")
+    assert first_diff(got, ref) is None, first_diff(got, ref)
+    assert cnt == rc
+
+
 @pytest.mark.parametrize("p,q", [(0.95, 0.0), (0.5, 0.5), (1.0, 0.0)])
 def test_sca_local_encoding_bit_exact(kpzb, oracle, p, q):
     """SchedulerSCA: ENC_LOCAL push/pop; dynamics identical to the per-site ENC_LOCAL oracle."""
@@ -163,7 +199,7 @@ def test_counters_fused(kpzb, oracle, monkeypatch, fusion, kernel):
     assert s.counters() == oracle.sca_mcs(ref, lx, ly, oracle.ENC_CBBIT, 8, 0, 0, 8, 0.6, 0.4)
 
 
-@pytest.mark.parametrize("kernel", ["stream", "band"])
+@pytest.mark.parametrize("kernel", ["stream", "band", "wave"])
 def test_full_size_16384_properties(kpzb, oracle, monkeypatch, kernel):
     """16384^2 (C2 size): fused == unfused bit for bit, invariants hold, height balance."""
     monkeypatch.setenv("KPZB_PASS_KERNEL", kernel)

@@ -35,11 +35,12 @@ PQS = [(1.0, 0.0), (0.5, 0.5)]
 METRIC = "site updates/ns (SCA, DT, batched) vs plain loop; exact correlator TOPS"
 UNIT = "attempted site updates/ns"
 
-# Per-launch DRAM traffic (dram__bytes_read.sum + dram__bytes_write.sum) of the fused pass
-# kernel at 16384^2, from one ncu capture per (p, q, MCS per pass); the commands and the
-# full figures are in profiles/scabit_fused_16384.md.
+# Per-launch DRAM traffic (dram__bytes_read.sum + dram__bytes_write.sum) of the pass kernels
+# at 16384^2, from one ncu capture per (p, q, pass kernel, MCS per pass); the commands and the
+# full figures are in profiles/scabit_fused_16384.md and profiles/scabit_wave_16384.md.
 NCU_TRAFFIC_PER_LAUNCH = {(1.0, 0.0, "band", 7): 67.324e6 + 23.171e6,
-                          (0.5, 0.5, "band", 4): 67.218e6 + 17.975e6}
+                          (0.5, 0.5, "band", 4): 67.218e6 + 17.975e6,
+                          (1.0, 0.0, "wave", 6): 89.707e6 + 19.618e6}
 
 
 def parse():

@@ -59,6 +59,7 @@ cudaError_t scabit_stream(const uint32_t* d_src, uint32_t* d_dst, int lx, int ly
 // of rows spanning the full quadrant-row width, the half-steps in registers.
 struct WaveShape {
     int mcs;       // MCS per pass (2, 4, 6 or 8)
+    int cps;       // CTAs per SM the bands and registers are sized for
     int threads;   // threads per CTA = words per quadrant row
     int band;      // output rows per CTA
     int grid;      // bands (CTAs)

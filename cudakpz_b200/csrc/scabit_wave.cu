@@ -59,8 +59,9 @@ __host__ __device__ inline WaveSmem wave_smem(int Wr, int K)
 
 constexpr int WAVE_MAX_THREADS = 256;  // lx <= 14: a quadrant row of at most 256 words
 
-template <int MODE, bool USEQ, bool COUNT, int K>
-__global__ void __launch_bounds__(WAVE_MAX_THREADS, 2)
+// MINB: CTAs per SM the register allocation is sized for (the tuner's CTAs-per-SM choice)
+template <int MODE, bool USEQ, bool COUNT, int K, int MINB>
+__global__ void __launch_bounds__(WAVE_MAX_THREADS, MINB)
 scabit_wave_kernel(const uint32_t* __restrict__ src, uint32_t* __restrict__ dst, int lx, int ly, int B,
                    uint32_t t0, Key key, uint32_t stream, Thresh tp, Thresh tq,
                    unsigned long long* __restrict__ counters, unsigned int* __restrict__ err)
@@ -294,7 +295,7 @@ WaveShape scabit_wave_shape(int lx, int ly, int mcs_per_pass, int sm_count, int 
     const int k = mcs_per_pass;
     if (lx < 11 || (1 << (lx - 6)) > WAVE_MAX_THREADS || (k != 2 && k != 4 && k != 6 && k != 8)) return s;
     if (mode != DEC_NONE && mode != DEC_ONE) return s;
-    if (ctas_per_sm < 1 || ctas_per_sm > 4) return s;
+    if (ctas_per_sm < 1 || ctas_per_sm > 3) return s;
     const int Wr = 1 << (lx - 6);
     const int64_t rows = 1ll << ly;
     const int64_t target = (int64_t)sm_count * ctas_per_sm;
@@ -302,6 +303,7 @@ WaveShape scabit_wave_shape(int lx, int ly, int mcs_per_pass, int sm_count, int 
     if (B < 8) B = 8;
     if (B > rows) B = rows;
     s.mcs = k;
+    s.cps = ctas_per_sm;
     s.threads = Wr;
     s.band = (int)B;
     s.grid = (int)((rows + B - 1) / B);
@@ -310,17 +312,29 @@ WaveShape scabit_wave_shape(int lx, int ly, int mcs_per_pass, int sm_count, int 
     return s;
 }
 
-template <int MODE, bool USEQ, bool COUNT, int K>
-static cudaError_t launch_wave_k(const uint32_t* d_src, uint32_t* d_dst, int lx, int ly, uint32_t t0, Key key,
-                                 uint32_t stream_id, Thresh tp, Thresh tq, const WaveShape& sh,
-                                 unsigned long long* d_counters, unsigned int* d_err, cudaStream_t st)
+template <int MODE, bool USEQ, bool COUNT, int K, int MINB>
+static cudaError_t launch_wave_kb(const uint32_t* d_src, uint32_t* d_dst, int lx, int ly, uint32_t t0, Key key,
+                                  uint32_t stream_id, Thresh tp, Thresh tq, const WaveShape& sh,
+                                  unsigned long long* d_counters, unsigned int* d_err, cudaStream_t st)
 {
-    auto kern = scabit_wave_kernel<MODE, USEQ, COUNT, K>;
+    auto kern = scabit_wave_kernel<MODE, USEQ, COUNT, K, MINB>;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh.smem);
     if (e != cudaSuccess) return e;
     kern<<<sh.grid, sh.threads, sh.smem, st>>>(d_src, d_dst, lx, ly, sh.band, t0, key, stream_id, tp, tq, d_counters,
                                                d_err);
     return cudaGetLastError();
+}
+
+template <int MODE, bool USEQ, bool COUNT, int K>
+static cudaError_t launch_wave_k(const uint32_t* d_src, uint32_t* d_dst, int lx, int ly, uint32_t t0, Key key,
+                                 uint32_t stream_id, Thresh tp, Thresh tq, const WaveShape& sh,
+                                 unsigned long long* d_counters, unsigned int* d_err, cudaStream_t st)
+{
+    if (sh.cps >= 3)
+        return launch_wave_kb<MODE, USEQ, COUNT, K, 3>(d_src, d_dst, lx, ly, t0, key, stream_id, tp, tq, sh,
+                                                        d_counters, d_err, st);
+    return launch_wave_kb<MODE, USEQ, COUNT, K, 2>(d_src, d_dst, lx, ly, t0, key, stream_id, tp, tq, sh, d_counters,
+                                                    d_err, st);
 }
 
 template <int MODE, bool USEQ, bool COUNT>

@@ -203,41 +203,42 @@ walk_kernel(const uint32_t* __restrict__ sys, const uint32_t* __restrict__ snap,
             }
         }
     }
-    if constexpr (MODE == 2) return;
-    // block reduction in fixed order
-    __shared__ Partial red[AN_THREADS / 32];
-    for (int o = 16; o > 0; o >>= 1) {
-        s1 += __shfl_xor_sync(0xffffffffu, s1, o);
-        s2 += __shfl_xor_sync(0xffffffffu, s2, o);
-        cross += __shfl_xor_sync(0xffffffffu, cross, o);
-        agree += __shfl_xor_sync(0xffffffffu, agree, o);
-        ss1 += __shfl_xor_sync(0xffffffffu, ss1, o);
-        hmin = min(hmin, __shfl_xor_sync(0xffffffffu, hmin, o));
-        hmax = max(hmax, __shfl_xor_sync(0xffffffffu, hmax, o));
-        s3 += __shfl_xor_sync(0xffffffffu, s3, o);
-        s4 += __shfl_xor_sync(0xffffffffu, s4, o);
-        s5 += __shfl_xor_sync(0xffffffffu, s5, o);
-        s6 += __shfl_xor_sync(0xffffffffu, s6, o);
-        s7 += __shfl_xor_sync(0xffffffffu, s7, o);
-    }
-    if (lane == 0) {
-        Partial p;
-        p.s1 = s1; p.s2 = s2; p.hmin = hmin; p.hmax = hmax; p.cross = cross; p.agree = agree;
-        p.snap_s1 = ss1; p.pad = 0;
-        p.s[0] = s3; p.s[1] = s4; p.s[2] = s5; p.s[3] = s6; p.s[4] = s7;
-        red[wid] = p;
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        Partial p = red[0];
-        for (int w = 1; w < AN_THREADS / 32; ++w) {
-            const Partial& q = red[w];
-            p.s1 += q.s1; p.s2 += q.s2; p.cross += q.cross; p.agree += q.agree;
-            p.snap_s1 += q.snap_s1;
-            p.hmin = min(p.hmin, q.hmin); p.hmax = max(p.hmax, q.hmax);
-            for (int k = 0; k < 5; ++k) p.s[k] += q.s[k];
+    if constexpr (MODE != 2) {
+        // block reduction in fixed order
+        __shared__ Partial red[AN_THREADS / 32];
+        for (int o = 16; o > 0; o >>= 1) {
+            s1 += __shfl_xor_sync(0xffffffffu, s1, o);
+            s2 += __shfl_xor_sync(0xffffffffu, s2, o);
+            cross += __shfl_xor_sync(0xffffffffu, cross, o);
+            agree += __shfl_xor_sync(0xffffffffu, agree, o);
+            ss1 += __shfl_xor_sync(0xffffffffu, ss1, o);
+            hmin = min(hmin, __shfl_xor_sync(0xffffffffu, hmin, o));
+            hmax = max(hmax, __shfl_xor_sync(0xffffffffu, hmax, o));
+            s3 += __shfl_xor_sync(0xffffffffu, s3, o);
+            s4 += __shfl_xor_sync(0xffffffffu, s4, o);
+            s5 += __shfl_xor_sync(0xffffffffu, s5, o);
+            s6 += __shfl_xor_sync(0xffffffffu, s6, o);
+            s7 += __shfl_xor_sync(0xffffffffu, s7, o);
         }
-        partials[blockIdx.x] = p;
+        if (lane == 0) {
+            Partial p;
+            p.s1 = s1; p.s2 = s2; p.hmin = hmin; p.hmax = hmax; p.cross = cross; p.agree = agree;
+            p.snap_s1 = ss1; p.pad = 0;
+            p.s[0] = s3; p.s[1] = s4; p.s[2] = s5; p.s[3] = s6; p.s[4] = s7;
+            red[wid] = p;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            Partial p = red[0];
+            for (int w = 1; w < AN_THREADS / 32; ++w) {
+                const Partial& q = red[w];
+                p.s1 += q.s1; p.s2 += q.s2; p.cross += q.cross; p.agree += q.agree;
+                p.snap_s1 += q.snap_s1;
+                p.hmin = min(p.hmin, q.hmin); p.hmax = max(p.hmax, q.hmax);
+                for (int k = 0; k < 5; ++k) p.s[k] += q.s[k];
+            }
+            partials[blockIdx.x] = p;
+        }
     }
 }
 

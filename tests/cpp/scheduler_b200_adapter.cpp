@@ -72,6 +72,12 @@ public:
         ck(kpzb_mcs_disorder(h_, n));
         m_deviceMcs += n;
     }
+    double mcsScale() const override
+    {
+        double s = 1.0;
+        ck(kpzb_mcs_scale(h_, &s));
+        return s;
+    }
     void randomize() override {}
 };
 }  // namespace Kpz

@@ -243,3 +243,14 @@ def test_db4_random_start_stream_and_invariants(kpzb, oracle):
     ok, rep = s.consitencyCheck()
     assert ok, rep
     s.close()
+
+
+def test_mcs_scale_per_scheduler(kpzb):
+    """SchedulerService::mcsScale: p + q for SCA / SCABit (kpz/schedulerSCABit.cu:39-42), 1 for
+    DT, the dead-border active fraction for DB4 (kpz/scheduler.cu:57-65)."""
+    for sched, lx in (("scaBit", 9), ("sca", 9), ("dt", 9), ("db4", 9)):
+        s = kpzb.Scheduler(lx, lx, scheduler=sched)
+        s.setPQ(0.7, 0.2)
+        want = {"scaBit": 0.9, "sca": 0.9, "dt": 1.0, "db4": 251 * 123 / 32768}[sched]
+        assert s.mcsScale() == pytest.approx(want), sched
+        s.close()

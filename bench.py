@@ -435,6 +435,23 @@ def port_sample():
     return upd / (dt * 1e9), dt
 
 
+def dtr_sample(threads):
+    """The reference's own CPU double-tiling scheduler SchedulerCPUDTr<TinyMT32>
+    (kpz/schedulerCPUDTr.cpp), compiled from its sources into oracle/_ref/kpz_ref: REF_MCS MCS
+    at p = 0.95, q = 0.05 on the 16384^2 lattice with `threads` threads (the C3 rates; the CPU
+    side of C3 runs at 2^14, where the growth regime is that of the 65536^2 run)."""
+    if not REF_BIN.exists():
+        return None
+    r = subprocess.run([str(REF_BIN), "bench-dtr", str(REF_LX), "0.95", "0.05", str(REF_MCS), str(threads)],
+                       capture_output=True, text=True, check=True)
+    line = [ln for ln in r.stdout.splitlines() if ln and not ln.startswith("#")][0].split()
+    secs = float(line[1])
+    v = float(1 << (2 * REF_LX)) * REF_MCS / (secs * 1e9)
+    return {"value": round(v, 6), "unit": UNIT, "cores": threads, "kind": "reference",
+            "sample": f"reference SchedulerCPUDTr<TinyMT32> (oracle/_ref), 16384^2, {REF_MCS} MCS at "
+                      f"p=0.95 q=0.05, {threads} threads, {secs:.2f} s timed"}
+
+
 def cpu_baseline_sample(threads):
     if REF_BIN.exists():
         v, secs = ref_sample(threads)
@@ -452,13 +469,15 @@ def run_reference(args, world, rank):
     if rank != 0:
         return None
     cores = os.cpu_count() or 1
+    rs = args.workload in ("dt", "db4") and REF_BIN.exists()
+    sample = (lambda: dtr_sample(cores)) if rs else (lambda: cpu_baseline_sample(cores))
     for _ in range(args.warmup):
-        cpu_baseline_sample(cores)
+        sample()
     vals = []
     t0 = time.perf_counter()
     last = None
     for _ in range(args.steps):
-        last = cpu_baseline_sample(cores)
+        last = sample()
         vals.append(last["value"])
     wall = time.perf_counter() - t0
     value = statistics.median(vals)
@@ -467,8 +486,10 @@ def run_reference(args, world, rank):
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": round(wall * 1e3 / args.steps, 3), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
-            "config": {"workload": "SCABit 16384^2 periodic, flat start, (p,q)=(1,0) and (0.5,0.5); "
-                                   "each CPU step 2 MCS per (p,q) on the 16384^2 lattice"},
+            "config": {"workload": ("random-sequential double tiling (SchedulerCPUDTr), p=0.95 q=0.05; each CPU "
+                                    "step 2 MCS on the 16384^2 lattice") if rs else
+                                   ("SCABit 16384^2 periodic, flat start, (p,q)=(1,0) and (0.5,0.5); "
+                                    "each CPU step 2 MCS per (p,q) on the 16384^2 lattice")},
             "cpu_baseline": last,
             "e2e": {"value": round(value, 6), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
@@ -596,6 +617,7 @@ def run_dt(args, world, rank, local):
     s.close()
     lop3, _ = kpzb.probe_alu_peak(local)
     opa = DT_ALU_OPS_PER_ATTEMPT
+    cpu = dtr_sample(os.cpu_count() or 1) if (rank == 0 and world == 1 and not args.no_cpu) else None
     int_roofline = {"bound": "int-alu", "achieved": round(value / world * opa / 1e3, 3),
                     "peak": round(lop3 / 1e12, 3), "unit": "Tops/s",
                     "frac": round(value / world * opa * 1e9 / lop3, 4),
@@ -613,7 +635,7 @@ def run_dt(args, world, rank, local):
                            "unit": "GB/s", "frac": round(ach / peak, 4), "traffic": None,
                            "note": "integer/barrier bound; " + ("1 B" if db4 else "0.52 B") + "/attempt algorithmic",
                            "slower_roofline": "int-alu", "int_roofline": int_roofline},
-                 clocks=clk, gpu_launches=launches, invariants_ok=ok)
+                 clocks=clk, gpu_launches=launches, invariants_ok=ok, cpu_baseline=cpu)
 
 
 def run_batch(args, world, rank, local):

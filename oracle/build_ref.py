@@ -37,6 +37,7 @@ SOURCES = [
     "kpz/schedulerServiceStash.cpp", "kpz/correlator.cpp", "kpz/correlatorLines.cpp",
     "kpz/schedulerCPU.cpp", "kpz/schedulerCPUBase.cpp", "kpz/schedulerCPUBaseThreaded.cpp",
     "kpz/CPURngIface.cpp", "kpz/schedulerCPUCBBit_instances.cpp", "kpz/schedulerCPUCB_instances.cpp",
+    "kpz/schedulerCPUDTr_instances.cpp",
     "inc/dSFMT/dSFMT.cpp", "inc/tinyMT/tinymt32.c", "inc/timer.cpp",
 ]
 
@@ -242,7 +243,7 @@ def main() -> int:
         path = WORK / src
         obj = WORK / (path.stem + ".o")
         cc = ["gcc", "-O2", "-w", f"-I{WORK / 'inc'}"] if src.endswith(".c") else ["g++", *flags]
-        extra = ["-Dprotected=public"] if "schedulerCPUCB_instances" in src else []
+        extra = ["-Dprotected=public"] if ("schedulerCPUCB_instances" in src or "schedulerCPUDTr" in src) else []
         subprocess.run([*cc, *extra, "-c", str(path), "-o", str(obj)], check=True)
         objs.append(str(obj))
     drv = WORK / "ref_driver.o"

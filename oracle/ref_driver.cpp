@@ -15,6 +15,8 @@
 //   check ENC LX IN                 SchedulerService::consitencyCheck(); prints 1/0
 //   bench-cbbit LX P Q N THR        time mcsPQSyncRng(N) of SchedulerCPUCBBit; prints upd/ns
 //   bench-rs LX N                   time SchedulerCPU::mcs(N); prints upd/ns
+//   bench-dtr LX P Q N THR          time SchedulerCPUDTr<TinyMT32>::mcsPQSyncRng(N) (the reference's
+//                                   CPU double-tiling scheduler, kpz/schedulerCPUDTr.cpp); upd/ns
 //   savebit LX SEED N FILE [META]   SchedulerService::saveBit of the RS lattice after N MCS
 //   rsdis LX SEED FILL N P0 Q0 P1 Q1 DISFILE LATFILE   generateDisorder2 + SchedulerCPU::mcsDisorder2
 #include <chrono>
@@ -32,6 +34,7 @@
 #include "schedulerCPU.h"
 #include "schedulerCPUCB.h"
 #include "schedulerCPUCBBit.h"
+#include "schedulerCPUDTr.h"
 #include "schedulerService.h"
 
 // The HDF5/libSplash and MPI entry points of SchedulerService are outside the hot path;
@@ -269,6 +272,26 @@ int main(int argc, char** argv)
         s.pushSystem();
         const double t0 = now();
         s.mcs(n);
+        const double t1 = now();
+        loud();
+        std::cout << std::setprecision(9) << (double)s.size().size() * n / ((t1 - t0) * 1e9) << ' '
+                  << (t1 - t0) << '\n';
+        return 0;
+    }
+    if (cmd == "bench-dtr") {
+        const int lx = std::atoi(argv[2]);
+        const double p = std::atof(argv[3]), q = std::atof(argv[4]);
+        const int n = std::atoi(argv[5]);
+        const int thr = std::atoi(argv[6]);
+        quiet();
+        Kpz::SchedulerCPUDTr<Kpz::RngIface::TinyMT32> s(lx, lx, thr);
+        s.supplySeed(1, 1);
+        s.randomize();
+        s.initHomogeneous(Kpz::SchedulerService::ENC_LOCAL);
+        s.pushSystem();
+        s.setPQ(p, q);
+        const double t0 = now();
+        s.mcsPQSyncRng(n);
         const double t1 = now();
         loud();
         std::cout << std::setprecision(9) << (double)s.size().size() * n / ((t1 - t0) * 1e9) << ' '

@@ -452,6 +452,39 @@ def dtr_sample(threads):
                       f"p=0.95 q=0.05, {threads} threads, {secs:.2f} s timed"}
 
 
+def batch_cpu_sample(threads):
+    """C4's CPU side: the reference's SchedulerCPUCBBit (the per-replica loop's rate) at the
+    three replica rates, 1 MCS each on an 8192^2 lattice, `threads` threads."""
+    if not REF_BIN.exists():
+        return None
+    upd, secs = 0.0, 0.0
+    for (p, q) in [(1.0, 0.0), (0.9, 0.1), (0.75, 0.25)]:
+        r = subprocess.run([str(REF_BIN), "bench-cbbit", "13", str(p), str(q), "1", str(threads)],
+                           capture_output=True, text=True, check=True)
+        line = [ln for ln in r.stdout.splitlines() if ln and not ln.startswith("#")][0].split()
+        secs += float(line[1])
+        upd += float(1 << 26)
+    return {"value": round(upd / (secs * 1e9), 6), "unit": UNIT, "cores": threads, "kind": "reference",
+            "sample": f"reference SchedulerCPUCBBit (oracle/_ref), 8192^2, 1 MCS at each of (1,0), (0.9,0.1), "
+                      f"(0.75,0.25), {threads} threads, {secs:.2f} s timed; a loop over the replicas runs at "
+                      "this rate"}
+
+
+def gram_cpu_sample(threads, N):
+    """C5's CPU side: one pair of the reference's Correlator::correlate (kpz/correlator.cpp) at
+    16384^2 with `threads` threads, scaled to the 64 x 65 / 2 = 2080 pairs of the Gram, in the
+    metric's unit (2*64*64*N height-product ops / s)."""
+    if not REF_BIN.exists():
+        return None
+    r = subprocess.run([str(REF_BIN), "bench-corr", "14", str(threads)], capture_output=True, text=True,
+                       check=True)
+    secs = float([ln for ln in r.stdout.splitlines() if ln and not ln.startswith("#")][0].split()[0])
+    return {"value": round(2.0 * 64 * 64 * N / (2080 * secs) / 1e12, 9), "unit": "TOPS (2*64*64*N height-product ops / s)",
+            "cores": threads, "kind": "reference",
+            "sample": f"reference Correlator::correlate (oracle/_ref), one pair at 16384^2, {threads} threads, "
+                      f"{secs:.2f} s; x 2080 pairs = {2080 * secs / 3600:.1f} h for the Gram"}
+
+
 def cpu_baseline_sample(threads):
     if REF_BIN.exists():
         v, secs = ref_sample(threads)
@@ -701,7 +734,9 @@ def run_batch(args, world, rank, local):
                   "mcs_per_step": m, "parallelism": f"replicas x{world}"},
                  plain_loop_value=round(plain, 3), speedup_vs_plain_loop=round(value / plain, 2),
                  replicas_bit_identical_to_single_runs=same, clocks=clk,
-                 timing="host wall clock around synchronous batch calls")
+                 timing="host wall clock around synchronous batch calls",
+                 cpu_baseline=batch_cpu_sample(os.cpu_count() or 1) if (rank == 0 and world == 1 and not args.no_cpu)
+                 else None)
 
 
 def run_measure(args, world, rank, local):
@@ -811,7 +846,9 @@ def run_gram(args, world, rank, local):
                  roofline={"bound": "hbm", "kernel": "gram_tc_kernel",
                            "achieved": round(hbm_bytes / dt0 / 1e9, 1), "peak": peak, "unit": "GB/s",
                            "frac": round(hbm_bytes / dt0 / 1e9 / peak, 4), "traffic": None},
-                 clocks=clk, timing="host wall clock around synchronous compute calls")
+                 clocks=clk, timing="host wall clock around synchronous compute calls",
+                 cpu_baseline=gram_cpu_sample(os.cpu_count() or 1, N) if (rank == 0 and world == 1 and not args.no_cpu)
+                 else None)
 
 
 def main():

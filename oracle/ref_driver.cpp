@@ -17,6 +17,8 @@
 //   bench-rs LX N                   time SchedulerCPU::mcs(N); prints upd/ns
 //   bench-dtr LX P Q N THR          time SchedulerCPUDTr<TinyMT32>::mcsPQSyncRng(N) (the reference's
 //                                   CPU double-tiling scheduler, kpz/schedulerCPUDTr.cpp); upd/ns
+//   bench-corr LX THR               time one Correlator::correlate() (kpz/correlator.cpp, THR
+//                                   threads) of an ENC_CBBIT lattice against a snapshot; seconds
 //   savebit LX SEED N FILE [META]   SchedulerService::saveBit of the RS lattice after N MCS
 //   rsdis LX SEED FILL N P0 Q0 P1 Q1 DISFILE LATFILE   generateDisorder2 + SchedulerCPU::mcsDisorder2
 #include <chrono>
@@ -276,6 +278,30 @@ int main(int argc, char** argv)
         loud();
         std::cout << std::setprecision(9) << (double)s.size().size() * n / ((t1 - t0) * 1e9) << ' '
                   << (t1 - t0) << '\n';
+        return 0;
+    }
+    if (cmd == "bench-corr") {
+        const int lx = std::atoi(argv[2]);
+        const int thr = std::atoi(argv[3]);
+        quiet();
+        Kpz::SchedulerCPUCBBit<Kpz::RngIface::TinyMT32> s(lx, lx, thr);
+        s.supplySeed(1, 1);
+        s.randomize();
+        s.initHomogeneous(Kpz::SchedulerService::ENC_CBBIT);
+        s.pushSystem();
+        s.setPQ(0.5, 0.5);
+        s.mcsPQSyncRng(2);
+        s.popSystem();
+        Kpz::Correlator::setNThreads(thr);
+        Kpz::Correlator c(&s);
+        c.set(2);
+        s.mcsPQSyncRng(1);
+        s.popSystem();
+        const double t0 = now();
+        const Kpz::Roughness r = c.correlate();
+        const double t1 = now();
+        loud();
+        std::cout << std::setprecision(9) << (t1 - t0) << ' ' << (double)r.w2 << '\n';
         return 0;
     }
     if (cmd == "bench-dtr") {

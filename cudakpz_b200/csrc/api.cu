@@ -315,7 +315,7 @@ static kpzb_status resolve_plan_raw(kpzb_handle* h, Plan* plan)
     if (lookup_plan(h->lx, h->ly, Tp, Tq, h->sm_count, plan)) return KPZB_OK;
     const char* env = getenv("KPZB_AUTOTUNE");
     if (env && env[0] == '0') {
-        *plan = default_plan(h->lx, h->ly);
+        *plan = default_plan(h->lx, h->ly, Tp, Tq, h->sm_count);
         return KPZB_OK;
     }
     KPZB_CU(tune_plan(h->d_sys, h->lx, h->ly, h->seed, h->stream_id, Tp, Tq, h->sm_count,

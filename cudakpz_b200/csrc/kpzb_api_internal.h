@@ -32,7 +32,7 @@ struct Plan {
 Plan explicit_plan(int lx, int ly, int k, int sm_count);
 bool plan_shape_ok(const Plan& p, int lx, int ly, int sm_count);
 bool lookup_plan(int lx, int ly, uint64_t Tp, uint64_t Tq, int sm_count, Plan* out);
-Plan default_plan(int lx, int ly);
+Plan default_plan(int lx, int ly, uint64_t Tp, uint64_t Tq, int sm_count);
 cudaError_t tune_plan(uint32_t* d_src, int lx, int ly, uint64_t seed, uint32_t stream_id,
                       uint64_t Tp, uint64_t Tq, int sm_count, unsigned int* d_err,
                       cudaStream_t st, Plan* out);

@@ -74,10 +74,14 @@ bool lookup_plan(int lx, int ly, uint64_t Tp, uint64_t Tq, int sm_count, Plan* o
     return true;
 }
 
-Plan default_plan(int lx, int ly)
+Plan default_plan(int lx, int ly, uint64_t Tp, uint64_t Tq, int sm_count)
 {
-    // the streaming kernel at 4 MCS per pass where it fits, else the band heuristic
-    if (scabit_stream_shape(lx, ly, 4, 148, 1).ok) return Plan{4, 1, 0.f, false, PASS_STREAM};
+    // without measuring: the register-wavefront kernel (6 MCS per pass, 2 CTAs per SM) for
+    // rates without random planes, where it fits -- the fastest shape measured at 16384^2 --
+    // else the band heuristic
+    if (dec_mode(make_thresh(Tp), make_thresh(Tq)) == DEC_NONE &&
+        scabit_wave_shape(lx, ly, 6, sm_count, 2, DEC_NONE).ok)
+        return Plan{6, 2, 0.f, false, PASS_WAVE};
     const int k = auto_fusion(lx, ly);
     return Plan{k, 0, 0.f, false, PASS_BAND};
 }

@@ -255,3 +255,22 @@ def test_async_push_pop_equals_sync(kpzb, oracle, sched):
     s.join()
     assert np.array_equal(out, ref)
     s.close()
+
+
+@pytest.mark.parametrize("p,q,kind", [(1.0, 0.0, "wave"), (0.5, 0.5, "band")])
+def test_untuned_default_plan(kpzb, oracle, monkeypatch, p, q, kind):
+    """KPZB_AUTOTUNE=0: no measurement; the wave kernel for rates without random planes, the band
+    heuristic otherwise -- word for word against the oracle either way."""
+    monkeypatch.setenv("KPZB_AUTOTUNE", "0")
+    monkeypatch.delenv("KPZB_TUNE_CACHE", raising=False)
+    lx, ly, n = 12, 8, 13
+    ref = oracle.homogeneous(lx, ly, oracle.ENC_CBBIT)
+    oracle.sca_mcs(ref, lx, ly, oracle.ENC_CBBIT, 4, 0, 0, n, p, q)
+    s = kpzb.Scheduler(lx, ly)
+    s.setPQ(p, q)
+    s.supplySeed(4)
+    s.mcsPQSyncRng(n)
+    assert s.plan()[2] == kind
+    got = s.popSystem()
+    s.close()
+    assert first_diff(got, ref) is None, first_diff(got, ref)

@@ -135,7 +135,8 @@ scabit_wave_kernel(const uint32_t* __restrict__ src, uint32_t* __restrict__ dst,
     const uint32_t hp = tp.planes ? 0xFFFFFFFFu : 0u, hq = tq.planes ? 0xFFFFFFFFu : 0u;
     const int par0 = (int)(ylo & 1u);  // (y_lo + tau) & 1: the tick's updates are shifted
     const uint32_t keep0 = lane ? 0xFFFFFFFFu : 0u;  // lane 0's carry-in comes from the left warp
-    // a shifted first tick reads the right warp's row-0 word (half-step 0 is the only update)
+    // a shifted first tick reads the right warp's row-0 word (half-step 0's is the tick's only
+    // exact update; the others read whatever the buffer holds and feed only inexact rows)
     if (par0 && lane == 0) xbuf[warp * NH] = win[2][H];
 
     if (__syncthreads_or(timed_out)) goto abort;

@@ -78,3 +78,34 @@ def test_load_rejects_wrong_size(kpzb, tmp_path):
         d.loadBit(f)
     for x in (s, t, d):
         x.close()
+
+
+@pytest.mark.parametrize("inner", ["dbsh", "dbshrep"])
+def test_dt_checkpoint_keeps_the_inner_scheme(kpzb, tmp_path, inner):
+    """A DT checkpoint carries the inner decomposition: a handle left at the default scheme
+    resumes with the saved one, bit for bit; DB4 checkpoints resume too."""
+    a = make(kpzb, 10, 9, "dt", 0.9, 0.2, 5)
+    a.setDtInner(inner)
+    a.mcsPQSyncRng(3)
+    f = tmp_path / "dt.bin"
+    a.saveBit(f)
+    a.mcsPQSyncRng(4)
+    ref = a.popSystem()
+    a.close()
+    b = kpzb.Scheduler(10, 9, scheduler="dt")
+    b.loadBit(f)
+    b.mcsPQSyncRng(4)
+    assert np.array_equal(b.popSystem(), ref)
+    b.close()
+    c = make(kpzb, 9, 8, "db4", 0.9, 0.2, 6)
+    c.mcsPQSyncRng(2)
+    g = tmp_path / "db4.bin"
+    c.saveBit(g)
+    c.mcsPQSyncRng(3)
+    ref4 = c.popSystem()
+    c.close()
+    d = kpzb.Scheduler(9, 8, scheduler="db4")
+    d.loadBit(g)
+    d.mcsPQSyncRng(3)
+    assert np.array_equal(d.popSystem(), ref4)
+    d.close()

@@ -133,6 +133,15 @@ constexpr int DT_VROW = 20;
 // An 8-byte table entry in shared memory: x = w | w_right << 16, y = w_down | sh << 10 |
 // (shr - 2) << 15 | (shd - 3) << 20 (the rotate amounts of site_entry, each read by shifting
 // y right and used modulo 32); bits 25-26 are left for flags.
+// The DT / DB4 table: the same with byte offsets (x = 4 w | 4 w_right << 16, y = 4 w_down |
+// sh << 11 | (shr - 2) << 16 | (shd - 3) << 21), so an address is one add to the thread's
+// byte base; bits 26-27 are left for flags.
+__device__ __forceinline__ uint2 pack_entry_bytes(const uint4 e)
+{
+    return make_uint2((4u * e.x) | ((4u * e.y) << 16),
+                      (4u * e.z) | ((e.w & 31u) << 11) | (((e.w >> 8) & 31u) << 16) | (((e.w >> 16) & 31u) << 21));
+}
+
 __device__ __forceinline__ uint2 pack_entry(const uint4 e)
 {
     return make_uint2(e.x | (e.y << 16),
@@ -190,16 +199,19 @@ dt_kernel(uint32_t* __restrict__ sys, int lxw, int lyw, int lnbx, int nblocks, i
             // is the block's last in its row / column (it starts 8 sites before the block's edge)
             const int sc = tid >> 4, pb = tid & 15;
             const int ux = 4 * (sc & 1) + (pb & 3), uy = 4 * (sc >> 1) + (pb >> 2);
-            uint2 e = pack_entry(site_entry(ux + ax, uy + ay));
-            e.y |= (ux >= 8 - DB4_BORDER ? 1u << 25 : 0u) | (uy >= 8 - DB4_BORDER ? 1u << 26 : 0u);
+            uint2 e = pack_entry_bytes(site_entry(ux + ax, uy + ay));
+            e.y |= (ux >= 8 - DB4_BORDER ? 1u << 26 : 0u) | (uy >= 8 - DB4_BORDER ? 1u << 27 : 0u);
             lut[tid] = e;
         }
     } else {
         for (int i = tid; i < NLUT; i += DT_THREADS) lut[i] = pack_entry(site_entry(i % DT_VROW, i / DT_VROW));
     }
     // DB4: the last thread column / row owns the block's dead border
-    const uint32_t dead_mask = (threadIdx.x == DT_TX - 1 ? 1u << 25 : 0u) | (threadIdx.y == DT_TY - 1 ? 1u << 26 : 0u);
+    const uint32_t dead_mask = (threadIdx.x == DT_TX - 1 ? 1u << 26 : 0u) | (threadIdx.y == DT_TY - 1 ? 1u << 27 : 0u);
     const int tbase = 2 * threadIdx.y * DT_TW + 2 * threadIdx.x;
+    // the thread cell's first word in the tiles, as byte pointers for the DT / DB4 table
+    char* tcell = reinterpret_cast<char*>(tile + tbase);
+    const char* dcell = reinterpret_cast<const char*>(dtile + (DIS ? tbase : 0));
     // a shifted cell whose site passes the block's right / lower edge wraps to its left / upper
     // edge (the reference masks coordinates with M_BLOCK_DIM): the cell's words move back by
     // a block's width / height
@@ -365,10 +377,11 @@ dt_kernel(uint32_t* __restrict__ sys, int lxw, int lyw, int lnbx, int nblocks, i
                 } else {
                     const uint2 e = lut[sc * 16u + pb];
                     if (!DB4 || (e.y & dead_mask) == 0u) {
-                        const int w = tbase + (int)(e.x & 0xFFFFu), wr = tbase + (int)(e.x >> 16);
-                        const int wd = tbase + (int)(e.y & 1023u);
-                        const uint32_t r1 = e.y >> 10, r2 = e.y >> 15, r3 = e.y >> 20;
-                        const uint32_t cw = tile[w], rw = tile[wr], dw = tile[wd];
+                        uint32_t* pw = reinterpret_cast<uint32_t*>(tcell + (e.x & 0xFFFFu));
+                        uint32_t* pr = reinterpret_cast<uint32_t*>(tcell + (e.x >> 16));
+                        uint32_t* pd = reinterpret_cast<uint32_t*>(tcell + (e.y & 2047u));
+                        const uint32_t r1 = e.y >> 11, r2 = e.y >> 16, r3 = e.y >> 21;
+                        const uint32_t cw = *pw, rw = *pr, dw = *pd;
                         const uint32_t cfg = (__funnelshift_r(cw, cw, r1) & 3u) | (__funnelshift_r(rw, rw, r2) & 4u) |
                                              (__funnelshift_r(dw, dw, r3) & 8u);
                         bool flip, is_p;
@@ -376,7 +389,8 @@ dt_kernel(uint32_t* __restrict__ sys, int lxw, int lyw, int lnbx, int nblocks, i
                             is_p = cfg == 12u;
                             flip = false;
                             if (is_p || cfg == 3u) {
-                                const int cls = (int)(__funnelshift_r(dtile[w], dtile[w], r1) & 3u);
+                                const uint32_t dw0 = *reinterpret_cast<const uint32_t*>(dcell + (e.x & 0xFFFFu));
+                                const int cls = (int)(__funnelshift_r(dw0, dw0, r1) & 3u);
                                 const Thresh& th = is_p ? dr.tp[cls] : dr.tq[cls];
                                 flip = th.always || (th.planes && u < th.t);
                             }
@@ -385,9 +399,9 @@ dt_kernel(uint32_t* __restrict__ sys, int lxw, int lyw, int lnbx, int nblocks, i
                             flip = (is_p || cfg == cfg_q) && u <= (is_p ? lim_p : lim_q);
                         }
                         if (flip) {
-                            atomicXor(&tile[w], __funnelshift_l(3u, 3u, r1));
-                            atomicXor(&tile[wr], __funnelshift_l(4u, 4u, r2));
-                            atomicXor(&tile[wd], __funnelshift_l(8u, 8u, r3));
+                            atomicXor(pw, __funnelshift_l(3u, 3u, r1));
+                            atomicXor(pr, __funnelshift_l(4u, 4u, r2));
+                            atomicXor(pd, __funnelshift_l(8u, 8u, r3));
                             if (COUNT) {
                                 if (is_p) ++ndep;
                                 else ++ndes;

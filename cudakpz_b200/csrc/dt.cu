@@ -66,17 +66,21 @@ struct DtRule {
 };
 
 // One attempt of the random-sequential rule (PQSyncRng::update,
-// kpz/kpzSimulationPrimitivesTemplates.cu:250-281) at tile word w, its right neighbour's word
-// wr and its lower neighbour's word wd.  r1, r2, r3: rotate amounts (used modulo 32) that
-// bring the site's two slope bits to bits 0-1, the right neighbour's x-slope bit to bit 2 and
-// the lower neighbour's y-slope bit to bit 3.
+// kpz/kpzSimulationPrimitivesTemplates.cu:250-281) at the site of table entry e (pack_entry_bytes)
+// relative to the byte bases tb (lattice tile) and db (disorder tile): the entry gives the
+// byte offsets of the site's word, its right neighbour's and its lower neighbour's, and the
+// rotate amounts (used modulo 32) that bring the site's two slope bits to bits 0-1, the right
+// neighbour's x-slope bit to bit 2 and the lower neighbour's y-slope bit to bit 3.
 template <bool COUNT, bool DIS>
-__device__ __forceinline__ void dt_attempt_at(uint32_t* tile, const uint32_t* dtile, int w, int wr, int wd,
-                                              uint32_t r1, uint32_t r2, uint32_t r3, uint32_t u, const DtRule rule,
+__device__ __forceinline__ void dt_attempt_at(char* tb, const char* db, uint2 e, uint32_t u, const DtRule rule,
                                               const DisorderRates& dr, unsigned long long& ndep,
                                               unsigned long long& ndes)
 {
-    const uint32_t cw = tile[w], rw = tile[wr], dw = tile[wd];
+    uint32_t* pw = reinterpret_cast<uint32_t*>(tb + (e.x & 0xFFFFu));
+    uint32_t* pr = reinterpret_cast<uint32_t*>(tb + (e.x >> 16));
+    uint32_t* pd = reinterpret_cast<uint32_t*>(tb + (e.y & 2047u));
+    const uint32_t r1 = e.y >> 11, r2 = e.y >> 16, r3 = e.y >> 21;
+    const uint32_t cw = *pw, rw = *pr, dw = *pd;
     // configuration c | s_x(x+1)<<2 | s_y(y+1)<<3 (kpz/kpzSimulationPrimitivesTemplates.cu:
     // 258-260): three rotations, one mask each
     const uint32_t cfg = (__funnelshift_r(cw, cw, r1) & 3u) | (__funnelshift_r(rw, rw, r2) & 4u) |
@@ -86,7 +90,8 @@ __device__ __forceinline__ void dt_attempt_at(uint32_t* tile, const uint32_t* dt
         is_p = cfg == 12u;
         flip = false;
         if (is_p || cfg == 3u) {
-            const int cls = (int)(__funnelshift_r(dtile[w], dtile[w], r1) & 3u);
+            const uint32_t dw0 = *reinterpret_cast<const uint32_t*>(db + (e.x & 0xFFFFu));
+            const int cls = (int)(__funnelshift_r(dw0, dw0, r1) & 3u);
             const Thresh& th = is_p ? dr.tp[cls] : dr.tq[cls];
             flip = th.always || (th.planes && u < th.t);
         }
@@ -99,9 +104,9 @@ __device__ __forceinline__ void dt_attempt_at(uint32_t* tile, const uint32_t* dt
         // this round (the atomics merely order its own three flips when two share a word);
         // under the dead-border schemes other threads' flips of the same phase may share them
         // (the reference's fctAtomicXor)
-        atomicXor(&tile[w], __funnelshift_l(3u, 3u, r1));
-        atomicXor(&tile[wr], __funnelshift_l(4u, 4u, r2));
-        atomicXor(&tile[wd], __funnelshift_l(8u, 8u, r3));
+        atomicXor(pw, __funnelshift_l(3u, 3u, r1));
+        atomicXor(pr, __funnelshift_l(4u, 4u, r2));
+        atomicXor(pd, __funnelshift_l(8u, 8u, r3));
         if (COUNT) {
             if (is_p) ++ndep;
             else ++ndes;
@@ -130,22 +135,14 @@ constexpr int DT_VSPAN = 18;  // in-cell offsets of the shifted schemes: up to 3
 // corner) then lie in 32 distinct banks, 8 bytes each
 constexpr int DT_VROW = 20;
 
-// An 8-byte table entry in shared memory: x = w | w_right << 16, y = w_down | sh << 10 |
-// (shr - 2) << 15 | (shd - 3) << 20 (the rotate amounts of site_entry, each read by shifting
-// y right and used modulo 32); bits 25-26 are left for flags.
-// The DT / DB4 table: the same with byte offsets (x = 4 w | 4 w_right << 16, y = 4 w_down |
-// sh << 11 | (shr - 2) << 16 | (shd - 3) << 21), so an address is one add to the thread's
-// byte base; bits 26-27 are left for flags.
+// An 8-byte table entry in shared memory, with byte offsets so that an address is one add to
+// a byte base: x = 4 w | 4 w_right << 16, y = 4 w_down | sh << 11 | (shr - 2) << 16 |
+// (shd - 3) << 21 (the rotate amounts of site_entry, each read by shifting y right and used
+// modulo 32); bits 26-27 are left for flags.
 __device__ __forceinline__ uint2 pack_entry_bytes(const uint4 e)
 {
     return make_uint2((4u * e.x) | ((4u * e.y) << 16),
                       (4u * e.z) | ((e.w & 31u) << 11) | (((e.w >> 8) & 31u) << 16) | (((e.w >> 16) & 31u) << 21));
-}
-
-__device__ __forceinline__ uint2 pack_entry(const uint4 e)
-{
-    return make_uint2(e.x | (e.y << 16),
-                      e.z | ((e.w & 31u) << 10) | (((e.w >> 8) & 31u) << 15) | (((e.w >> 16) & 31u) << 20));
 }
 
 // DIS: quenched disorder (Disorder2SyncRng_shared, kpz/kpzSimulationPrimitivesTemplates.cu:
@@ -204,7 +201,7 @@ dt_kernel(uint32_t* __restrict__ sys, int lxw, int lyw, int lnbx, int nblocks, i
             lut[tid] = e;
         }
     } else {
-        for (int i = tid; i < NLUT; i += DT_THREADS) lut[i] = pack_entry(site_entry(i % DT_VROW, i / DT_VROW));
+        for (int i = tid; i < NLUT; i += DT_THREADS) lut[i] = pack_entry_bytes(site_entry(i % DT_VROW, i / DT_VROW));
     }
     // DB4: the last thread column / row owns the block's dead border
     const uint32_t dead_mask = (threadIdx.x == DT_TX - 1 ? 1u << 26 : 0u) | (threadIdx.y == DT_TY - 1 ? 1u << 27 : 0u);
@@ -273,20 +270,16 @@ dt_kernel(uint32_t* __restrict__ sys, int lxw, int lyw, int lnbx, int nblocks, i
                     const int vy = ay + py + (SCHEME == DT_SCHEME_DB ? 0 : (int)((ob >> 3) & 7u));
                     const uint2 e = lut[vy * DT_VROW + vx];
                     const int base = wrapped_base(vx, vy);
-                    const int w = base + (int)(e.x & 0xFFFFu), wr = base + (int)(e.x >> 16);
-                    const int wd = base + (int)(e.y & 1023u);
+                    char* tb = reinterpret_cast<char*>(tile + base);
+                    const char* db = reinterpret_cast<const char*>(dtile + (DIS ? base : 0));
                     const uint32_t u = pick4(uu, j & 3);
                     if (REP) {
-                        if (ph == 0)
-                            dt_attempt_at<COUNT, DIS>(tile, dtile, w, wr, wd, e.y >> 10, e.y >> 15, e.y >> 20, u, rule,
-                                                      dr, ndep, ndes);
+                        if (ph == 0) dt_attempt_at<COUNT, DIS>(tb, db, e, u, rule, dr, ndep, ndes);
                         else ++hits;
                         __syncthreads();
                     } else {
                         for (int phase = 0; phase < 3; ++phase) {
-                            if (ph == phase)
-                                dt_attempt_at<COUNT, DIS>(tile, dtile, w, wr, wd, e.y >> 10, e.y >> 15, e.y >> 20, u,
-                                                          rule, dr, ndep, ndes);
+                            if (ph == phase) dt_attempt_at<COUNT, DIS>(tb, db, e, u, rule, dr, ndep, ndes);
                             __syncthreads();
                         }
                     }
@@ -329,13 +322,11 @@ dt_kernel(uint32_t* __restrict__ sys, int lxw, int lyw, int lnbx, int nblocks, i
                         const int vx = ax + px + (int)(ob & 7u), vy = ay + py + (int)((ob >> 3) & 7u);
                         const uint2 e = lut[vy * DT_VROW + vx];
                         const int base = wrapped_base(vx, vy);
-                        const int w = base + (int)(e.x & 0xFFFFu), wr = base + (int)(e.x >> 16);
-                        const int wd = base + (int)(e.y & 1023u);
+                        char* tb = reinterpret_cast<char*>(tile + base);
+                        const char* db = reinterpret_cast<const char*>(dtile + (DIS ? base : 0));
                         const uint32_t u = pick4(ruu, j & 3);
                         for (int phase = 0; phase < 3; ++phase) {
-                            if (ph == phase)
-                                dt_attempt_at<COUNT, DIS>(tile, dtile, w, wr, wd, e.y >> 10, e.y >> 15, e.y >> 20, u, rule,
-                                                          dr, ndep, ndes);
+                            if (ph == phase) dt_attempt_at<COUNT, DIS>(tb, db, e, u, rule, dr, ndep, ndes);
                             __syncthreads();
                         }
                     }
@@ -371,8 +362,8 @@ dt_kernel(uint32_t* __restrict__ sys, int lxw, int lyw, int lnbx, int nblocks, i
                     const int uy = 2 * (int)(sc & 2u) + (int)(pb >> 2) + (int)((ob >> 3) & 7u);
                     const uint2 e = lut[(uy + ay) * DT_VROW + ux + ax];
                     const int base = wrapped_base(ux, uy);
-                    dt_attempt_at<COUNT, DIS>(tile, dtile, base + (int)(e.x & 0xFFFFu), base + (int)(e.x >> 16),
-                                              base + (int)(e.y & 1023u), e.y >> 10, e.y >> 15, e.y >> 20, u, rule, dr,
+                    dt_attempt_at<COUNT, DIS>(reinterpret_cast<char*>(tile + base),
+                                              reinterpret_cast<const char*>(dtile + (DIS ? base : 0)), e, u, rule, dr,
                                               ndep, ndes);
                 } else {
                     const uint2 e = lut[sc * 16u + pb];

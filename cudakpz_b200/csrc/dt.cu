@@ -333,7 +333,8 @@ dt_kernel(uint32_t* __restrict__ sys, int lxw, int lyw, int lnbx, int nblocks, i
                 }
             }
         }
-        for (int rb = 0; !BORDER && rb < ROUNDS; rb += 8) {
+#pragma unroll 4
+        for (int rb = 0; rb < (BORDER ? 0 : ROUNDS); rb += 8) {
             if ((rb & 31) == 0)
                 pos = philox4x32_10(
                     make_uint4(cid, t, (T_POS << 24) | ((uint32_t)d << 16) | (uint32_t)(rb >> 5), stream), key);

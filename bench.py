@@ -346,11 +346,13 @@ def alu_ops_per_word(p, q):
 
 def run_e2e(args, torch, kpzb, scheds, N, M, world):
     """Public API with host buffers: push (pinned H2D) -> mcs -> pop (D2H) -> roughness, every
-    step, both lattices, through the asynchronous push/pop entry points.  Each lattice runs on
-    its own stream and its MCS waits for the other lattice's MCS to finish, so the lattices take
-    turns on the SMs and one lattice's copies and W^2 read overlap the other's MCS (two MCS
-    passes sharing the SMs would finish together and leave the copies exposed); each step's
-    W^2 is read while the other lattice's step runs."""
+    step, both lattices, through the asynchronous entry points.  Each lattice runs on its own
+    stream and its MCS waits for the other lattice's MCS to finish, so the lattices take turns
+    on the SMs and one lattice's copies and W^2 read overlap the other's MCS (two MCS passes
+    sharing the SMs would finish together and leave the copies exposed).  A step's roughness
+    is enqueued behind its pop, then the next step's input is pushed: kpzb_push_async copies it
+    into the handle's stage buffer on a copy stream while the current step is still queued, and
+    each step's W^2 is read while the other lattice's step runs."""
     import numpy as np
     nw = scheds[0].size_words()
     host = [torch.empty(nw, dtype=torch.int32).pin_memory() for _ in scheds]
@@ -371,9 +373,10 @@ def run_e2e(args, torch, kpzb, scheds, N, M, world):
     L = len(scheds)
     unread = [False] * L
     mcs_done = [None] * L
-    for _ in range(steps):
+    for h, s in zip(host, scheds):
+        s.pushSystemAsync(h.numpy().view(np.uint32))
+    for step in range(steps):
         for j, (h, o, s) in enumerate(zip(host, outs, scheds)):
-            s.pushSystemAsync(h.numpy().view(np.uint32))
             prev = (j - 1) % L  # with one lattice: itself
             if mcs_done[prev] is not None and prev != j:
                 streams[j].wait_event(mcs_done[prev])
@@ -382,15 +385,16 @@ def run_e2e(args, torch, kpzb, scheds, N, M, world):
             ev.record(streams[j])
             mcs_done[j] = ev
             s.popSystemAsync(o.numpy().view(np.uint32))
+            s.roughnessAsync()
+            if step + 1 < steps:
+                s.pushSystemAsync(h.numpy().view(np.uint32))
             unread[j] = True
             if unread[prev]:
-                scheds[prev].join()
-                scheds[prev].roughness()
+                scheds[prev].joinRoughness()
                 unread[prev] = False
     for j, s in enumerate(scheds):  # every step's result is read before the clock stops
         if unread[j]:
-            s.join()
-            s.roughness()
+            s.joinRoughness()
     torch.cuda.synchronize()
     dt = time.perf_counter() - t0
     dt = max_over_ranks(dt, world)

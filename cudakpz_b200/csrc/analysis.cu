@@ -4,7 +4,8 @@
 // Heights follow the reference's path walk (kpz/correlator.cpp:47-96, :337-399):
 //   row y starts at Hs(y) = h(0,y-1) + (2*s_y(0,y)-1) with h(0,-1) = 0, walks x = 1..L-1
 //   adding 2*s_x(x,y)-1, and the wrap adds 2*s_x(0,y)-1 giving h(0,y) = Hs(y) + rowsum(y).
-// Moments: S1 and S2 exact in int64, S3..S7 in FP64; ch uses the exact int64 cross sum;
+// Moments: S1 and S2 exact in int64, S3..S7 in FP64 (per 64-site chunk from exact integer
+// power sums of the offsets from the chunk's first height); ch uses the exact int64 cross sum;
 // cs counts equal minus different slope bits (kpz/correlator.cpp:463-477).
 // Invariants extend SchedulerService::consitencyCheck (kpz/schedulerService.cpp:733-854)
 // to ENC_CBBIT: x-slope row sums, y-slope column sums, plaquette loops.
@@ -174,6 +175,62 @@ walk_kernel(const uint32_t* __restrict__ sys, const uint32_t* __restrict__ snap,
             run = segc[ty];
             run_s = segc_s[ty];
             __syncthreads();
+            if constexpr (MODE == 0) {
+                // The chunk's heights are b + d_i with b the height before its first site and
+                // |d_i| <= 64, so the power sums of d are exact in 32/64-bit integers (d^4 sums to
+                // at most 64 * 64^4 < 2^31; d^5..d^7 accumulate in int64) and the moments of h
+                // follow once per chunk by the binomial expansion in FP64.  The row's first site
+                // (x = 0, height Hs + rowsum) is left out of the sums and added directly.
+                const long long b = Hs - e0 + P;
+                const bool first = c == 0;
+                int d = 0, a1 = 0, a2 = 0, a3 = 0, a4 = 0, dmin = 64, dmax = -64;
+                long long a5 = 0, a6 = 0, a7 = 0;
+#pragma unroll
+                for (int i = 0; i < 64; ++i) {
+                    const int bit = (int)((((i & 1) ? O : E) >> (i >> 1)) & 1u);
+                    d += 2 * bit - 1;
+                    if (i == 0 && first) continue;
+                    const int d2 = d * d, d3 = d2 * d, d4 = d2 * d2;
+                    a1 += d;
+                    a2 += d2;
+                    a3 += d3;
+                    a4 += d4;
+                    a5 += (long long)d4 * d;
+                    a6 += (long long)d3 * d3;
+                    a7 += (long long)d4 * d3;
+                    dmin = min(dmin, d);
+                    dmax = max(dmax, d);
+                }
+                const int n = first ? 63 : 64;
+                s1 += (long long)n * b + a1;
+                s2 += (long long)n * b * b + 2 * b * a1 + a2;
+                hmin = min(hmin, b + dmin);
+                hmax = max(hmax, b + dmax);
+                const double B = (double)b, B2 = B * B, B3 = B2 * B, B4 = B2 * B2, B5 = B4 * B, B6 = B3 * B3,
+                             B7 = B6 * B;
+                const double n_ = n, A1 = a1, A2 = a2, A3 = a3, A4 = a4, A5 = (double)a5, A6 = (double)a6,
+                             A7 = (double)a7;
+                s3 += n_ * B3 + 3.0 * B2 * A1 + 3.0 * B * A2 + A3;
+                s4 += n_ * B4 + 4.0 * B3 * A1 + 6.0 * B2 * A2 + 4.0 * B * A3 + A4;
+                s5 += n_ * B5 + 5.0 * B4 * A1 + 10.0 * B3 * A2 + 10.0 * B2 * A3 + 5.0 * B * A4 + A5;
+                s6 += n_ * B6 + 6.0 * B5 * A1 + 15.0 * B4 * A2 + 20.0 * B3 * A3 + 15.0 * B2 * A4 + 6.0 * B * A5 + A6;
+                s7 += n_ * B7 + 7.0 * B6 * A1 + 21.0 * B5 * A2 + 35.0 * B4 * A3 + 35.0 * B3 * A4 + 21.0 * B2 * A5 +
+                      7.0 * B * A6 + A7;
+                if (first) {
+                    const long long h = Hs + rsum;
+                    s1 += h;
+                    s2 += h * h;
+                    const double dh = (double)h, dh2 = dh * dh, dh3 = dh2 * dh;
+                    s3 += dh3;
+                    s4 += dh2 * dh2;
+                    s5 += dh3 * dh2;
+                    s6 += dh3 * dh3;
+                    s7 += dh3 * dh3 * dh;
+                    hmin = min(hmin, h);
+                    hmax = max(hmax, h);
+                }
+                continue;
+            }
             for (int i = 0; i < 64; ++i) {
                 const uint32_t bit = (((i & 1) ? O : E) >> (i >> 1)) & 1u;
                 P += 2 * (long long)bit - 1;

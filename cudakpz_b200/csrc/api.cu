@@ -49,6 +49,14 @@ struct kpzb_handle {
     uint32_t* d_sys = nullptr;   // internal layout: CBBIT (SCA, SCABIT) or LOCAL (DT)
     uint32_t* d_tmp = nullptr;   // scratch lattice (transcoding, fused double buffer)
     uint32_t* d_snap = nullptr;  // correlator snapshot, CBBIT
+    // kpzb_push_async of the SCABit and random-sequential dynamics: the host words land in a
+    // third lattice buffer on a copy stream, which then trades places with d_sys.  ev_ready
+    // (copy done) gates the handle's stream; ev_free (recorded on the handle's stream at the
+    // trade) gates the next copy into the buffer that d_sys was, until every read of it
+    // enqueued before the trade (a pop, a roughness) has run.
+    uint32_t* d_stage = nullptr;
+    cudaStream_t copy_st = nullptr;
+    cudaEvent_t ev_ready = nullptr, ev_free = nullptr;
     double snap_mean = 0.0;
     bool has_snap = false;
     uint64_t seed = 0;
@@ -156,8 +164,13 @@ extern "C" kpzb_status kpzb_destroy(kpzb_handle* h)
     if (!h) return KPZB_OK;
     cudaSetDevice(h->device);
     if (h->st) cudaStreamSynchronize(h->st);
+    if (h->copy_st) cudaStreamSynchronize(h->copy_st);
     cudaFree(h->d_sys);
     cudaFree(h->d_tmp);
+    cudaFree(h->d_stage);
+    if (h->ev_ready) cudaEventDestroy(h->ev_ready);
+    if (h->ev_free) cudaEventDestroy(h->ev_free);
+    if (h->copy_st) cudaStreamDestroy(h->copy_st);
     cudaFree(h->d_snap);
     cudaFree(h->d_counters);
     cudaFree(h->d_dis);
@@ -500,8 +513,29 @@ extern "C" kpzb_status kpzb_mcs(kpzb_handle* h, int n)
 extern "C" size_t kpzb_size_words(const kpzb_handle* h) { return h ? h->words() : 0; }
 extern "C" int kpzb_encoding(const kpzb_handle* h) { return h ? h->encoding() : -1; }
 
+// Asynchronous host push without a transcode: copy into the stage buffer on the copy stream
+// while the handle's stream still runs (an MCS, a pop of the previous lattice), then make the
+// stage the lattice.  The copy waits only for the reads of its target enqueued before the
+// previous trade.
+static kpzb_status push_staged(kpzb_handle* h, const uint32_t* src)
+{
+    if (!h->d_stage) KPZB_CU(cudaMalloc(&h->d_stage, h->words() * 4), "cudaMalloc(stage)");
+    if (!h->copy_st) KPZB_CU(cudaStreamCreateWithFlags(&h->copy_st, cudaStreamNonBlocking), "copy stream");
+    if (!h->ev_ready) KPZB_CU(cudaEventCreateWithFlags(&h->ev_ready, cudaEventDisableTiming), "event");
+    // a fresh stage has no readers: waiting on the not yet recorded ev_free is a no-op
+    if (!h->ev_free) KPZB_CU(cudaEventCreateWithFlags(&h->ev_free, cudaEventDisableTiming), "event");
+    KPZB_CU(cudaStreamWaitEvent(h->copy_st, h->ev_free, 0), "stage wait");
+    KPZB_CU(cudaMemcpyAsync(h->d_stage, src, h->words() * 4, cudaMemcpyHostToDevice, h->copy_st), "push copy");
+    KPZB_CU(cudaEventRecord(h->ev_ready, h->copy_st), "event record");
+    KPZB_CU(cudaStreamWaitEvent(h->st, h->ev_ready, 0), "stage ready");
+    std::swap(h->d_sys, h->d_stage);
+    KPZB_CU(cudaEventRecord(h->ev_free, h->st), "event record");
+    return KPZB_OK;
+}
+
 static kpzb_status push_from(kpzb_handle* h, const uint32_t* src, cudaMemcpyKind kind, bool sync = true)
 {
+    if (!sync && kind == cudaMemcpyHostToDevice && h->dyn != KPZB_DYN_SCA) return push_staged(h, src);
     if (h->dyn == KPZB_DYN_SCA) {
         kpzb_status s = ensure_tmp(h);
         if (s != KPZB_OK) return s;

@@ -155,8 +155,11 @@ kpzb_status kpzb_push(kpzb_handle* h, const uint32_t* words);
 kpzb_status kpzb_pop(kpzb_handle* h, uint32_t* words);
 /* Asynchronous push/pop: enqueued on the handle's stream behind earlier work, returning at
  * once; the host buffer must stay valid until kpzb_join.  With page-locked host buffers the
- * copies overlap other handles' MCS.  (The reference copies synchronously after join():
- * kpz/schedulerBase.cu:35-52.) */
+ * copies overlap other handles' MCS.  For the SCABit, DT and DB4 dynamics kpzb_push_async
+ * copies into a stage buffer of the handle on a copy stream of its own, so the copy also
+ * overlaps this handle's queued MCS, pops and roughness, which still see the previous
+ * lattice; work enqueued after the push sees the new one.  (The reference copies
+ * synchronously after join(): kpz/schedulerBase.cu:35-52.) */
 kpzb_status kpzb_push_async(kpzb_handle* h, const uint32_t* words);
 kpzb_status kpzb_pop_async(kpzb_handle* h, uint32_t* words);
 /* Same, with device buffers of the caller (cudaMemcpyDeviceToDevice on the handle's stream). */
@@ -211,7 +214,8 @@ kpzb_status kpzb_enable_counters(kpzb_handle* h, int on);
 kpzb_status kpzb_check_invariants(kpzb_handle* h, int64_t rep[3]);
 
 /* Device pointer to the lattice in the handle's internal layout (ENC_CBBIT for SCA and
- * SCABit, ENC_LOCAL for DT) for tests and zero-copy callers. */
+ * SCABit, ENC_LOCAL for DT) for tests and zero-copy callers.  The lattice moves between the
+ * handle's buffers on an MCS and on kpzb_push_async: ask again after either. */
 kpzb_status kpzb_device_ptr(kpzb_handle* h, uint32_t** d_words, size_t* nwords);
 /* The CUDA stream the handle enqueues on (as void*, a cudaStream_t). */
 void* kpzb_stream(kpzb_handle* h);

@@ -257,6 +257,54 @@ def test_async_push_pop_equals_sync(kpzb, oracle, sched):
     s.close()
 
 
+@pytest.mark.parametrize("sched,lx", [("scaBit", 11), ("dt", 10), ("db4", 10)])
+def test_pipelined_push_equals_sync(kpzb, oracle, sched, lx):
+    """A staged kpzb_push_async (the next lattice copied from page-locked memory while the
+    current one's MCS, pop and roughness are still queued) gives, step for step, the lattices
+    and roughness of the synchronous push -> mcs -> pop -> roughness sequence on a second
+    handle, bit for bit; a second push before the next MCS replaces the first."""
+    import torch
+    ly = lx
+    enc = oracle.ENC_CBBIT if sched == "scaBit" else oracle.ENC_LOCAL
+    inputs = []
+    for k in range(3):
+        a = oracle.random_lattice(lx, ly, oracle.ENC_CBBIT, seed=31 + k, mcs=2 + k)
+        if enc == oracle.ENC_LOCAL:
+            a = oracle.cbbit_to_local(a, lx, ly)
+        t = torch.empty(a.size, dtype=torch.int32).pin_memory()
+        t.numpy().view(np.uint32)[:] = a
+        inputs.append(t)
+    outs = [torch.empty(inputs[0].numel(), dtype=torch.int32).pin_memory() for _ in range(3)]
+    n = 5
+    sa = kpzb.Scheduler(lx, ly, scheduler=sched)
+    sb = kpzb.Scheduler(lx, ly, scheduler=sched)
+    for s in (sa, sb):
+        s.setPQ(0.75, 0.25)
+        s.supplySeed(17)
+    got_r = []
+    sa.pushSystemAsync(inputs[0].numpy().view(np.uint32))
+    for k in range(3):
+        sa.mcsPQSyncRngAsync(n)
+        sa.popSystemAsync(outs[k].numpy().view(np.uint32))
+        sa.roughnessAsync()
+        if k + 1 < 3:
+            if k == 0:  # replaced by the push below before any MCS reads it
+                sa.pushSystemAsync(inputs[2].numpy().view(np.uint32))
+            sa.pushSystemAsync(inputs[k + 1].numpy().view(np.uint32))
+        got_r.append(sa.joinRoughness())
+    sa.join()
+    for k in range(3):
+        sb.pushSystem(inputs[k].numpy().view(np.uint32))
+        sb.mcsPQSyncRng(n)
+        ref = sb.popSystem()
+        got = outs[k].numpy().view(np.uint32)
+        assert first_diff(got, ref) is None, (k, first_diff(got, ref))
+        r = sb.roughness()
+        assert (got_r[k].w2, got_r[k].h) == (r.w2, r.h), k
+    sa.close()
+    sb.close()
+
+
 @pytest.mark.parametrize("p,q,kind", [(1.0, 0.0, "wave"), (0.5, 0.5, "band")])
 def test_untuned_default_plan(kpzb, oracle, monkeypatch, p, q, kind):
     """KPZB_AUTOTUNE=0: no measurement; the wave kernel for rates without random planes, the band

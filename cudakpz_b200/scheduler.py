@@ -257,7 +257,9 @@ class Scheduler:
 
     def pushSystemAsync(self, words: np.ndarray) -> None:
         """Enqueue the host->device copy; `words` must stay alive (and should be page-locked)
-        until join()."""
+        until join().  For scaBit, dt and db4 the copy runs on the handle's copy stream into a
+        stage buffer, overlapping work already queued (which still sees the previous lattice);
+        work queued afterwards sees the pushed one."""
         if words.dtype != np.uint32 or not words.flags.c_contiguous or words.size != self.size_words():
             raise ValueError("expected a contiguous uint32 array of size_words() words")
         check(lib.kpzb_push_async(self._h, words.ctypes.data), "kpzb_push_async")

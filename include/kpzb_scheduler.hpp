@@ -142,6 +142,12 @@ public:
         check(kpzb_pop(h_, host_.data()), "kpzb_pop");
     }
 
+    // asynchronous copies from / to a caller's buffer of sizeW() words (page-locked for the
+    // copies to overlap queued work), valid until join(); the reference copies synchronously
+    // after join() and has no counterpart
+    void pushSystemAsync(const uint32_t* words) { check(kpzb_push_async(h_, words), "kpzb_push_async"); }
+    void popSystemAsync(uint32_t* words) { check(kpzb_pop_async(h_, words), "kpzb_pop_async"); }
+
     Roughness roughness()
     {
         double o[8];

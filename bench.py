@@ -38,6 +38,7 @@ UNIT = "attempted site updates/ns"
 # Per-launch DRAM traffic (dram__bytes_read.sum + dram__bytes_write.sum) of the pass kernels
 # at 16384^2, from one ncu capture per (p, q, pass kernel, MCS per pass); the commands and the
 # full figures are in profiles/scabit_fused_16384.md and profiles/scabit_wave_16384.md.
+DT_NCU_BYTES_32768 = 103.849e6 + 36.303e6
 NCU_TRAFFIC_PER_LAUNCH = {(1.0, 0.0, "band", 7): 67.324e6 + 23.171e6,
                           (0.5, 0.5, "band", 4): 67.218e6 + 17.975e6,
                           (1.0, 0.0, "wave", 6): 89.707e6 + 19.618e6}
@@ -649,6 +650,10 @@ def run_dt(args, world, rank, local):
     peak = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()).get("hbm_gbs", 6650.0) if (
         ROOT / "MEASURED_PEAKS.json").exists() else 6650.0
     ach = alg_launch / (per_launch * 1e-3) / 1e9
+    # DRAM bytes of one DT launch from an ncu capture of dt_kernel at 32768^2 (103.8 MB read +
+    # 36.3 MB written for 2^28 attempts), scaled by the lattice's sites: every launch reads and
+    # writes its domain set's blocks and halos once, so the traffic grows with N
+    traffic = round(DT_NCU_BYTES_32768 * N / (1 << 30)) if (not db4 and args.dt_inner == "dt") else None
     s.setStream(0)
     ok, rep = s.consitencyCheck()
     s.close()
@@ -669,8 +674,9 @@ def run_dt(args, world, rank, local):
                                f"inner scheme {args.dt_inner.upper()}"),
                   "mcs_per_step": m, "lattice": f"{1 << lx}x{1 << lx}", "parallelism": f"replicas x{world}"},
                  roofline={"bound": "hbm", "kernel": "dt_kernel", "achieved": round(ach, 1), "peak": peak,
-                           "unit": "GB/s", "frac": round(ach / peak, 4), "traffic": None,
-                           "note": "integer/barrier bound; " + ("1 B" if db4 else "0.52 B") + "/attempt algorithmic",
+                           "unit": "GB/s", "frac": round(ach / peak, 4), "traffic": traffic,
+                           "note": "integer/barrier bound; " + ("1 B" if db4 else "0.52 B") + "/attempt algorithmic"
+                           + ("; traffic scaled from a 32768^2 ncu capture" if traffic else ""),
                            "slower_roofline": "int-alu", "int_roofline": int_roofline},
                  clocks=clk, gpu_launches=launches, invariants_ok=ok, cpu_baseline=cpu)
 

@@ -1,6 +1,6 @@
 // SchedulerB200: the Kpz::SchedulerService subclass a maintainer adds to the CudaKpz tree to
-// run the reference's frontend on this library (the adapter of INTEGRATION.md, section 2).  It
-// forwards the scheduler virtuals to the kpzb C ABI and keeps the reference's host lattice
+// run the reference's frontend on this library.  It forwards the scheduler virtuals to the
+// kpzb C ABI and keeps the reference's host lattice
 // m_system in the reference's word layout, so the reference's own host analysis --
 // SchedulerService::roughness (kpz/schedulerService.cpp:292-297) and consitencyCheck
 // (:721-854) -- runs unchanged on lattices this library produced.

@@ -14,6 +14,8 @@
 // get row-start heights, (3) per-site walk with a CTA-wide scan of 64-site chunk sums.
 // Per-CTA partials are reduced in a fixed order so the FP64 sums are deterministic.
 #include <cstring>
+#include <map>
+#include <mutex>
 #include "kpzb_api_internal.h"
 #include "kpzb_common.cuh"
 #include "kpzb_internal.h"
@@ -566,15 +568,19 @@ cudaError_t analysis_invariants(const uint32_t* d_sys, int lx, int ly, AnalysisS
 // not stall other streams -- cudaMalloc and cudaFree can synchronize the device.  For them
 // this entry point reads a caller's device lattice and writes the caller's host output, and
 // keeps its scratch (row tables and per-CTA partial sums) in one file-scope device array of
-// fixed size.  Every GPU that loads the library holds the array until the process exits.
+// fixed size.  Every GPU that loads the library's module holds the array until the process
+// exits.
 //
 // Limit: ly <= NOALLOC_MAX_LY (at most 65536 rows); any lx the other entry points accept.
 // The array is shared by every call: concurrent calls that overlap on the GPU (on different
 // streams or host threads) race on it and must be serialized by the caller.  Every kernel
 // writes each scratch word before reading it, so nothing has to be cleared between calls.
-// On each device the first call looks up the array's device address with
-// cudaGetSymbolAddress while that device is current; that first call should therefore come
-// before any stream capture the caller starts.
+// Set-up: the array's device address is looked up with cudaGetSymbolAddress once per device
+// and CUDA context, while that device is current, and cached under the context's unique id;
+// a context created anew (after the caller's cudaDeviceReset) gets a fresh lookup.  That
+// first call may also load the library's module, and the array with it, so a caller with a
+// window in which nothing may be allocated makes one call before the window opens; the
+// first call on a device should come before any stream capture the caller starts.
 // ---------------------------------------------------------------------------------------
 namespace kpzb {
 
@@ -587,9 +593,66 @@ constexpr size_t NOALLOC_BYTES = NOALLOC_ROWINFO + NOALLOC_ROWSTART + NOALLOC_PA
 static __device__ __align__(256) unsigned char g_noalloc_scratch[NOALLOC_BYTES];
 
 namespace {
-constexpr int NOALLOC_MAX_DEVICES = 64;
-void* g_noalloc_addr[NOALLOC_MAX_DEVICES] = {};
+// driver entry points for the current context and its process-unique id (CUDA >= 12.0),
+// resolved once through the runtime so the library needs no link against libcuda
+using CtxGetCurrentFn = int (*)(void**);
+using CtxGetIdFn = int (*)(void*, unsigned long long*);
+struct NoallocSetup {
+    unsigned long long ctx_id = 0;
+    void* addr = nullptr;
+};
+std::mutex g_noalloc_mu;
+std::map<int, NoallocSetup> g_noalloc_setup;  // per device: context id -> symbol address
+CtxGetCurrentFn g_ctx_get_current = nullptr;
+CtxGetIdFn g_ctx_get_id = nullptr;
+bool g_ctx_fns_looked_up = false;
+
+// id of the context current on this thread; false when there is none (or it is gone)
+bool current_ctx_id(unsigned long long* id)
+{
+    if (!g_ctx_fns_looked_up) {
+        g_ctx_fns_looked_up = true;
+        cudaDriverEntryPointQueryResult q1, q2;
+        void* f1 = nullptr;
+        void* f2 = nullptr;
+        if (cudaGetDriverEntryPointByVersion("cuCtxGetCurrent", &f1, 12000, cudaEnableDefault, &q1) ==
+                cudaSuccess && q1 == cudaDriverEntryPointSuccess &&
+            cudaGetDriverEntryPointByVersion("cuCtxGetId", &f2, 12000, cudaEnableDefault, &q2) == cudaSuccess &&
+            q2 == cudaDriverEntryPointSuccess) {
+            g_ctx_get_current = reinterpret_cast<CtxGetCurrentFn>(f1);
+            g_ctx_get_id = reinterpret_cast<CtxGetIdFn>(f2);
+        }
+    }
+    if (!g_ctx_get_current || !g_ctx_get_id) return false;
+    void* ctx = nullptr;
+    if (g_ctx_get_current(&ctx) != 0 || !ctx) return false;
+    return g_ctx_get_id(ctx, id) == 0;
+}
 }  // namespace
+
+// The scratch array's device address on the current device (set-up once per device and
+// context; see above).
+static cudaError_t noalloc_scratch_addr(int dev, void** out)
+{
+    std::lock_guard<std::mutex> lk(g_noalloc_mu);
+    unsigned long long id = 0;
+    const bool have_ctx = current_ctx_id(&id);
+    auto it = g_noalloc_setup.find(dev);
+    if (have_ctx && it != g_noalloc_setup.end() && it->second.ctx_id == id && it->second.addr) {
+        *out = it->second.addr;
+        return cudaSuccess;
+    }
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess) return e;
+    if (!p) return cudaErrorInvalidSymbol;
+    unsigned long long id_after = 0;
+    // the lookup makes the device's primary context current if none was
+    if (current_ctx_id(&id_after)) g_noalloc_setup[dev] = NoallocSetup{id_after, p};
+    else g_noalloc_setup.erase(dev);  // no id to key on: look up again next time
+    *out = p;
+    return cudaSuccess;
+}
 
 }  // namespace kpzb
 
@@ -605,14 +668,10 @@ extern "C" kpzb_status kpzb_roughness_noalloc(const uint32_t* d_cbbit, int lx, i
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
-    if (dev < 0 || dev >= NOALLOC_MAX_DEVICES) return fail(KPZB_EINVAL, "device index beyond 63");
-    if (!g_noalloc_addr[dev]) {
-        void* p = nullptr;
-        e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-        if (e != cudaSuccess || !p) return cuda_fail(e, "cudaGetSymbolAddress(no-alloc scratch)");
-        g_noalloc_addr[dev] = p;
-    }
-    unsigned char* base = static_cast<unsigned char*>(g_noalloc_addr[dev]);
+    void* addr = nullptr;
+    e = noalloc_scratch_addr(dev, &addr);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(no-alloc scratch)");
+    unsigned char* base = static_cast<unsigned char*>(addr);
     AnalysisScratch view;
     view.rowinfo = reinterpret_cast<int32_t*>(base);
     view.rowstart = reinterpret_cast<int64_t*>(base + NOALLOC_ROWINFO);

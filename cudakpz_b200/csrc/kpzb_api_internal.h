@@ -54,7 +54,7 @@ enum DtScheme {
 struct DtState {
     int grid = 0;
     bool ready = false;
-    int scheme = DT_SCHEME_DT;  // inner decomposition of a block
+    int scheme = DT_SCHEME_DBSH;  // inner decomposition of a block (the reference's default)
 };
 kpzb_status dt_init(DtState* s, int lx, int ly, int sm_count, bool db4 = false);
 void dt_free(DtState* s);

@@ -91,6 +91,9 @@ Plan explicit_plan(int lx, int ly, int k, int sm_count)
     const char* env = getenv("KPZB_PASS_KERNEL");
     const std::string v = env ? env : "";
     if (k <= 1 || v == "band") return Plan{k, 0, 0.f, false, PASS_BAND};
+    // "band1" .. "band3": the band kernel with that CTAs-per-SM choice (the tuner's candidates)
+    if (v.size() == 5 && v.compare(0, 4, "band") == 0 && v[4] >= '1' && v[4] <= '3')
+        return Plan{k, v[4] - '0', 0.f, false, PASS_BAND};
     if (v.compare(0, 4, "wave") == 0) {
         const int cps = v.size() > 4 ? v[4] - '0' : 2;
         if (scabit_wave_shape(lx, ly, k, sm_count, cps, DEC_NONE).ok) return Plan{k, cps, 0.f, false, PASS_WAVE};

@@ -110,10 +110,11 @@ class Scheduler:
         return True
 
     def setDtInner(self, inner: str) -> None:
-        """DT handles: "dt" (single-hit double tiling, default), "dbsh" (the reference's
-        default single-hit dead border inner decomposition), "db" (dead border, no offset),
-        "dtdbsh" (double tiling with a per-round cell offset) or "dbshrep" (DBSH with the
-        border hits replaced after the rounds)."""
+        """DT handles: "dbsh" (single-hit dead border: the reference's default build,
+        kpz/param.h:36, and the default of a new handle), "dt" (single-hit double tiling,
+        about twice as fast), "db" (dead border, no offset), "dtdbsh" (double tiling with a
+        per-round cell offset) or "dbshrep" (DBSH with the border hits replaced after the
+        rounds)."""
         if inner not in _DT_INNER:
             raise ValueError(f"unknown DT inner scheme {inner!r}; expected one of {sorted(_DT_INNER)}")
         check(lib.kpzb_set_dt_inner(self._h, _DT_INNER[inner]), "kpzb_set_dt_inner")

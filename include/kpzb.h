@@ -83,9 +83,11 @@ kpzb_status kpzb_set_pq(kpzb_handle* h, double p, double q);
 kpzb_status kpzb_seed(kpzb_handle* h, uint64_t seed, uint32_t stream);
 
 /* DT only: the inner decomposition of a block, the reference's compile-time KPZ_INNER_DD
- * (kpz/param.h, kpz/kpzConst.h:26-35): KPZB_DT_INNER_DT (single-hit double tiling, the
- * default here), KPZB_DT_INNER_DBSH (single-hit dead border, the reference's default:
+ * (kpz/param.h, kpz/kpzConst.h:26-35): KPZB_DT_INNER_DBSH (single-hit dead border, the
+ * reference's default build (kpz/param.h:36) and the default of a new DT handle:
  * BaseDTInnerDBSH, kpz/kpzSimulationPrimitivesTemplates_BaseInnerDB.cu:110-163),
+ * KPZB_DT_INNER_DT (single-hit double tiling, about twice as fast; a different
+ * decomposition, so W^2(t) differs from DBSH's by about 0.5 % at early times),
  * KPZB_DT_INNER_DB (dead border without the per-round cell offset: BaseDTInnerDB, :30-74),
  * KPZB_DT_INNER_DTDBSH (double tiling with a random per-round cell offset:
  * BaseDTInnerDTDBSH, kpz/kpzSimulationPrimitivesTemplates_BaseInnerDTr.cu:30-85) or
@@ -180,12 +182,16 @@ kpzb_status kpzb_roughness_async(kpzb_handle* h);
 kpzb_status kpzb_roughness_join(kpzb_handle* h, double out[8]);
 /* Roughness (as kpzb_roughness) of a caller's device ENC_CBBIT lattice, without allocating:
  * no cudaMalloc/cudaFree or allocating library call; scratch lives in a fixed device array
- * of about 1.2 MB held by every GPU that loads the library.  For callers that cannot
- * allocate device memory at measurement time (their allocator owns the device, or an
+ * of about 1.2 MB held by every GPU that loads the library's module.  For callers that
+ * cannot allocate device memory at measurement time (their allocator owns the device, or an
  * allocation would synchronize the device inside a timing loop).  No counterpart in the
- * reference.  Limit: ly <= 16.  Calls overlapping on the GPU race on the shared scratch; the
- * first call on each device looks up the scratch address and should precede any stream
- * capture.  `stream` is a cudaStream_t (NULL: default stream); synchronous. */
+ * reference.  Limit: ly <= 16.  Calls overlapping on the GPU race on the shared scratch.
+ * Set-up: the scratch's device address is looked up once per device and CUDA context (again
+ * after the caller recreates the context, e.g. by cudaDeviceReset); that first call may also
+ * load the library's module with its array, so a caller whose no-allocation window must see
+ * no allocation at all makes one call before the window, and the first call on a device
+ * should precede any stream capture.  `stream` is a cudaStream_t (NULL: default stream);
+ * synchronous. */
 kpzb_status kpzb_roughness_noalloc(const uint32_t* d_cbbit, int lx, int ly, double out[8], void* stream);
 /* Exact power sums of the relative heights: s12[0] = sum h, s12[1] = sum h^2,
  * hminmax[0..1] = min/max height. */

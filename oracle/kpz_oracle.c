@@ -242,6 +242,93 @@ void ko_sca_mcs(uint32_t* w, int lx, int ly, int encoding, uint64_t seed, uint32
 }
 
 /* ------------------------------------------------------------------------ */
+/* Word-parallel form of the same dynamics on ENC_CBBIT words: 32 sites of   */
+/* one sublattice per word, the mask algebra of kpz/kpzSCABitCores.cu:69-74, */
+/* 139-145 on the geometry of kpz/kpzSCABit.cu:120-172 (row y of sublattice */
+/* sigma reads the other sublattice's X word one bit to the right when x is */
+/* odd, i.e. when (y ^ sigma) & 1; kpz/schedulerCPUCBBit_nested.inl:208-257 */
+/* does the same 64 sites at a time).  The decision u < T is taken plane by  */
+/* plane from the MSB over the words of ko_plane_word: a site is below T at  */
+/* the first plane where its bit is 0 and T's is 1, above it where its bit  */
+/* is 1 and T's 0; once T has no 1 bit left below the plane, sites still    */
+/* equal can no longer fall below it.  Gives ko_sca_mcs's lattice and       */
+/* counts for every rate (checked on the CPU), in a few seconds at 16384^2. */
+/* ------------------------------------------------------------------------ */
+static uint32_t words_below(uint32_t cand, uint64_t T, uint64_t seed, uint32_t stream, uint32_t step,
+                            uint64_t qword, const uint32_t* plane_cache, int* planes_done)
+{
+    if (!cand || T == 0) return 0;
+    if (T >= ((uint64_t)1 << 32)) return cand;
+    uint32_t t = (uint32_t)T, lt = 0, eq = cand;
+    for (int k = 0; k < 32 && eq; ++k) {
+        uint32_t r;
+        if (k < *planes_done) {
+            r = plane_cache[k];
+        } else {
+            r = ko_plane_word(seed, stream, KO_TAG_SCA, step, (uint32_t)k, qword);
+            ((uint32_t*)plane_cache)[k] = r;
+            *planes_done = k + 1;
+        }
+        if ((t >> (31 - k)) & 1u) {
+            lt |= eq & ~r;
+            eq &= r;
+        } else {
+            eq &= ~r;
+        }
+        if ((t & (0xFFFFFFFFu >> (k + 1))) == 0 || k == 31) eq = 0; /* no 1 bit of T below plane k */
+    }
+    return lt;
+}
+
+void ko_sca_mcs_words(uint32_t* w, int lx, int ly, uint64_t seed, uint32_t stream, uint64_t t0, int n,
+                      double p, double q, int64_t* dep, int64_t* des)
+{
+    const uint64_t Tp = ko_threshold(p), Tq = ko_threshold(q);
+    const uint64_t Q = (uint64_t)1 << (lx + ly - 6), Wr = (uint64_t)1 << (lx - 6), M = (uint64_t)1 << ly;
+    int64_t nd = 0, nr = 0;
+    for (int i = 0; i < n; ++i)
+        for (int sigma = 0; sigma < 2; ++sigma) {
+            const uint32_t step = (uint32_t)(2 * (t0 + (uint64_t)i) + (uint64_t)sigma);
+            uint32_t* tXq = w + (uint64_t)(2 * sigma) * Q;
+            uint32_t* tYq = tXq + Q;
+            uint32_t* oXq = w + (uint64_t)(2 * (1 - sigma)) * Q;
+            uint32_t* oYq = oXq + Q;
+            for (uint64_t y = 0; y < M; ++y) {
+                const int shifted = (int)((y ^ (uint64_t)sigma) & 1u);
+                uint32_t* tX = tXq + y * Wr;
+                uint32_t* tY = tYq + y * Wr;
+                uint32_t* oX = oXq + y * Wr;
+                uint32_t* oY = oYq + ((y + 1) & (M - 1)) * Wr;
+                for (uint64_t j = 0; j < Wr; ++j) {
+                    const uint64_t jn = (j + 1) & (Wr - 1);
+                    const uint32_t xX = shifted ? (oX[j] >> 1) | (oX[jn] << 31) : oX[j];
+                    const uint32_t cp = ~tX[j] & ~tY[j] & xX & oY[j];
+                    const uint32_t cq = tX[j] & tY[j] & ~xX & ~oY[j];
+                    uint32_t cache[32];
+                    int done = 0;
+                    const uint64_t qword = y * Wr + j;
+                    const uint32_t m = words_below(cp, Tp, seed, stream, step, qword, cache, &done) |
+                                       words_below(cq, Tq, seed, stream, step, qword, cache, &done);
+                    if (!m) continue;
+                    nd += __builtin_popcount(m & cp);
+                    nr += __builtin_popcount(m & cq);
+                    tX[j] ^= m;
+                    tY[j] ^= m;
+                    oY[j] ^= m;
+                    if (shifted) {
+                        oX[j] ^= m << 1;
+                        oX[jn] ^= m >> 31;
+                    } else {
+                        oX[j] ^= m;
+                    }
+                }
+            }
+        }
+    if (dep) *dep += nd;
+    if (des) *des += nr;
+}
+
+/* ------------------------------------------------------------------------ */
 /* Heights: kpz/correlator.cpp:47-96. Start of row y adds s_y(0,y); then     */
 /* x = 1..L-1 adds s_x(x,y); then the wrap adds s_x(0,y) giving h(0,y).     */
 /* h(0,y) is recorded last; the value carried into row y+1 is h(0,y).       */

@@ -77,6 +77,10 @@ void ko_sca_mcs_dis(uint32_t* w, int lx, int ly, int encoding, uint64_t seed, ui
                     int64_t* dep, int64_t* des);
 void ko_sca_mcs(uint32_t* w, int lx, int ly, int encoding, uint64_t seed, uint32_t stream,
                 uint64_t t0, int n, double p, double q, int64_t* dep, int64_t* des);
+/* The same n MCS on ENC_CBBIT words, 32 sites per word operation (same lattice and counts as
+ * ko_sca_mcs with encoding ENC_CBBIT; fast enough for 16384^2 lattices). */
+void ko_sca_mcs_words(uint32_t* w, int lx, int ly, uint64_t seed, uint32_t stream, uint64_t t0, int n,
+                      double p, double q, int64_t* dep, int64_t* des);
 
 /* ---- heights, roughness, correlator ---- */
 /* Relative heights along the reference's path walk; h is int32[2^(lx+ly)], row-major. */

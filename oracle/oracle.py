@@ -43,6 +43,8 @@ def _load():
                                    C.c_uint32, C.c_uint32, C.c_uint64, C.c_uint64, i64p, i64p]),
         "ko_sca_mcs": (None, [u32p, C.c_int, C.c_int, C.c_int, C.c_uint64, C.c_uint32, C.c_uint64,
                               C.c_int, C.c_double, C.c_double, i64p, i64p]),
+        "ko_sca_mcs_words": (None, [u32p, C.c_int, C.c_int, C.c_uint64, C.c_uint32, C.c_uint64, C.c_int,
+                                    C.c_double, C.c_double, i64p, i64p]),
         "ko_heights": (None, [u32p, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_int32)]),
         "ko_power_sums": (None, [C.POINTER(C.c_int32), C.c_uint64, i64p, i64p]),
         "ko_roughness": (None, [u32p, C.c_int, C.c_int, C.c_int, dblp]),
@@ -133,6 +135,15 @@ def sca_mcs(w: np.ndarray, lx: int, ly: int, encoding: int, seed: int, stream: i
     """In place; returns (#deposits, #desorptions)."""
     dep, des = C.c_int64(0), C.c_int64(0)
     lib.ko_sca_mcs(_u32(w), lx, ly, encoding, seed, stream, t0, n, p, q, C.byref(dep), C.byref(des))
+    return dep.value, des.value
+
+
+def sca_mcs_words(w: np.ndarray, lx: int, ly: int, seed: int, stream: int, t0: int, n: int, p: float,
+                  q: float):
+    """ko_sca_mcs on ENC_CBBIT words, 32 sites per operation (equal results, fast at 16384^2).
+    In place; returns (#deposits, #desorptions)."""
+    dep, des = C.c_int64(0), C.c_int64(0)
+    lib.ko_sca_mcs_words(_u32(w), lx, ly, seed, stream, t0, n, p, q, C.byref(dep), C.byref(des))
     return dep.value, des.value
 
 

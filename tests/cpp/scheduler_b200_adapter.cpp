@@ -8,9 +8,13 @@
 // oracle/build_ref.py compiles it against the reference's headers and CPU objects (never
 // copied into this repository) into oracle/_ref/kpz_ref_adapter.  Usage:
 //   kpz_ref_adapter LX P Q SEED N   ->  "RESULT <reference W2> <kpzb W2> <reference consistency ok>"
+//   kpz_ref_adapter dtcurve LX P Q SEED T1 T2 ...
+//       --scheduler dt through the adapter: "<t> <W2>" per time, W2 from the reference's own
+//       SchedulerService::roughness on the popped lattice
 #include <cstdio>
 #include <cstdlib>
 #include <iostream>
+#include <sstream>
 #include <stdexcept>
 #include <string>
 
@@ -35,6 +39,9 @@ public:
         : SchedulerService(lx, ly, dynamics == KPZB_DYN_SCABIT ? ENC_CBBIT : ENC_LOCAL)
     {
         ck(kpzb_create(&h_, lx, ly, dynamics, device));
+        // the block-level decomposition the reference's DT scheduler is built with by
+        // default (KPZ_INNER_DD = KPZ_INNER_DBSH, kpz/param.h:36), set explicitly
+        if (dynamics == KPZB_DYN_DT) ck(kpzb_set_dt_inner(h_, KPZB_DT_INNER_DBSH));
     }
     ~SchedulerB200() override { kpzb_destroy(h_); }
     kpzb_handle* handle() { return h_; }
@@ -82,8 +89,41 @@ public:
 };
 }  // namespace Kpz
 
+static int dt_curve(int argc, char** argv)
+{
+    const int lx = std::atoi(argv[2]);
+    const double p = std::atof(argv[3]), q = std::atof(argv[4]);
+    const unsigned long long seed = std::strtoull(argv[5], nullptr, 10);
+    try {
+        std::streambuf* keep = std::cout.rdbuf();
+        std::cout.rdbuf(nullptr);
+        Kpz::Correlator::setNThreads(2);
+        Kpz::SchedulerB200 s(lx, lx, KPZB_DYN_DT, 0);
+        s.seed(seed);
+        s.initHomogeneous(Kpz::SchedulerService::ENC_LOCAL);
+        s.setPQ(p, q);
+        int t = 0;
+        std::ostringstream out;
+        out.precision(17);
+        for (int i = 6; i < argc; ++i) {
+            const int T = std::atoi(argv[i]);
+            s.mcsPQSyncRng(T - t);
+            t = T;
+            s.popSystem();
+            out << T << " " << (double)s.roughness().w2 << "\n";
+        }
+        std::cout.rdbuf(keep);
+        std::cout << out.str() << std::flush;
+    } catch (const std::exception& e) {
+        std::fprintf(stderr, "error: %s\n", e.what());
+        return 1;
+    }
+    return 0;
+}
+
 int main(int argc, char** argv)
 {
+    if (argc >= 7 && std::string(argv[1]) == "dtcurve") return dt_curve(argc, argv);
     if (argc < 6) {
         std::cerr << "usage: kpz_ref_adapter LX P Q SEED N\n";
         return 2;

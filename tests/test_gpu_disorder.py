@@ -48,6 +48,7 @@ def test_dt_disorder_bit_exact(kpzb, oracle):
     p, q = [0.95, 0.5], [0.05, 0.5]
     dis = disorder_words(oracle, lx, ly, 0.4, 8)
     s = kpzb.Scheduler(lx, ly, scheduler="dt")
+    s.setDtInner("dt")  # ko_dt_mcs_dis emulates the DT scheme
     s.setPQ(p[0], q[0])
     s.setPQ(p[1], q[1], 1)
     s.supplySeed(3)

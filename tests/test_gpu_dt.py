@@ -19,6 +19,7 @@ pytestmark = pytest.mark.gpu
 
 def run_dt(kpzb, lx, ly, p, q, seed, n, init=None, stream=0, counters=False):
     s = kpzb.Scheduler(lx, ly, scheduler="dt")
+    s.setDtInner("dt")  # the scheme ko_dt_mcs emulates (a new handle runs DBSH)
     s.setPQ(p, q)
     s.supplySeed(seed, stream)
     if init is not None:
@@ -86,6 +87,7 @@ def test_dt_statistics_match_random_sequential(kpzb, oracle):
     w_dt, w_rs, v_dt, v_rs = [], [], [], []
     for sd in seeds:
         s = kpzb.Scheduler(lx, ly, scheduler="dt")
+        s.setDtInner("dt")
         s.setPQ(p, q)
         s.supplySeed(sd)
         s.enableCounters(True)

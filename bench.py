@@ -252,7 +252,8 @@ def run_ours(args, world, rank, local):
         fused = (M // k) if k > 1 else 0
         launches_per_step += fused + 2 * (M - fused * k)
     kinds = sorted({pl[2] for pl in plans if pl[0] > 1})
-    kernel_names = {"stream": "scabit_stream_kernel", "band": "scabit_fused_kernel", "wave": "scabit_wave_kernel"}
+    kernel_names = {"stream": "scabit_stream_kernel", "band": "scabit_fused_kernel", "wave": "scabit_wave_kernel",
+                    "strip": "scabit_strip_kernel"}
     dominant = "+".join(kernel_names[k] for k in kinds) if kinds else "scabit_half_kernel"
     # algorithmic bytes: 1 B per attempted update over the whole timed region, divided by the
     # device time of the launches (fused passes carry more than 95 % of it)

@@ -301,8 +301,11 @@ extern "C" kpzb_status kpzb_get_plan(kpzb_handle* h, int* mcs_per_pass, int* cta
     if (s != KPZB_OK) return s;
     if (p.k > 1 && plan_shape_ok(p, h->lx, h->ly, h->sm_count)) {
         *mcs_per_pass = p.k;
-        *ctas_per_sm = p.kind == PASS_STREAM && p.cps == 0 ? 1 : p.cps;
-        *pass_kernel = p.kind == PASS_STREAM ? KPZB_PASS_STREAM : p.kind == PASS_WAVE ? KPZB_PASS_WAVE : KPZB_PASS_BAND;
+        *ctas_per_sm = p.kind == PASS_STRIP ? p.band : p.kind == PASS_STREAM && p.cps == 0 ? 1 : p.cps;
+        *pass_kernel = p.kind == PASS_STREAM  ? KPZB_PASS_STREAM
+                       : p.kind == PASS_WAVE  ? KPZB_PASS_WAVE
+                       : p.kind == PASS_STRIP ? KPZB_PASS_STRIP
+                                              : KPZB_PASS_BAND;
     }
     return KPZB_OK;
 }
@@ -350,6 +353,13 @@ static kpzb_status resolve_plan(kpzb_handle* h, Plan* plan)
             plan->cps = 0;
         }
     }
+    if (plan->kind == PASS_STRIP) {
+        const int mode = dec_mode(make_thresh(thresh_of(h->p)), make_thresh(thresh_of(h->q)));
+        if (!scabit_strip_shape(h->lx, h->ly, plan->k, plan->band, mode).ok) {
+            plan->kind = PASS_BAND;
+            plan->cps = 0;
+        }
+    }
     return KPZB_OK;
 }
 
@@ -380,7 +390,19 @@ static kpzb_status enqueue_sca(kpzb_handle* h, int n)
     const int mode = dec_mode(make_thresh(Tp), make_thresh(Tq));
     const WaveShape ws = plan.kind == PASS_WAVE ? scabit_wave_shape(h->lx, h->ly, k, h->sm_count, plan.cps, mode)
                                                 : WaveShape{};
-    if (k > 1 && plan.kind == PASS_WAVE && ws.ok) {
+    const StripShape tile = plan.kind == PASS_STRIP ? scabit_strip_shape(h->lx, h->ly, k, plan.band, mode)
+                                                    : StripShape{};
+    if (k > 1 && plan.kind == PASS_STRIP && tile.ok) {
+        kpzb_status s = ensure_tmp(h);
+        if (s != KPZB_OK) return s;
+        while (n - done >= k) {
+            KPZB_CU(scabit_strip(h->d_sys, h->d_tmp, h->lx, h->ly, (uint32_t)(h->tdev + done), h->seed,
+                                 h->stream_id, Tp, Tq, tile, cnt, h->st),
+                    "scabit_strip");
+            std::swap(h->d_sys, h->d_tmp);
+            done += k;
+        }
+    } else if (k > 1 && plan.kind == PASS_WAVE && ws.ok) {
         kpzb_status s = ensure_tmp(h);
         if (s != KPZB_OK) return s;
         while (n - done >= k) {

@@ -15,20 +15,24 @@ int sm_count_of(int device);
 int auto_fusion(int lx, int ly);
 
 // SCABit pass shape: k MCS per HBM pass (1 = one launch per half-step), cps CTAs per SM
-// (0 = shape heuristic), the measured cost when it came from the tuner, and the pass kernel
-// (band: scabit_fused_kernel, stream: scabit_stream_kernel, wave: scabit_wave_kernel).
-enum PassKernel { PASS_BAND = 0, PASS_STREAM = 1, PASS_WAVE = 2 };
+// (0 = shape heuristic), the measured cost when it came from the tuner, the pass kernel
+// (band: scabit_fused_kernel, stream: scabit_stream_kernel, wave: scabit_wave_kernel, strip:
+// scabit_strip_kernel) and, for the strip kernel, the output rows of a tile.
+enum PassKernel { PASS_BAND = 0, PASS_STREAM = 1, PASS_WAVE = 2, PASS_STRIP = 3 };
 struct Plan {
     int k;
     int cps;
     float ms_per_mcs;
     bool tuned;
     int kind;
+    int band = 0;
 };
 // Pass kernel and CTAs per SM for an explicitly set fusion depth: the streaming kernel with one
-// chunk per SM, unless the environment variable KPZB_PASS_KERNEL says "band", "stream2" (two
-// chunks per SM) or "wave" / "wave1".."wave4" (the register-wavefront kernel, 2 or the given
-// CTAs per SM), or that shape does not fit.
+// chunk per SM, unless the environment variable KPZB_PASS_KERNEL says "band" / "band1".."band3"
+// (the band kernel, the shape heuristic's or the given CTAs per SM), "stream2" (two chunks per
+// SM), "wave" / "wave1".."wave3" (the register-wavefront kernel, 2 or the given CTAs per SM) or
+// "strip" / "strip<rows>" (the warp-tile kernel, tiles of 64 or the given output rows), or
+// that shape does not fit.
 Plan explicit_plan(int lx, int ly, int k, int sm_count);
 bool plan_shape_ok(const Plan& p, int lx, int ly, int sm_count);
 bool lookup_plan(int lx, int ly, uint64_t Tp, uint64_t Tq, int sm_count, Plan* out);

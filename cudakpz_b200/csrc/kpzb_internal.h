@@ -72,6 +72,28 @@ cudaError_t scabit_wave(const uint32_t* d_src, uint32_t* d_dst, int lx, int ly, 
                         uint32_t stream_id, uint64_t Tp, uint64_t Tq, const WaveShape& sh,
                         unsigned long long* d_counters, unsigned int* d_err, cudaStream_t st);
 
+// Warp-tile register-wavefront temporal blocking (scabit_strip.cu): k MCS per HBM pass, one
+// warp per tile of a 32-column strip of a quadrant row and a band of rows, the half-steps in
+// registers; strips overlap by two columns (one recomputed column each side).
+struct StripShape {
+    int mcs;           // MCS per pass (4, 6 or 8)
+    int band;          // output rows per tile
+    int nstrips;       // strips per quadrant row
+    int ntiles;        // strips x bands (warps)
+    int grid;          // CTAs
+    int threads;       // threads per CTA
+    bool random_plane; // strips laid out for rates with one random plane (DEC_ONE)
+    bool ok;
+};
+// mode: the DecMode of the rates (the kernel covers DEC_NONE and DEC_ONE); band_rows even.
+// A tile runs whole cycles of strip_cycle_rows(k) ticks over its band + 4k halo rows, so band
+// heights of m * strip_cycle_rows(k) - 4k rows waste no tick.
+int strip_cycle_rows(int mcs_per_pass);
+StripShape scabit_strip_shape(int lx, int ly, int mcs_per_pass, int band_rows, int mode);
+cudaError_t scabit_strip(const uint32_t* d_src, uint32_t* d_dst, int lx, int ly, uint32_t t0, uint64_t seed,
+                         uint32_t stream_id, uint64_t Tp, uint64_t Tq, const StripShape& sh,
+                         unsigned long long* d_counters, cudaStream_t st);
+
 // codec / init
 cudaError_t init_homogeneous_dev(uint32_t* d, int lx, int ly, int encoding, cudaStream_t st);
 cudaError_t local_to_cbbit_dev(const uint32_t* local, uint32_t* cbbit, int lx, int ly, cudaStream_t st);

@@ -31,7 +31,7 @@ std::string plan_key(int lx, int ly, uint64_t Tp, uint64_t Tq, int sm_count)
     const int planes = a.planes > b.planes ? a.planes : b.planes;
     const int pclass = planes == 0 ? 0 : planes == 1 ? 1 : planes <= 4 ? 2 : 3;
     char buf[96];
-    snprintf(buf, sizeof buf, "scabit3:%d:%d:rng%d:sm%d", lx, ly, pclass, sm_count);
+    snprintf(buf, sizeof buf, "scabit4:%d:%d:rng%d:sm%d", lx, ly, pclass, sm_count);
     return buf;
 }
 
@@ -44,10 +44,10 @@ void load_file()
     FILE* f = fopen(path, "r");
     if (!f) return;
     char key[96];
-    int kind, k, cps;
+    int kind, k, cps, band;
     float ms;
-    while (fscanf(f, "%95s %d %d %d %f", key, &kind, &k, &cps, &ms) == 5)
-        g_plans[key] = Plan{k, cps, ms, true, kind};
+    while (fscanf(f, "%95s %d %d %d %f %d", key, &kind, &k, &cps, &ms, &band) == 6)
+        g_plans[key] = Plan{k, cps, ms, true, kind, band};
     fclose(f);
 }
 
@@ -58,8 +58,8 @@ void save_file()
     FILE* f = fopen(path, "w");
     if (!f) return;
     for (const auto& kv : g_plans)
-        fprintf(f, "%s %d %d %d %.6f\n", kv.first.c_str(), kv.second.kind, kv.second.k, kv.second.cps,
-                kv.second.ms_per_mcs);
+        fprintf(f, "%s %d %d %d %.6f %d\n", kv.first.c_str(), kv.second.kind, kv.second.k, kv.second.cps,
+                kv.second.ms_per_mcs, kv.second.band);
     fclose(f);
 }
 }  // namespace
@@ -94,6 +94,12 @@ Plan explicit_plan(int lx, int ly, int k, int sm_count)
     // "band1" .. "band3": the band kernel with that CTAs-per-SM choice (the tuner's candidates)
     if (v.size() == 5 && v.compare(0, 4, "band") == 0 && v[4] >= '1' && v[4] <= '3')
         return Plan{k, v[4] - '0', 0.f, false, PASS_BAND};
+    if (v.compare(0, 5, "strip") == 0) {
+        const int band = v.size() > 5 ? atoi(v.c_str() + 5) : 64;
+        Plan p{k, 0, 0.f, false, PASS_STRIP, band};
+        if (scabit_strip_shape(lx, ly, k, band, DEC_NONE).ok) return p;
+        return Plan{k, 0, 0.f, false, PASS_BAND};
+    }
     if (v.compare(0, 4, "wave") == 0) {
         const int cps = v.size() > 4 ? v[4] - '0' : 2;
         if (scabit_wave_shape(lx, ly, k, sm_count, cps, DEC_NONE).ok) return Plan{k, cps, 0.f, false, PASS_WAVE};
@@ -109,6 +115,7 @@ bool plan_shape_ok(const Plan& p, int lx, int ly, int sm_count)
     if (p.k <= 1) return true;
     if (p.kind == PASS_STREAM) return scabit_stream_shape(lx, ly, p.k, sm_count, p.cps ? p.cps : 1).ok;
     if (p.kind == PASS_WAVE) return scabit_wave_shape(lx, ly, p.k, sm_count, p.cps, DEC_NONE).ok;
+    if (p.kind == PASS_STRIP) return scabit_strip_shape(lx, ly, p.k, p.band, DEC_NONE).ok;
     return scabit_fused_shape_cps(lx, ly, p.k, p.cps, 0).ok;
 }
 
@@ -130,18 +137,33 @@ cudaError_t tune_plan(uint32_t* d_src, int lx, int ly, uint64_t seed, uint32_t s
     cudaEventCreate(&e1);
 
     struct Cand {
-        int k, cps, kind;
+        int k, cps, kind, band;
     };
     const int mode = dec_mode(make_thresh(Tp), make_thresh(Tq));
-    std::vector<Cand> cands{{1, 0, PASS_BAND}};
+    std::vector<Cand> cands{{1, 0, PASS_BAND, 0}};
     for (int k = 2; k <= 8; ++k)
         for (int cps = 1; cps <= 3; ++cps) {
             FusedShape f = scabit_fused_shape_cps(lx, ly, k, cps, 0);
-            if (f.ok && f.band >= 2) cands.push_back({k, cps, PASS_BAND});
-            if (cps <= 2 && scabit_stream_shape(lx, ly, k, sm_count, cps).ok) cands.push_back({k, cps, PASS_STREAM});
-            if (scabit_wave_shape(lx, ly, k, sm_count, cps, mode).ok) cands.push_back({k, cps, PASS_WAVE});
+            if (f.ok && f.band >= 2) cands.push_back({k, cps, PASS_BAND, 0});
+            if (cps <= 2 && scabit_stream_shape(lx, ly, k, sm_count, cps).ok)
+                cands.push_back({k, cps, PASS_STREAM, 0});
+            if (scabit_wave_shape(lx, ly, k, sm_count, cps, mode).ok) cands.push_back({k, cps, PASS_WAVE, 0});
         }
-    Plan best{1, 0, 1e30f, true, PASS_BAND};
+    // the warp-tile kernel: depth x tile height (taller tiles recompute fewer halo rows, shorter
+    // ones make more warps), heights that fill whole tick cycles; heights that leave the same
+    // tiles as a shorter one are skipped
+    for (int k = 4; k <= 8; k += 2) {
+        int last_tiles = -1;
+        for (int m = 2; m <= 12; ++m) {
+            const int band = m * strip_cycle_rows(k) - 4 * k;
+            if (band < 8) continue;
+            const StripShape ps = scabit_strip_shape(lx, ly, k, band, mode);
+            if (!ps.ok || ps.ntiles == last_tiles) continue;
+            last_tiles = ps.ntiles;
+            cands.push_back({k, 0, PASS_STRIP, band});
+        }
+    }
+    Plan best{1, 0, 1e30f, true, PASS_BAND, 0};
     const ScabitShape hs = scabit_shape(lx, ly, sm_count);
     for (const Cand& c : cands) {
         // enough MCS per measurement to dwarf launch overhead, capped by lattice size
@@ -159,9 +181,12 @@ cudaError_t tune_plan(uint32_t* d_src, int lx, int ly, uint64_t seed, uint32_t s
             const FusedShape f = scabit_fused_shape_cps(lx, ly, c.k, c.cps, 0);
             const StreamShape ss = scabit_stream_shape(lx, ly, c.k, sm_count, c.cps);
             const WaveShape ws = scabit_wave_shape(lx, ly, c.k, sm_count, c.cps, mode);
+            const StripShape ps = scabit_strip_shape(lx, ly, c.k, c.band, mode);
             uint32_t *s = a, *d = b;
             for (int m = 0; m + c.k <= mcs; m += c.k) {
-                cudaError_t r = c.kind == PASS_STREAM
+                cudaError_t r = c.kind == PASS_STRIP
+                                    ? scabit_strip(s, d, lx, ly, (uint32_t)m, seed, stream_id, Tp, Tq, ps, nullptr, st)
+                                : c.kind == PASS_STREAM
                                     ? scabit_stream(s, d, lx, ly, (uint32_t)m, seed, stream_id, Tp, Tq, ss,
                                                     nullptr, d_err, st)
                                 : c.kind == PASS_WAVE
@@ -184,10 +209,13 @@ cudaError_t tune_plan(uint32_t* d_src, int lx, int ly, uint64_t seed, uint32_t s
         cudaEventElapsedTime(&ms, e0, e1);
         const float per = ms / (float)mcs;
         if (getenv("KPZB_TUNE_VERBOSE"))
-            fprintf(stderr, "kpzb tune lx=%d ly=%d %s k=%d cps=%d: %.4f ms/MCS, %.1f upd/ns\n", lx, ly,
-                    c.kind == PASS_STREAM ? "stream" : c.kind == PASS_WAVE ? "wave" : "band", c.k, c.cps, per,
-                    (double)(1ull << (lx + ly)) / (per * 1e6));
-        if (per < best.ms_per_mcs) best = Plan{c.k, c.cps, per, true, c.kind};
+            fprintf(stderr, "kpzb tune lx=%d ly=%d %s k=%d cps=%d band=%d: %.4f ms/MCS, %.1f upd/ns\n", lx, ly,
+                    c.kind == PASS_STREAM  ? "stream"
+                    : c.kind == PASS_WAVE  ? "wave"
+                    : c.kind == PASS_STRIP ? "strip"
+                                           : "band",
+                    c.k, c.cps, c.band, per, (double)(1ull << (lx + ly)) / (per * 1e6));
+        if (per < best.ms_per_mcs) best = Plan{c.k, c.cps, per, true, c.kind, c.band};
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);

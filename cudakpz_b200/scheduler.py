@@ -160,10 +160,11 @@ class Scheduler:
 
     def plan(self):
         """(mcs_per_pass, ctas_per_sm, pass_kernel) used for the current rates; pass_kernel is
-        "half-steps", "band", "stream" or "wave" (kpzb_get_plan)."""
+        "half-steps", "band", "stream", "wave" or "strip" (kpzb_get_plan; for "strip" the middle
+        entry is the output rows of a tile)."""
         k, c, kind = C.c_int(), C.c_int(), C.c_int()
         check(lib.kpzb_get_plan(self._h, C.byref(k), C.byref(c), C.byref(kind)), "kpzb_get_plan")
-        return int(k.value), int(c.value), ("half-steps", "band", "stream", "wave")[kind.value]
+        return int(k.value), int(c.value), ("half-steps", "band", "stream", "wave", "strip")[kind.value]
 
     def saveBit(self, path: str, meta: Optional[str] = None) -> None:
         """SchedulerService::saveBit's file (kpz/schedulerService.cpp:389-401) plus the resume

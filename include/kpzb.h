@@ -139,10 +139,11 @@ kpzb_status kpzb_set_fusion(kpzb_handle* h, int mcs_per_pass);
 kpzb_status kpzb_get_fusion(kpzb_handle* h, int* mcs_per_pass);
 /* The full pass plan for the current rates: MCS per pass, CTAs per SM and the pass kernel
  * (KPZB_PASS_HALF_STEPS: one launch per half-step; KPZB_PASS_BAND: band kernel;
- * KPZB_PASS_STREAM: streaming wavefront kernel; KPZB_PASS_WAVE: register-wavefront kernel).
- * No counterpart in the reference (introspection of the measured choice, e.g. for launch
- * accounting). */
-enum { KPZB_PASS_HALF_STEPS = 0, KPZB_PASS_BAND = 1, KPZB_PASS_STREAM = 2, KPZB_PASS_WAVE = 3 };
+ * KPZB_PASS_STREAM: streaming wavefront kernel; KPZB_PASS_WAVE: register-wavefront kernel;
+ * KPZB_PASS_STRIP: warp-tile register-wavefront kernel, for which ctas_per_sm reports the
+ * output rows of a tile).  No counterpart in the reference (introspection of the measured
+ * choice, e.g. for launch accounting). */
+enum { KPZB_PASS_HALF_STEPS = 0, KPZB_PASS_BAND = 1, KPZB_PASS_STREAM = 2, KPZB_PASS_WAVE = 3, KPZB_PASS_STRIP = 4 };
 kpzb_status kpzb_get_plan(kpzb_handle* h, int* mcs_per_pass, int* ctas_per_sm, int* pass_kernel);
 /* Time every pass shape (MCS per pass x CTAs per SM) on scratch copies of the current
  * lattice and cache the fastest for this size and rate class (in memory, and in the file

@@ -322,3 +322,43 @@ def test_untuned_default_plan(kpzb, oracle, monkeypatch, p, q, kind):
     got = s.popSystem()
     s.close()
     assert first_diff(got, ref) is None, first_diff(got, ref)
+
+
+@pytest.mark.parametrize("lx,ly,k,band,p,q", [
+    (11, 7, 4, 16, 1.0, 0.0),    # a 32-word row: one periodic strip, shuffles wrap the warp
+    (11, 5, 6, 64, 0.5, 0.5),    # fewer rows than a tile: the halo wraps the lattice
+    (12, 8, 4, 2, 0.5, 0.5),     # two-row tiles: nearly every row is halo
+    (12, 6, 8, 16, 1.0, 1.0),    # the deepest pass; every candidate flips
+    (13, 7, 6, 24, 0.5, 0.0),    # one random plane, no maxima
+    (13, 5, 4, 32, 0.0, 1.0),    # only maxima
+    (13, 6, 4, 16, 0.0, 0.5),
+    (14, 6, 6, 32, 1.0, 0.0),    # the headline width: nine strips, the last one partly wrapped
+    (14, 5, 4, 16, 0.5, 0.5),    # ten strips of 28 columns
+    (14, 6, 6, 64, 1.0, 0.5),    # always deposit, desorb on the MSB plane
+    (14, 5, 4, 16, 0.5, 1.0),
+    (15, 4, 8, 8, 1.0, 0.0),     # 512-word rows
+    (14, 4, 4, 16, 0.0, 0.0),    # nothing flips: the pass copies
+    (13, 4, 4, 16, 0.9, 0.1),    # generic rates: the strip kernel does not cover them, band fallback
+])
+def test_strip_kernel_bit_exact(kpzb, oracle, monkeypatch, lx, ly, k, band, p, q):
+    """The warp-tile pass kernel (scabit_strip_kernel), word for word with counters: one or
+    many strips per row, strips of 30 or 28 columns, tiles of 2 to 64 rows, halos that wrap."""
+    monkeypatch.setenv("KPZB_PASS_KERNEL", f"strip{band}")
+    n = 2 * k + 1
+    init = oracle.random_lattice(lx, ly, oracle.ENC_CBBIT, seed=19, mcs=2)
+    ref = init.copy()
+    rc = oracle.sca_mcs_words(ref, lx, ly, 11, 5, 0, n, p, q)
+    s = kpzb.Scheduler(lx, ly)
+    s.pushSystem(init)
+    s.setPQ(p, q)
+    s.supplySeed(11, 5)
+    s.setFusion(k)
+    s.enableCounters(True)
+    s.mcsPQSyncRng(n)
+    got = s.popSystem()
+    cnt = s.counters()
+    plan = s.plan()
+    s.close()
+    assert plan[2] == ("band" if (p, q) == (0.9, 0.1) else "strip"), plan
+    assert first_diff(got, ref) is None, first_diff(got, ref)
+    assert cnt == rc

@@ -46,6 +46,10 @@ def oracle_run(oracle, p, q, n):
 HEADLINE_PLANS = [
     (1.0, 0.0, "wave2", 6, 13, ("wave", 2)),   # 2 passes + 1 MCS of half-step launches
     (0.5, 0.5, "band1", 4, 9, ("band", 1)),    # 2 passes + 1 MCS
+    (1.0, 0.0, "strip64", 6, 13, ("strip", 64)),
+    (1.0, 0.0, "strip128", 8, 17, ("strip", 128)),
+    (0.5, 0.5, "strip64", 4, 9, ("strip", 64)),
+    (0.5, 0.5, "strip32", 6, 13, ("strip", 32)),
 ]
 
 

@@ -36,12 +36,14 @@ METRIC = "site updates/ns (SCA, DT, batched) vs plain loop; exact correlator TOP
 UNIT = "attempted site updates/ns"
 
 # Per-launch DRAM traffic (dram__bytes_read.sum + dram__bytes_write.sum) of the pass kernels
-# at 16384^2, from one ncu capture per (p, q, pass kernel, MCS per pass); the commands and the
-# full figures are in profiles/scabit_fused_16384.md and profiles/scabit_wave_16384.md.
+# at 16384^2, from one ncu capture per (p, q, pass kernel, MCS per pass, CTAs per SM or tile
+# rows): the first pass after an L2 flush, so an upper bound for passes that follow one another
 DT_NCU_BYTES_32768 = 103.849e6 + 36.303e6
-NCU_TRAFFIC_PER_LAUNCH = {(1.0, 0.0, "band", 7): 67.324e6 + 23.171e6,
-                          (0.5, 0.5, "band", 4): 67.218e6 + 17.975e6,
-                          (1.0, 0.0, "wave", 6): 89.707e6 + 19.618e6}
+NCU_TRAFFIC_PER_LAUNCH = {(1.0, 0.0, "band", 7, 0): 67.324e6 + 23.171e6,
+                          (0.5, 0.5, "band", 4, 1): 67.218e6 + 17.975e6,
+                          (1.0, 0.0, "wave", 6, 2): 89.707e6 + 19.618e6,
+                          (1.0, 0.0, "strip", 8, 128): 85.564e6 + 22.054e6,
+                          (0.5, 0.5, "strip", 4, 56): 71.193e6 + 19.824e6}
 
 
 def parse():
@@ -63,13 +65,20 @@ def parse():
     ap.add_argument("--reference-gpu", action="store_true",
                     help="with --impl reference: time the reference's own CUDA scheduler on this GPU "
                          "(oracle/_ref/kpz_ref_gpu) instead of its CPU scheduler")
+    ap.add_argument("--dry-run", action="store_true",
+                    help="launcher check: form the process group (gloo, CPU), barrier, max over ranks, print")
+    ap.add_argument("--no-configs", action="store_true",
+                    help="skip the configs / reference_gpu blocks measured after the headline")
     ap.add_argument("--workload", choices=["scabit", "dt", "db4", "batch", "gram", "measure"], default="scabit",
                     help="scabit: the headline 16384^2 SCA runs; dt / batch / gram: the other configs; "
                          "db4: the C3 lattice under the DB4 scheduler")
     return ap.parse_args()
 
 
-def dist_setup(n):
+def dist_setup(args):
+    """One process per GPU: RANK / LOCAL_RANK / WORLD_SIZE / MASTER_* from the environment
+    (torchrun, or spawn_ranks below).  NCCL carries only the barriers and the max-over-ranks of
+    the timings (the replicas exchange nothing); --dry-run uses gloo on the CPU."""
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -77,8 +86,31 @@ def dist_setup(n):
         import datetime
 
         import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        dist.init_process_group("gloo" if args.dry_run else "nccl", timeout=datetime.timedelta(seconds=120))
     return world, rank, local
+
+
+def spawn_ranks(args):
+    """--gpus N without torchrun: start N rank processes of this script on this host, one per
+    GPU (LOCAL_RANK = i), rendezvous on 127.0.0.1, and return the worst exit code.  Refuses
+    N larger than the number of visible GPUs (except for --dry-run, which runs on the CPU)."""
+    import socket
+    if not args.dry_run:
+        import torch
+        nvis = torch.cuda.device_count()
+        if args.gpus > nvis:
+            print(json.dumps({"error": f"--gpus {args.gpus} but {nvis} GPU(s) visible"}), flush=True)
+            return 2
+    with socket.socket() as sk:
+        sk.bind(("127.0.0.1", 0))
+        port = sk.getsockname()[1]
+    procs = []
+    for r in range(args.gpus):
+        env = dict(os.environ, RANK=str(r), LOCAL_RANK=str(r), WORLD_SIZE=str(args.gpus),
+                   LOCAL_WORLD_SIZE=str(args.gpus), MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+        procs.append(subprocess.Popen([sys.executable, str(Path(__file__).resolve()), *sys.argv[1:]], env=env))
+    rcs = [pr.wait() for pr in procs]
+    return max(rcs)
 
 
 def barrier(world):
@@ -87,14 +119,25 @@ def barrier(world):
         dist.barrier()
 
 
-def max_over_ranks(x, world):
+def max_over_ranks(x, world, device="cuda"):
     if world == 1:
         return x
     import torch
     import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    t = torch.tensor([x], dtype=torch.float64, device=device)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def run_dry(args, world, rank):
+    """--dry-run: the launcher and rank plumbing without GPU work -- every rank joins the
+    group, passes a barrier and contributes its rank to a max-over-ranks (gloo, CPU)."""
+    barrier(world)
+    top = max_over_ranks(float(rank), world, device="cpu")
+    if rank != 0:
+        return None
+    return {"metric": METRIC, "dry_run": True, "impl": args.impl, "n_gpus": world, "max_rank": int(top),
+            "scaling": "weak", "config": {"parallelism": f"replicas x{world}"}}
 
 
 class ClockSampler:
@@ -255,40 +298,52 @@ def run_ours(args, world, rank, local):
     kernel_names = {"stream": "scabit_stream_kernel", "band": "scabit_fused_kernel", "wave": "scabit_wave_kernel",
                     "strip": "scabit_strip_kernel"}
     dominant = "+".join(kernel_names[k] for k in kinds) if kinds else "scabit_half_kernel"
-    # algorithmic bytes: 1 B per attempted update over the whole timed region, divided by the
-    # device time of the launches (fused passes carry more than 95 % of it)
+    # HBM: algorithmic bytes, 1 B per attempted update, over the device time of the launches
+    # (fused passes carry more than 95 % of it); with temporal blocking this exceeds the copy
+    # peak -- reported as the fusion gain, not as a roofline fraction
     per_launch_ms = sum(per_lat) / (args.steps * launches_per_step)
     bytes_per_launch = float(N) * M * len(scheds) / launches_per_step
     peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (
         ROOT / "MEASURED_PEAKS.json").exists() else {}
     peak = peaks.get("hbm_gbs", 6650.0)
     achieved = bytes_per_launch / (per_launch_ms * 1e-3) / 1e9
-    roofline = {"bound": "hbm", "kernel": dominant, "achieved": round(achieved, 1),
-                "peak": peak, "peak_source": "measured" if "hbm_gbs" in peaks else "fallback",
-                "unit": "GB/s", "frac": round(achieved / peak, 4),
-                "traffic": fused_traffic(pqs, plans, M, LX), "algorithmic_bytes_per_launch": bytes_per_launch,
-                "launch_ms": round(per_launch_ms, 4), "mcs_per_pass": ks,
-                "plans": [{"mcs_per_pass": a, "ctas_per_sm": b, "kernel": c} for a, b, c in plans]}
+    hbm = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak,
+           "peak_source": "measured (MEASURED_PEAKS.json hbm_gbs)" if "hbm_gbs" in peaks else "fallback",
+           "unit": "GB/s", "frac": round(achieved / peak, 4),
+           "algorithmic_bytes_per_launch": bytes_per_launch, "launch_ms": round(per_launch_ms, 4)}
 
-    # INT roofline: the bitwise update's algorithmic ALU operations against the measured
-    # LOP3 throughput of this GPU (probe kernel, a few ms, after the timed region)
+    # INT roofline, the binding one: the bitwise update's algorithmic ALU operations against the
+    # LOP3 throughput of this GPU measured live (probe kernel, a few ms, after the timed region)
     lop3, iadd3 = kpzb.probe_alu_peak(local)
     opw = [alu_ops_per_word(p, q) for (p, q) in pqs]
-    int_roofline = None
+    traffic = fused_traffic(pqs, plans, M, LX)
+    roofline = {"bound": "int-alu", "kernel": dominant, "achieved": None, "peak": round(lop3 / 1e12, 3),
+                "unit": "Tops/s (algorithmic integer ops)", "frac": None, "traffic": traffic,
+                "traffic_note": "dram bytes per pass launch from an ncu capture of the same plan (first pass "
+                                "after an L2 flush), launch-weighted" if traffic else "no capture of this plan",
+                "peak_source": "measured live (kpzb_probe_alu_peak, 3-input LOP3 chains); of measured",
+                "iadd3_peak": round(iadd3 / 1e12, 3), "mcs_per_pass": ks,
+                "plans": [{"mcs_per_pass": a, "ctas_per_sm_or_tile_rows": b, "kernel": c} for a, b, c in plans],
+                "hbm": hbm, "fusion_gain": hbm["frac"]}
     if None not in opw:
         ops_step = sum(float(N) * M * o / 32.0 for o in opw)
         int_ach = ops_step * args.steps / (sum(per_lat) * 1e-3)
         upd_per_op = float(N) * M * len(scheds) / ops_step  # attempts per algorithmic ALU op
         int_roof_upd = lop3 * upd_per_op / 1e9
         hbm_roof_upd = peak  # 1 B per attempt: GB/s == attempts/ns
-        int_roofline = {"bound": "int-alu", "achieved": round(int_ach / 1e12, 3),
-                        "peak": round(lop3 / 1e12, 3), "unit": "Tops/s", "frac": round(int_ach / lop3, 4),
-                        "peak_source": "measured live (kpzb_probe_alu_peak, 3-input LOP3 chains)",
-                        "iadd3_peak": round(iadd3 / 1e12, 3),
-                        "alu_ops_per_word": {f"{p},{q}": o for (p, q), o in zip(pqs, opw)},
-                        "roofline_upd_per_ns": round(int_roof_upd, 1)}
+        roofline.update({"achieved": round(int_ach / 1e12, 3), "frac": round(int_ach / lop3, 4),
+                         "alu_ops_per_word": {f"{p},{q}": o for (p, q), o in zip(pqs, opw)},
+                         "roofline_upd_per_ns": round(int_roof_upd, 1),
+                         "per_lattice_frac": {f"{p},{q}": round(float(N) * M * args.steps * o / 32.0
+                                                                 / (t * 1e-3) / lop3, 4)
+                                              for (p, q), o, t in zip(pqs, opw, per_lat)}})
+        # the slower of the two rooflines bounds the update rate; with temporal blocking the HBM
+        # one (1 B per attempt) is the faster, so the binding fraction is the INT one
         roofline["slower_roofline"] = "hbm" if hbm_roof_upd <= int_roof_upd else "int-alu"
         roofline["frac_of_slower_roofline"] = round(value / min(hbm_roof_upd, int_roof_upd), 4)
+        if achieved > peak:
+            roofline["frac_of_slower_roofline"] = roofline["frac"]
+            roofline["slower_roofline"] = "int-alu (HBM exceeded by temporal blocking: see fusion_gain)"
 
     e2e = None
     if not args.no_e2e:
@@ -299,7 +354,6 @@ def run_ours(args, world, rank, local):
     per_lattice = [{"p": p, "q": q, "mcs_per_pass": kk, "kernel": pl[2],
                     "upd_per_ns": round(float(N) * M * args.steps / (t * 1e6), 1)}
                    for (p, q), kk, pl, t in zip(pqs, ks, plans, per_lat)]
-    roofline["int_roofline"] = int_roofline
     return value, ms, wall, clk, roofline, e2e, launches_per_step * args.steps, ks, per_lattice
 
 
@@ -309,8 +363,8 @@ def fused_traffic(pqs, plans, M, lx):
     if lx != 14:
         return None
     tot, n = 0.0, 0
-    for (p, q), (k, _, kind) in zip(pqs, plans):
-        t = NCU_TRAFFIC_PER_LAUNCH.get((p, q, kind, k))
+    for (p, q), (k, c, kind) in zip(pqs, plans):
+        t = NCU_TRAFFIC_PER_LAUNCH.get((p, q, kind, k, c))
         if t is None or k < 2:
             return None
         tot += t * (M // k)
@@ -369,6 +423,15 @@ def run_e2e(args, torch, kpzb, scheds, N, M, world):
     streams = [torch.cuda.Stream() for _ in scheds]
     for s, st in zip(scheds, streams):
         s.setStream(st.cuda_stream)
+    # one untimed pass through the whole pipeline, so that one-time work (the stage buffer and
+    # copy stream of the first asynchronous push, first launches of the analysis kernels) stays
+    # out of the timed region
+    for h, o, s in zip(host, outs, scheds):
+        s.pushSystemAsync(h.numpy().view(np.uint32))
+        s.mcsPQSyncRngAsync(M)
+        s.popSystemAsync(o.numpy().view(np.uint32))
+        s.roughnessAsync()
+        s.joinRoughness()
     torch.cuda.synchronize()
     barrier(world)
     t0 = time.perf_counter()
@@ -410,7 +473,7 @@ def run_e2e(args, torch, kpzb, scheds, N, M, world):
 
 REF_BIN = ROOT / "oracle" / "_ref" / "kpz_ref"
 REF_LX = 14  # CPU sample on the benchmark lattice itself (16384^2)
-REF_MCS = 2  # MCS per (p,q) per sample: a few seconds of CPU work on 8 cores
+REF_MCS = 12  # MCS per (p,q) per sample: about 10 s of CPU work on 16 cores
 
 
 def ref_sample(threads):
@@ -510,7 +573,7 @@ def run_reference(args, world, rank):
     cores = os.cpu_count() or 1
     rs = args.workload in ("dt", "db4") and REF_BIN.exists()
     sample = (lambda: dtr_sample(cores)) if rs else (lambda: cpu_baseline_sample(cores))
-    for _ in range(args.warmup):
+    for _ in range(min(args.warmup, 1)):  # a CPU sample needs no more than one warm-up
         sample()
     vals = []
     t0 = time.perf_counter()
@@ -522,13 +585,14 @@ def run_reference(args, world, rank):
     value = statistics.median(vals)
     last["value"] = round(value, 6)
     return {"metric": METRIC, "value": round(value, 6), "unit": UNIT, "impl": "reference",
-            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": round(wall * 1e3 / args.steps, 3), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
             "config": {"workload": ("random-sequential double tiling (SchedulerCPUDTr), p=0.95 q=0.05; each CPU "
-                                    "step 2 MCS on the 16384^2 lattice") if rs else
+                                    f"step {REF_MCS} MCS on the 16384^2 lattice") if rs else
                                    ("SCABit 16384^2 periodic, flat start, (p,q)=(1,0) and (0.5,0.5); "
-                                    "each CPU step 2 MCS per (p,q) on the 16384^2 lattice")},
+                                    f"each CPU step {REF_MCS} MCS per (p,q) on the 16384^2 lattice"),
+                       "value": "median over the steps"},
             "cpu_baseline": last,
             "e2e": {"value": round(value, 6), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
@@ -728,6 +792,20 @@ def run_batch(args, world, rank, local):
         s.join()
     dt_plain = time.perf_counter() - t0
     plain = sites * m / (dt_plain * 1e9)
+    # the same loop with each lattice at its tuned pass plan (temporal blocking per lattice)
+    for s in hs:
+        s.setFusion(0)
+    for s in hs:
+        s.mcsPQSyncRngAsync(8)  # resolves (and tunes, once per size and rate class) the plans
+    for s in hs:
+        s.join()
+    t0 = time.perf_counter()
+    for s in hs:
+        s.mcsPQSyncRngAsync(m)
+    for s in hs:
+        s.join()
+    dt_tuned = time.perf_counter() - t0
+    tuned = sites * m / (dt_tuned * 1e9)
     # identical per-replica lattices: compare a sample of replicas after equal MCS
     same = True
     for i in (0, 300, 400, 500):
@@ -744,6 +822,7 @@ def run_batch(args, world, rank, local):
                  {"workload": "512 SCABit replicas (256x256^2,128x1024^2,64x2048^2,64x4096^2), mixed (p,q)",
                   "mcs_per_step": m, "parallelism": f"replicas x{world}"},
                  plain_loop_value=round(plain, 3), speedup_vs_plain_loop=round(value / plain, 2),
+                 tuned_loop_value=round(tuned, 3), speedup_vs_tuned_loop=round(value / tuned, 2),
                  replicas_bit_identical_to_single_runs=same, clocks=clk,
                  timing="host wall clock around synchronous batch calls",
                  cpu_baseline=batch_cpu_sample(os.cpu_count() or 1) if (rank == 0 and world == 1 and not args.no_cpu)
@@ -862,9 +941,82 @@ def run_gram(args, world, rank, local):
                  else None)
 
 
+def run_configs(args, local):
+    """The other configurations and the reference's own CUDA schedulers, measured after the
+    headline in the same run (rank 0, one GPU): C3 (DT and the reference's default DBSH scheme
+    on 65536^2, the reference's builds of the same schemes on 16384^2), C4 (512 batched
+    replicas against the per-lattice loops), C5 (the exact 64x64 Gram against int64), and the
+    reference's SchedulerSCABit<SLCG64> on the headline lattices.  A part that fails reports
+    its error instead of a number."""
+    import copy
+
+    def sub(**kw):
+        a = copy.copy(args)
+        a.no_cpu, a.no_e2e = True, True
+        for k, v in kw.items():
+            setattr(a, k, v)
+        return a
+
+    def guard(fn):
+        try:
+            return fn()
+        except Exception as e:  # reported in the line, never fatal to the headline
+            return {"error": f"{type(e).__name__}: {e}"[:300]}
+
+    t0 = time.perf_counter()
+    out = {}
+    out["reference_gpu"] = guard(lambda: {
+        k: v for k, v in run_reference_gpu(sub(impl="reference", reference_gpu=True, workload="scabit", lx=14,
+                                               steps=1, warmup=2, mcs_per_step=20), 1, 0, local).items()
+        if k in ("value", "unit", "per_lattice", "timing", "clocks", "config", "unavailable")})
+
+    def c3():
+        res = {"ours_65536": {}, "reference_gpu_16384": {}, "ours_16384": {}}
+        for inner in ("dt", "dbsh"):
+            for lx, key in ((16, "ours_65536"), (14, "ours_16384")):
+                ln = run_dt(sub(workload="dt", dt_inner=inner, lx=lx, steps=4, warmup=3, mcs_per_step=100), 1, 0,
+                            local)
+                res[key][inner] = {"upd_per_ns": ln["value"], "int_alu_frac": ln["roofline"]["frac"]}
+            r = run_reference_gpu(sub(impl="reference", reference_gpu=True, workload="dt", dt_inner=inner, lx=14,
+                                      steps=4, warmup=3, mcs_per_step=100), 1, 0, local)
+            res["reference_gpu_16384"][inner] = r.get("value", r.get("unavailable"))
+        for inner in ("dt", "dbsh"):
+            ref = res["reference_gpu_16384"][inner]
+            if isinstance(ref, (int, float)) and ref > 0:
+                res[f"ratio_{inner}_16384"] = round(res["ours_16384"][inner]["upd_per_ns"] / ref, 2)
+        res["workload"] = "DT random-sequential, p=0.95 q=0.05, flat start; dbsh = the reference's default scheme"
+        return res
+    out["C3"] = guard(c3)
+
+    def c4():
+        ln = run_batch(sub(workload="batch", steps=2, warmup=1), 1, 0, local)
+        return {k: ln[k] for k in ("value", "unit", "plain_loop_value", "speedup_vs_plain_loop",
+                                   "tuned_loop_value", "speedup_vs_tuned_loop",
+                                   "replicas_bit_identical_to_single_runs", "config") if k in ln}
+    out["C4"] = guard(c4)
+
+    def c5():
+        ln = run_gram(sub(workload="gram", steps=3, warmup=1), 1, 0, local)
+        return {k: ln[k] for k in ("value", "unit", "speedup_vs_int64", "exact_match_int64", "int64_cuda_core_s",
+                                   "ms_per_step", "roofline", "config") if k in ln}
+    out["C5"] = guard(c5)
+    out["seconds"] = round(time.perf_counter() - t0, 1)
+    return out
+
+
 def main():
     args = parse()
-    world, rank, local = dist_setup(args.gpus)
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        sys.exit(spawn_ranks(args))
+    world, rank, local = dist_setup(args)
+    if args.dry_run:
+        line = run_dry(args, world, rank)
+        if line is not None:
+            print(json.dumps(line), flush=True)
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+        return
     if args.workload != "scabit" and args.impl == "ours":
         fn = {"dt": run_dt, "db4": run_dt, "batch": run_batch, "gram": run_gram,
               "measure": run_measure}[args.workload]
@@ -909,6 +1061,10 @@ def main():
                 "per_lattice": per_lattice, "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
                 "clocks": clk,
                 "gpu_launches": launches, "wall_s": round(wall, 3)}
+        if world == 1 and not args.no_configs:
+            extra = run_configs(args, local)
+            line["reference_gpu"] = extra.pop("reference_gpu")
+            line["configs"] = extra
         print(json.dumps(line), flush=True)
     if world > 1:
         import torch.distributed as dist

@@ -84,7 +84,8 @@ scabit_strip_kernel(const uint32_t* __restrict__ src, uint32_t* __restrict__ dst
     constexpr bool RND = PM == 2 || QM == 2;
     constexpr int STRIDE = strip_stride(RND);
     __shared__ __align__(16) uint32_t ring_s[STRIP_WARPS][S][4][32];
-    __shared__ __align__(16) uint32_t rnd_s[STRIP_WARPS][8 * STRIP_QUAD_STRIDE];
+    constexpr int NG = RND ? NH / 4 : 1;  // Philox calls per lane per tick
+    __shared__ __align__(16) uint32_t rnd_s[STRIP_WARPS][NG][8 * STRIP_QUAD_STRIDE];
 
     const int lane = (int)threadIdx.x & 31, wid = (int)threadIdx.x >> 5;
     const int tile = (int)blockIdx.x * STRIP_WARPS + wid;
@@ -108,7 +109,39 @@ scabit_strip_kernel(const uint32_t* __restrict__ src, uint32_t* __restrict__ dst
     const uint32_t* s0 = src + wcol;
     uint32_t* d0 = dst + wcol;
     const int lgG = lx - 8;  // log2 of 4-word groups per quadrant row
-    uint32_t* rs = rnd_s[wid] + (lane >> 2) * STRIP_QUAD_STRIDE;
+    uint32_t* rs = &rnd_s[wid][0][0] + (lane >> 2) * STRIP_QUAD_STRIDE;
+
+    // random words (RND), one tick ahead: at tick tau the lanes compute tick tau + 1's Philox
+    // calls -- lane j of each quad the call of half-step 4g + j for the quad's 4-word group --
+    // while tick tau's updates run, and exchange them through shared memory at its end
+    uint32_t rwc[RND ? NH : 1];  // this tick's word of every half-step
+    uint4 cn[NG];                // the next tick's calls
+    // counter word 0 of half-step hj's call: quadrant row (ylo + tau - hj) mod rows times the
+    // groups per row, plus this lane's group (one multiply-add and one mask per call)
+    const uint32_t gpr = 1u << lgG, lane_grp = wcol >> 2;
+    auto calls = [&](int tau_) {
+#pragma unroll
+        for (int g = 0; g < NG; ++g) {
+            const int hj = 4 * g + (lane & 3);
+            const uint32_t gy = (ylo - (uint32_t)hj + (uint32_t)tau_) & rmask;
+            cn[g] = philox4x32_10(make_uint4(gy * gpr + lane_grp, 2u * t0 + (uint32_t)hj, TAG_SCA << 8, stream), key);
+        }
+    };
+    auto exchange = [&]() {
+        __syncwarp();
+#pragma unroll
+        for (int g = 0; g < NG; ++g)
+            *reinterpret_cast<uint4*>(rs + g * 8 * STRIP_QUAD_STRIDE + (lane & 3) * 4) = cn[g];
+        __syncwarp();
+#pragma unroll
+        for (int g = 0; g < NG; ++g)
+#pragma unroll
+            for (int u = 0; u < 4; ++u) rwc[4 * g + u] = rs[g * 8 * STRIP_QUAD_STRIDE + u * 4 + (lane & 3)];
+    };
+    if (RND) {
+        calls(0);
+        exchange();
+    }
     uint32_t(*ring)[4][32] = ring_s[wid];
 
     // local row rho -> ring slot rho % S: this lane's four quadrant words, one copy group per row
@@ -147,23 +180,9 @@ scabit_strip_kernel(const uint32_t* __restrict__ src, uint32_t* __restrict__ dst
 #pragma unroll
                 for (int q = 0; q < 4; ++q) win[q][(i + 1) % NW] = ring[sl][q][lane];
             }
-            uint32_t rw[4];  // random words of half-steps h .. h + 3 (RND)
+            if (RND) calls(tau + 1);
 #pragma unroll
             for (int h = 0; h < NH; ++h) {
-                if (RND && (h & 3) == 0) {
-                    // lane j of each quad computes half-step h + j's Philox call for the quad's
-                    // group; the quad's four lanes exchange the four words of each call
-                    const int hj = h + (lane & 3);
-                    const uint32_t gy = (ylo + (uint32_t)(tau - hj)) & rmask;
-                    const uint32_t step = 2u * t0 + (uint32_t)hj;
-                    const uint4 c =
-                        philox4x32_10(make_uint4((gy << lgG) + (wcol >> 2), step, TAG_SCA << 8, stream), key);
-                    __syncwarp();
-                    *reinterpret_cast<uint4*>(rs + (lane & 3) * 4) = c;
-                    __syncwarp();
-#pragma unroll
-                    for (int u = 0; u < 4; ++u) rw[u] = rs[u * 4 + (lane & 3)];
-                }
                 const int sg = h & 1;                          // sublattice updated
                 const int sr = ((i - h) % NW + NW) % NW;       // slot of row tau - h
                 const int sr1 = ((i - h + 1) % NW + NW) % NW;  // slot of row tau - h + 1
@@ -173,9 +192,16 @@ scabit_strip_kernel(const uint32_t* __restrict__ src, uint32_t* __restrict__ dst
                 if (shifted) xX = __funnelshift_r(oX, __shfl_sync(0xFFFFFFFFu, oX, src_dn), 1);
                 uint32_t pm = 0u, qm = 0u;
                 if (PM == 1) pm = ~(tX | tY) & xX & oY;
-                if (PM == 2) pm = ~(tX | tY) & xX & oY & ~rw[h & 3];
+                if (PM == 2) pm = ~(tX | tY) & xX & oY & ~rwc[h];
                 if (QM == 1) qm = tX & tY & ~(xX | oY);
-                if (QM == 2) qm = tX & tY & ~(xX | oY) & ~rw[h & 3];
+                if (QM == 2) qm = tX & tY & ~(xX | oY) & ~rwc[h];
+                if (PM == 2 && QM == 2 && !COUNT) {
+                    // both kinds on the same random word: a candidate has tX == tY, xX == oY and
+                    // tX != xX (a minimum 0,0,1,1 or a maximum 1,1,0,0), so the flip mask is
+                    // ((tX ^ tY) | ~(tX ^ xX))' & ((xX ^ oY) | r)' -- three 3-input operations
+                    pm = (~(tX ^ tY) & (tX ^ xX)) & (~(xX ^ oY) & ~rwc[h]);
+                    qm = 0u;
+                }
                 if (COUNT) {
                     const int r = tau - h;
                     if (owned && r >= H && r < H + Bc) {
@@ -206,6 +232,7 @@ scabit_strip_kernel(const uint32_t* __restrict__ src, uint32_t* __restrict__ dst
             }
             // row tau + S into the ring slot row tau left a tick ago
             issue(tau + S);
+            if (RND) exchange();
         }
     }
     cp_async_wait<0>();  // no copy may land in this warp's ring after it has left

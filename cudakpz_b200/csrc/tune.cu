@@ -4,7 +4,7 @@
 // half-step, not by thread), so the tuner is free to time real passes on scratch copies of
 // the lattice and keep the fastest.  Results are cached per (lattice size, rate class,
 // SM count) in memory and, when KPZB_TUNE_CACHE names a file, in that file
-// (one "key k cps ms_per_mcs" line per entry).
+// (one "key kind k cps ms_per_mcs band" line per entry).
 #include <cstdio>
 #include <cstdlib>
 #include <map>
@@ -76,12 +76,13 @@ bool lookup_plan(int lx, int ly, uint64_t Tp, uint64_t Tq, int sm_count, Plan* o
 
 Plan default_plan(int lx, int ly, uint64_t Tp, uint64_t Tq, int sm_count)
 {
-    // without measuring: the register-wavefront kernel (6 MCS per pass, 2 CTAs per SM) for
-    // rates without random planes, where it fits -- the fastest shape measured at 16384^2 --
-    // else the band heuristic
-    if (dec_mode(make_thresh(Tp), make_thresh(Tq)) == DEC_NONE &&
-        scabit_wave_shape(lx, ly, 6, sm_count, 2, DEC_NONE).ok)
-        return Plan{6, 2, 0.f, false, PASS_WAVE};
+    // without measuring: the warp-tile kernel for rates of at most one random plane, in the
+    // shapes measured fastest at 16384^2 on a B200 (8 MCS per pass and 128-row tiles without a
+    // random plane, 4 MCS and 56-row tiles with one), else the band heuristic
+    (void)sm_count;
+    const int mode = dec_mode(make_thresh(Tp), make_thresh(Tq));
+    if (mode == DEC_NONE && scabit_strip_shape(lx, ly, 8, 128, mode).ok) return Plan{8, 0, 0.f, false, PASS_STRIP, 128};
+    if (mode == DEC_ONE && scabit_strip_shape(lx, ly, 4, 56, mode).ok) return Plan{4, 0, 0.f, false, PASS_STRIP, 56};
     const int k = auto_fusion(lx, ly);
     return Plan{k, 0, 0.f, false, PASS_BAND};
 }
@@ -167,7 +168,7 @@ cudaError_t tune_plan(uint32_t* d_src, int lx, int ly, uint64_t seed, uint32_t s
     const ScabitShape hs = scabit_shape(lx, ly, sm_count);
     for (const Cand& c : cands) {
         // enough MCS per measurement to dwarf launch overhead, capped by lattice size
-        const int target = (lx + ly >= 26) ? 8 : 32;
+        const int target = (lx + ly >= 26) ? 16 : 32;
         auto run = [&](int mcs) -> cudaError_t {
             if (c.k == 1) {
                 for (int m = 0; m < mcs; ++m)

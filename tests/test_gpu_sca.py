@@ -305,10 +305,10 @@ def test_pipelined_push_equals_sync(kpzb, oracle, sched, lx):
     sb.close()
 
 
-@pytest.mark.parametrize("p,q,kind", [(1.0, 0.0, "wave"), (0.5, 0.5, "band")])
+@pytest.mark.parametrize("p,q,kind", [(1.0, 0.0, "strip"), (0.5, 0.5, "strip"), (0.9, 0.1, "band")])
 def test_untuned_default_plan(kpzb, oracle, monkeypatch, p, q, kind):
-    """KPZB_AUTOTUNE=0: no measurement; the wave kernel for rates without random planes, the band
-    heuristic otherwise -- word for word against the oracle either way."""
+    """KPZB_AUTOTUNE=0: no measurement; the warp-tile kernel for rates of at most one random
+    plane, the band heuristic otherwise -- word for word against the oracle either way."""
     monkeypatch.setenv("KPZB_AUTOTUNE", "0")
     monkeypatch.delenv("KPZB_TUNE_CACHE", raising=False)
     lx, ly, n = 13, 7, 13  # a size no other test tunes (the process caches tuned plans)

@@ -1,7 +1,8 @@
 #!/usr/bin/env python
 """Build the reference's own CPU schedulers into oracle/_ref/kpz_ref -- TEST INFRASTRUCTURE.
 
-Compiles CudaKpz sources where they lie (read from /root/reference, never copied into this
+Compiles CudaKpz sources where they lie (read from the tree named by KPZ_REFERENCE, by default
+the `reference` directory beside this repository; never copied into this
 repository) together with oracle/ref_driver.cpp.  The reference's own build system needs
 MPI, HDF5/libSplash and a TinyMT parameter table that is not shipped, and its code falls off
 the end of several non-void functions, which current g++ turns into traps.  So this recipe:
@@ -27,7 +28,7 @@ import subprocess
 import sys
 from pathlib import Path
 
-REF = Path(os.environ.get("KPZ_REFERENCE", "/root/reference"))
+REF = Path(os.environ.get("KPZ_REFERENCE", str(Path(__file__).resolve().parent.parent.parent / "reference")))
 HERE = Path(__file__).resolve().parent
 OUT = HERE / "_ref"
 WORK = Path("/tmp/kpzb_refbuild")

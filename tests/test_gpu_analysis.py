@@ -103,3 +103,49 @@ def test_invariants_local_encoding(kpzb, oracle):
     s.pushSystem(bad)
     ok, rep = s.consitencyCheck()
     assert rep == oracle.check_invariants(bad, 9, 9, enc)
+
+
+def sawtooth_lattice(oracle, lx, amp):
+    """ENC_CBBIT words of the surface h(x, y) = t(x) + t(y), t a triangle wave rising and falling
+    by one per site between -amp/2 and amp/2 (a sum of two +-1 walks, so every plaquette closes):
+    heights near zero with steep slopes, i.e. large offsets inside every 64-site chunk."""
+    L = 1 << lx
+    x = np.arange(L)
+    ph = (x + amp // 2) % (2 * amp)  # t(0) = 0: the walk starts at mid height
+    t = np.where(ph < amp, ph, 2 * amp - ph) - amp // 2
+    h = t[None, :] + t[:, None]  # h[y, x]
+    sx = (h > np.roll(h, 1, axis=1)).astype(np.uint32)  # s_x(x, y) = [h(x,y) > h(x-1,y)]
+    sy = (h > np.roll(h, 1, axis=0)).astype(np.uint32)  # s_y(x, y) = [h(x,y) > h(x,y-1)]
+    yy, xx = np.meshgrid(np.arange(L), x, indexing="ij")
+    word = (yy >> 2) * (L >> 2) + (xx >> 2)
+    bit = ((xx & 3) << 1) | ((yy & 3) << 3)
+    local = np.zeros(L * L // 16, dtype=np.uint64)
+    np.add.at(local, word.ravel(), ((sx | (sy << 1)).astype(np.uint64) << bit.astype(np.uint64)).ravel())
+    return oracle.local_to_cbbit(local.astype(np.uint32), lx, lx)
+
+
+@pytest.mark.parametrize("case", ["flat6", "rough300", "sawtooth"])
+def test_odd_moments_near_zero_height(kpzb, oracle, case):
+    """The roughness walk builds each 64-site chunk's sum of h^k from exact integer power sums of
+    the offsets from the chunk's first height, expanded binomially in FP64 once per chunk; where
+    heights are near zero while the offsets are large, the expansion's terms cancel.  The odd
+    moments <h^3>, <h^5>, <h^7> against the oracle's per-site long-double sums (exact integers
+    here): absolute error at most 1e-12 * <|h|^k> + 1e-12, on a flat start after 6 MCS, a rough
+    surface after 300 MCS (p = q = 1/2), and a steep sawtooth surface centred on zero."""
+    lx = ly = 9
+    if case == "sawtooth":
+        w = sawtooth_lattice(oracle, lx, 64)
+    else:
+        w = oracle.homogeneous(lx, ly, oracle.ENC_CBBIT)
+        oracle.sca_mcs_words(w, lx, ly, 5, 0, 0, 6 if case == "flat6" else 300, 0.5, 0.5)
+    rep = oracle.check_invariants(w, lx, ly, oracle.ENC_CBBIT)
+    assert list(rep) == [0, 0, 0], rep  # a valid surface
+    s = kpzb.Scheduler(lx, ly)
+    s.pushSystem(w)
+    r = s.roughness()
+    s.close()
+    ref = oracle.roughness(w, lx, ly, oracle.ENC_CBBIT)
+    h = oracle.heights(w, lx, ly, oracle.ENC_CBBIT).astype(np.float64)
+    for k in (3, 5, 7):
+        scale = float(np.mean(np.abs(h) ** k))
+        assert abs(r.h[k - 1] - ref[k]) <= 1e-12 * scale + 1e-12, (k, r.h[k - 1], ref[k], scale)

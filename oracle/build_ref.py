@@ -14,7 +14,8 @@ the end of several non-void functions, which current g++ turns into traps.  So t
   3. adds the missing return statements,
   4. writes a placeholder TinyMT parameter table (TinyMT's published default parameter set
      repeated; the reference's table is absent, so TinyMT streams are not the reference's),
-  5. compiles with g++ -O2 and writes the binary to oracle/_ref/kpz_ref.
+  5. compiles with g++ -O2 and writes the binary to oracle/_ref/kpz_ref (with oracle/ref_inject.cpp,
+     the reference's CBBit scheduler fed this project's per-site decisions, and the C oracle).
 
 Only code paths that do not depend on the TinyMT table are used as golden vectors
 (p = 1 or q = 1 deterministic SCA, dSFMT random-sequential, roughness, correlator).
@@ -248,8 +249,16 @@ def main() -> int:
         subprocess.run([*cc, *extra, "-c", str(path), "-o", str(obj)], check=True)
         objs.append(str(obj))
     drv = WORK / "ref_driver.o"
-    subprocess.run(["g++", *flags, "-c", str(HERE / "ref_driver.cpp"), "-o", str(drv)], check=True)
-    subprocess.run(["g++", "-pthread", "-o", str(OUT / "kpz_ref"), str(drv), *objs], check=True)
+    subprocess.run(["g++", *flags, f"-I{HERE}", "-c", str(HERE / "ref_driver.cpp"), "-o", str(drv)], check=True)
+    # the decision-injection unit (the reference's CBBit scheduler with a stand-in generator fed by
+    # the oracle's restatement of the counter stream) and that restatement itself
+    inj = WORK / "ref_inject.o"
+    subprocess.run(["g++", *flags, "-Dprotected=public", f"-I{HERE}", "-c", str(HERE / "ref_inject.cpp"), "-o",
+                    str(inj)], check=True)
+    orc = WORK / "kpz_oracle.o"
+    subprocess.run(["gcc", "-O2", "-std=c11", "-c", str(HERE / "kpz_oracle.c"), "-o", str(orc)], check=True)
+    subprocess.run(["g++", "-pthread", "-o", str(OUT / "kpz_ref"), str(drv), str(inj), str(orc), *objs, "-lm"],
+                   check=True)
     print(f"built {OUT / 'kpz_ref'}")
     build_adapter(objs, flags)
     build_gpu(objs)

@@ -9,6 +9,9 @@
 //                                   writes the final lattice to OUT
 //   cbbit LX P Q N IN|flat OUT THR  SchedulerCPUCBBit<TinyMT32>::mcsPQSyncRng(N) (ENC_CBBIT)
 //   cb LX P Q N IN|flat OUT THR     SchedulerCPUCB<TinyMT32>::mcsPQSyncRng(N) (ENC_LOCAL SCA)
+//   cbbit-inject LX P Q N IN|flat OUT SEED STREAM
+//                                   SchedulerCPUCBBit::mcsPQSyncRng(N), its per-site path fed the
+//                                   counter stream's decisions (ref_inject.cpp), one thread
 //   rough ENC LX IN                 SchedulerService::roughness() (Correlator::roughnessThreaded)
 //   corr ENC LX SNAP SYS            Correlator::set(SNAP) then Correlator::correlate() on SYS;
 //                                   prints W2 h1..h7 ch cs
@@ -38,6 +41,13 @@
 #include "schedulerCPUCBBit.h"
 #include "schedulerCPUDTr.h"
 #include "schedulerService.h"
+
+extern "C" {
+#include "kpz_oracle.h"
+}
+// ref_inject.cpp
+int ref_cbbit_injected(int lx, double p, double q, int n, uint32_t* words, uint64_t seed, uint32_t stream,
+                       uint64_t t0);
 
 // The HDF5/libSplash and MPI entry points of SchedulerService are outside the hot path;
 // the build strips their definitions, and these keep the vtables complete.
@@ -167,6 +177,27 @@ int main(int argc, char** argv)
         const bool ok = s.saveBit(argv[5], argc > 6 ? argv[6] : nullptr);
         loud();
         return ok ? 0 : 1;
+    }
+    if (cmd == "cbbit-inject" && argc >= 10) {
+        const int lx = std::atoi(argv[2]);
+        const double p = std::atof(argv[3]), q = std::atof(argv[4]);
+        const int n = std::atoi(argv[5]);
+        const size_t nw = (size_t)1 << (2 * lx - 4);
+        std::vector<uint32_t> w(nw);
+        if (std::string(argv[6]) == "flat")
+            ko_init_homogeneous(w.data(), lx, lx, 1);
+        else
+            w = load(argv[6], nw);
+        quiet();
+        const int rc = ref_cbbit_injected(lx, p, q, n, w.data(), std::strtoull(argv[8], nullptr, 10),
+                                          (uint32_t)std::strtoul(argv[9], nullptr, 10), 0);
+        loud();
+        if (rc != 0) {
+            std::cerr << "cbbit-inject: rates not on the per-site path, or not separable in float\n";
+            return 1;
+        }
+        save(argv[7], w.data(), nw);
+        return 0;
     }
     if (cmd == "cbbit" || cmd == "cb") {
         const int lx = std::atoi(argv[2]);

@@ -106,8 +106,35 @@ def main():
     # 6. SchedulerService::saveBit file of the RS lattice (256^2, seed 1, 16 MCS): the lattice
     #    file format the checkpoint entry points keep (kpz/schedulerService.cpp:389-401)
     run("savebit", 8, 1, 16, HERE / "ref_savebit_rs256.bin", "CudaKpz saveBit fixture")
+    inject_cases(tmp)
     print("golden vectors written to", HERE)
 
 
+# rates, lx, MCS, start: random rates through the reference's per-site path
+INJECT_CASES = [((0.5, 0.5), 8, 3, "flat"), ((0.9, 0.1), 9, 4, "flat"), ((0.3, 0.7), 8, 3, "rand"),
+                ((0.75, 0.25), 8, 5, "rand"), ((0.95, 0.05), 9, 2, "flat")]
+INJECT_SEED, INJECT_STREAM = 42, 3
+
+
+def inject_cases(tmp: Path):
+    """7. random rates: the reference's SchedulerCPUCBBit::mcsPQSyncRng per-site path
+    (kpz/schedulerCPUCBBit_nested.inl:261-295) with its generator replaced by a stand-in that
+    hands it the counter stream's per-site decisions (oracle/ref_inject.cpp), one thread;
+    random starts are oracle lattices stored beside the results."""
+    out = {}
+    for (p, q), lx, n, init in INJECT_CASES:
+        w = o.homogeneous(lx, lx, o.ENC_CBBIT) if init == "flat" else o.random_lattice(lx, lx, o.ENC_CBBIT, seed=8, mcs=3)
+        key = f"p{p}_q{q}_lx{lx}_n{n}_{init}"
+        w.tofile(tmp / "in.bin")
+        run("cbbit-inject", lx, p, q, n, tmp / "in.bin", tmp / "out.bin", INJECT_SEED, INJECT_STREAM)
+        if init != "flat":
+            out[key + "_in"] = w
+        out[key + "_out"] = np.fromfile(tmp / "out.bin", dtype=np.uint32)
+    np.savez_compressed(HERE / "ref_inject_cbbit.npz", **out)
+
+
 if __name__ == "__main__":
-    main()
+    if sys.argv[1:] == ["inject"]:
+        inject_cases(Path(tempfile.mkdtemp()))
+    else:
+        main()

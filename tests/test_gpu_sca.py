@@ -362,3 +362,21 @@ def test_strip_kernel_bit_exact(kpzb, oracle, monkeypatch, lx, ly, k, band, p, q
     assert plan[2] == ("band" if (p, q) == (0.9, 0.1) else "strip"), plan
     assert first_diff(got, ref) is None, first_diff(got, ref)
     assert cnt == rc
+
+
+@pytest.mark.parametrize("fusion", [1, 0])
+def test_random_rates_vs_reference_with_injected_decisions(kpzb, oracle, fusion):
+    """At random rates, the GPU lattice against the reference's own per-site update fed the
+    counter stream's decisions (tests/golden/ref_inject_cbbit.npz, from oracle/ref_inject.cpp),
+    one half-step per launch and the tuned pass plan."""
+    from test_oracle_ref_inject import STREAM, SEED, cases
+    for name, p, q, lx, n, w, want in cases(oracle):
+        s = kpzb.Scheduler(lx, lx)
+        s.pushSystem(w)
+        s.setPQ(p, q)
+        s.supplySeed(SEED, STREAM)
+        s.setFusion(fusion)
+        s.mcsPQSyncRng(n)
+        got = s.popSystem()
+        s.close()
+        assert first_diff(got, want) is None, (name, first_diff(got, want))

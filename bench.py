@@ -768,7 +768,8 @@ def run_batch(args, world, rank, local):
     sites = float(sum(1 << (2 * lx) for lx in lxs))
     b = kpzb.Batch(lxs, [a for a, _ in pq], [c for _, c in pq], seeds, device=local)
     m = 64
-    b.mcs(m * args.warmup)
+    b.mcs(m * max(1, args.warmup))  # the first MCS tunes the pass shape (replicas restored after)
+    plan = b.plan()
     torch.cuda.synchronize()
     clocks = ClockSampler(local)
     clocks.start()
@@ -824,9 +825,30 @@ def run_batch(args, world, rank, local):
     for s in hs:
         s.close()
     b.close()
+
+    # where the time goes: the same kind of batch restricted to one size class or one rate class
+    def sub_rate(sel):
+        idx = [i for i in range(len(lxs)) if sel(i)]
+        sb = kpzb.Batch([lxs[i] for i in idx], [pq[i][0] for i in idx], [pq[i][1] for i in idx],
+                        [seeds[i] for i in idx], device=local)
+        sb.mcs(m)
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
+        sb.mcs(m)
+        d = time.perf_counter() - t1
+        out = {"replicas": len(idx), "upd_per_ns": round(sum(1 << (2 * lxs[i]) for i in idx) * m / (d * 1e9), 1),
+               "plan": {"mcs_per_pass": sb.plan()[0], "ctas_per_sm": sb.plan()[1]}}
+        sb.close()
+        return out
+    breakdown = {"256^2 replicas (resident in shared memory)": sub_rate(lambda i: lxs[i] == 8),
+                 "1024^2-4096^2 replicas (banded)": sub_rate(lambda i: lxs[i] > 8),
+                 "rate (1,0): no random plane": sub_rate(lambda i: pq[i] == (1.0, 0.0)),
+                 "rates (0.9,0.1) and (0.75,0.25): bit-serial planes": sub_rate(lambda i: pq[i] != (1.0, 0.0))}
     return _line(value, dt_b * 1e3 / args.steps, args, world,
                  {"workload": "512 SCABit replicas (256x256^2,128x1024^2,64x2048^2,64x4096^2), mixed (p,q)",
                   "mcs_per_step": m, "parallelism": f"replicas x{world}"},
+                 plan={"mcs_per_pass": plan[0], "ctas_per_sm": plan[1], "source": "kpzb_batch_autotune"},
+                 breakdown=breakdown,
                  plain_loop_value=round(plain, 3), speedup_vs_plain_loop=round(value / plain, 2),
                  tuned_loop_value=round(tuned, 3), speedup_vs_tuned_loop=round(value / tuned, 2),
                  replicas_bit_identical_to_single_runs=same, clocks=clk,
@@ -996,7 +1018,7 @@ def run_configs(args, local):
 
     def c4():
         ln = run_batch(sub(workload="batch", steps=2, warmup=1), 1, 0, local)
-        return {k: ln[k] for k in ("value", "unit", "plain_loop_value", "speedup_vs_plain_loop",
+        return {k: ln[k] for k in ("value", "unit", "plan", "breakdown", "plain_loop_value", "speedup_vs_plain_loop",
                                    "tuned_loop_value", "speedup_vs_tuned_loop",
                                    "replicas_bit_identical_to_single_runs", "config") if k in ln}
     out["C4"] = guard(c4)

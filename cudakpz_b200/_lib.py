@@ -100,6 +100,9 @@ SIGNATURES = {
     "kpzb_batch_init_homogeneous": (C.c_int, [_vp]),
     "kpzb_batch_mcs": (C.c_int, [_vp, C.c_int]),
     "kpzb_batch_set_fusion": (C.c_int, [_vp, C.c_int, C.c_int]),
+    "kpzb_batch_set_ctas_per_sm": (C.c_int, [_vp, C.c_int]),
+    "kpzb_batch_get_plan": (C.c_int, [_vp, _intp, _intp]),
+    "kpzb_batch_autotune": (C.c_int, [_vp, _intp, _intp, C.POINTER(C.c_float)]),
     "kpzb_batch_get_mcs": (C.c_int, [_vp, _u64p]),
     "kpzb_batch_push": (C.c_int, [_vp, C.c_int, _vp]),
     "kpzb_batch_pop": (C.c_int, [_vp, C.c_int, _vp]),

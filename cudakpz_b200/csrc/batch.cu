@@ -12,7 +12,12 @@
 // (seed, stream, half-step, site).
 #include <algorithm>
 #include <cmath>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
+#include <map>
+#include <mutex>
+#include <string>
 #include <vector>
 
 #include "kpzb_api_internal.h"
@@ -22,8 +27,12 @@
 
 namespace kpzb {
 
-constexpr int BATCH_THREADS = 512;
+constexpr int BATCH_THREADS = 512;  // threads of a CTA at one CTA per SM; 256 at two or three
 constexpr size_t BATCH_SMEM = 227 * 1024 - 1024;
+
+// shared memory of one CTA at `cps` CTAs per SM (the SM's 228 KB split, 1 KB each reserved)
+inline size_t batch_smem(int cps) { return cps <= 1 ? BATCH_SMEM : ((228 * 1024) / (size_t)cps - 1024) & ~(size_t)127; }
+inline int batch_threads(int cps) { return cps <= 1 ? BATCH_THREADS : 256; }
 
 struct RepDesc {
     uint32_t* buf[2];  // double buffer; buf[parity] holds the current state
@@ -47,7 +56,8 @@ struct PassState {
     uint32_t err;     // set when a bounded wait expired
 };
 
-__global__ void __launch_bounds__(BATCH_THREADS)
+template <int THREADS>
+__global__ void __launch_bounds__(THREADS)
 batch_pass_kernel(const RepDesc* __restrict__ reps, const Item* __restrict__ items, int nitems,
                   PassState* st, int k)
 {
@@ -77,7 +87,7 @@ batch_pass_kernel(const RepDesc* __restrict__ reps, const Item* __restrict__ ite
                          r.resident != 0, t0, r.key, r.stream, r.tp, r.tq};
         // rates differ between replicas of one launch: the run-time decision mode (a per-item
         // dispatch to rate-specialised copies measured 2-5 % slower: larger code, more registers)
-        if (!scabit_band<-1, true, false, BATCH_THREADS>(smem, ctl, g, nd, nr, &st->err)) return;
+        if (!scabit_band<-1, true, false, THREADS>(smem, ctl, g, nd, nr, &st->err)) return;
         phase ^= 1u;
     }
 }
@@ -108,6 +118,8 @@ struct kpzb_batch {
     uint32_t t = 0, parity = 0;  // host mirror of the pass state
     int k = 8;                   // MCS per pass
     int chunk = 8;               // passes per graph replay
+    int cps = 1;                 // CTAs per SM (1: 512 threads, 2 or 3: 256 threads each)
+    bool planned = false;        // k and cps set by the caller or the tuner (else tuned on first MCS)
     cudaGraphExec_t graph = nullptr;
     AnalysisScratch an{};
     int max_ly = 0;
@@ -135,14 +147,15 @@ static kpzb_status batch_layout(kpzb_batch* b)
         const uint64_t Wr = 1ull << (r.lx - 6);
         const uint64_t row_bytes = 16ull * Wr;
         const int64_t rows = 1ll << r.ly;
-        if ((uint64_t)rows * row_bytes <= BATCH_SMEM) {
+        const size_t smem = batch_smem(b->cps);
+        if ((uint64_t)rows * row_bytes <= smem) {
             r.resident = 1;
             r.B = (int)rows;
             work.push_back({(double)rows * Wr, Item{i, 0}});
             continue;
         }
         r.resident = 0;
-        const int Rmax = (int)(BATCH_SMEM / row_bytes);
+        const int Rmax = (int)(smem / row_bytes);
         const int Bmax = Rmax - 4 * b->k;
         if (Bmax < 1) return fail(KPZB_EINVAL, "batch: lattice rows too wide for the pass depth");
         const int nb = (int)((rows + Bmax - 1) / Bmax);
@@ -173,8 +186,12 @@ static kpzb_status batch_layout(kpzb_batch* b)
 
 static cudaError_t enqueue_pass(kpzb_batch* b)
 {
-    batch_pass_kernel<<<b->sm_count, BATCH_THREADS, BATCH_SMEM, b->st>>>(b->d_reps, b->d_items,
-                                                                         b->nitems, b->d_state, b->k);
+    if (b->cps <= 1)
+        batch_pass_kernel<BATCH_THREADS><<<b->sm_count, BATCH_THREADS, BATCH_SMEM, b->st>>>(
+            b->d_reps, b->d_items, b->nitems, b->d_state, b->k);
+    else
+        batch_pass_kernel<256><<<b->sm_count * b->cps, 256, batch_smem(b->cps), b->st>>>(
+            b->d_reps, b->d_items, b->nitems, b->d_state, b->k);
     batch_advance_kernel<<<1, 1, 0, b->st>>>(b->d_state, b->k);
     return cudaGetLastError();
 }
@@ -235,8 +252,10 @@ extern "C" kpzb_status kpzb_batch_create(kpzb_batch** out, int n, const int* lx,
         return bail(cuda_fail(e, "cudaMalloc(state)"));
     cudaMemset(b->d_state, 0, sizeof(PassState));
     if ((e = analysis_alloc(&b->an, b->max_ly)) != cudaSuccess) return bail(cuda_fail(e, "analysis_alloc"));
-    if ((e = cudaFuncSetAttribute(batch_pass_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)BATCH_SMEM)) != cudaSuccess)
+    if ((e = cudaFuncSetAttribute(batch_pass_kernel<BATCH_THREADS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)BATCH_SMEM)) != cudaSuccess ||
+        (e = cudaFuncSetAttribute(batch_pass_kernel<256>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)batch_smem(2))) != cudaSuccess)
         return bail(cuda_fail(e, "smem attribute"));
     kpzb_status s = batch_layout(b);
     if (s != KPZB_OK) return bail(s);
@@ -283,7 +302,164 @@ extern "C" kpzb_status kpzb_batch_set_fusion(kpzb_batch* b, int mcs_per_pass, in
         return fail(KPZB_EINVAL, "batch fusion: 1 <= mcs_per_pass <= 32, 1 <= passes_per_graph <= 256");
     b->k = mcs_per_pass;
     b->chunk = passes_per_graph;
+    b->planned = true;
     return batch_layout(b);
+}
+
+extern "C" kpzb_status kpzb_batch_set_ctas_per_sm(kpzb_batch* b, int ctas_per_sm)
+{
+    BCHECK(b);
+    if (ctas_per_sm < 1 || ctas_per_sm > 3) return fail(KPZB_EINVAL, "batch: 1 <= ctas_per_sm <= 3");
+    b->cps = ctas_per_sm;
+    b->planned = true;
+    return batch_layout(b);
+}
+
+extern "C" kpzb_status kpzb_batch_get_plan(const kpzb_batch* b, int* mcs_per_pass, int* ctas_per_sm)
+{
+    if (!b || !mcs_per_pass || !ctas_per_sm) return fail(KPZB_EINVAL, "null argument");
+    *mcs_per_pass = b->k;
+    *ctas_per_sm = b->cps;
+    return KPZB_OK;
+}
+
+namespace {
+std::mutex g_batch_mu;
+std::map<std::string, std::pair<int, int>> g_batch_plans;  // batch signature -> (k, cps)
+
+// the replicas' sizes and rate classes (random planes the decision needs), and the SM count:
+// what the cost of a pass depends on
+std::string batch_signature(const kpzb_batch* b)
+{
+    std::map<std::pair<int, int>, int> census;
+    for (const RepDesc& r : b->reps) {
+        const int planes = std::max(r.tp.planes, r.tq.planes);
+        census[{r.lx, planes == 0 ? 0 : planes == 1 ? 1 : planes <= 4 ? 2 : 3}]++;
+    }
+    std::string key = "batch1:sm" + std::to_string(b->sm_count);
+    for (auto& c : census)
+        key += ":" + std::to_string(c.first.first) + "r" + std::to_string(c.first.second) + "x" +
+               std::to_string(c.second);
+    return key;
+}
+}  // namespace
+
+// Times every (MCS per pass, CTAs per SM) shape on the replicas as they are and keeps the
+// fastest; the replicas and the pass state are restored afterwards, so tuning changes no
+// result (every shape gives bit-identical replicas).  Cached per batch signature.
+extern "C" kpzb_status kpzb_batch_autotune(kpzb_batch* b, int* mcs_per_pass, int* ctas_per_sm, float* ms_per_mcs)
+{
+    BCHECK(b);
+    cudaError_t e;
+    if ((e = cudaStreamSynchronize(b->st)) != cudaSuccess) return cuda_fail(e, "batch sync");
+    // snapshot of every replica's current buffer and of the pass state
+    size_t total = 0;
+    for (const RepDesc& r : b->reps) total += (size_t)1 << (2 * r.lx - 2);
+    unsigned char* snap = nullptr;
+    if ((e = cudaMalloc(&snap, total)) != cudaSuccess) return cuda_fail(e, "cudaMalloc(tune snapshot)");
+    PassState saved{};
+    size_t off = 0;
+    for (const RepDesc& r : b->reps) {
+        const size_t bytes = (size_t)1 << (2 * r.lx - 2);
+        cudaMemcpyAsync(snap + off, r.buf[b->parity], bytes, cudaMemcpyDeviceToDevice, b->st);
+        off += bytes;
+    }
+    cudaMemcpyAsync(&saved, b->d_state, sizeof saved, cudaMemcpyDeviceToHost, b->st);
+    if ((e = cudaStreamSynchronize(b->st)) != cudaSuccess) {
+        cudaFree(snap);
+        return cuda_fail(e, "batch tune snapshot");
+    }
+    const int k0 = b->k, cps0 = b->cps;
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    float best = 1e30f;
+    int bk = k0, bc = cps0;
+    kpzb_status st = KPZB_OK;
+    const bool verbose = getenv("KPZB_TUNE_VERBOSE") != nullptr;
+    for (int cps = 1; cps <= 3 && st == KPZB_OK; ++cps)
+        for (int k : {2, 4, 6, 8}) {
+            b->k = k;
+            b->cps = cps;
+            if ((st = batch_layout(b)) != KPZB_OK) {
+                if (st == KPZB_EINVAL) {  // a lattice row too wide for this depth: not a candidate
+                    st = KPZB_OK;
+                    continue;
+                }
+                break;
+            }
+            const int passes = std::max(1, (16 + k - 1) / k);
+            if ((e = enqueue_pass(b)) != cudaSuccess) break;  // warm-up
+            cudaEventRecord(e0, b->st);
+            for (int i = 0; i < passes && e == cudaSuccess; ++i) e = enqueue_pass(b);
+            cudaEventRecord(e1, b->st);
+            if (e != cudaSuccess || (e = cudaEventSynchronize(e1)) != cudaSuccess) break;
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, e0, e1);
+            const float per = ms / (float)(passes * k);
+            if (verbose) fprintf(stderr, "kpzb batch tune k=%d cps=%d: %.4f ms/MCS\n", k, cps, per);
+            if (per < best) {
+                best = per;
+                bk = k;
+                bc = cps;
+            }
+        }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    // restore the replicas and the pass state
+    off = 0;
+    for (const RepDesc& r : b->reps) {
+        const size_t bytes = (size_t)1 << (2 * r.lx - 2);
+        cudaMemcpyAsync(r.buf[b->parity], snap + off, bytes, cudaMemcpyDeviceToDevice, b->st);
+        off += bytes;
+    }
+    PassState hs;
+    cudaMemcpyAsync(&hs, b->d_state, sizeof hs, cudaMemcpyDeviceToHost, b->st);
+    const cudaError_t se = cudaStreamSynchronize(b->st);
+    const bool timed_out = se == cudaSuccess && hs.err != 0;
+    saved.queue = 0;
+    cudaMemcpy(b->d_state, &saved, sizeof saved, cudaMemcpyHostToDevice);
+    cudaFree(snap);
+    b->k = (e == cudaSuccess && st == KPZB_OK && best < 1e30f) ? bk : k0;
+    b->cps = (e == cudaSuccess && st == KPZB_OK && best < 1e30f) ? bc : cps0;
+    const kpzb_status ls = batch_layout(b);
+    if (e != cudaSuccess) return cuda_fail(e, "batch tune");
+    if (se != cudaSuccess) return cuda_fail(se, "batch tune restore");
+    if (st != KPZB_OK) return st;
+    if (ls != KPZB_OK) return ls;
+    if (timed_out) return fail(KPZB_ETIMEOUT, "a bounded device wait (TMA mbarrier) expired while tuning");
+    b->planned = true;
+    {
+        std::lock_guard<std::mutex> lk(g_batch_mu);
+        g_batch_plans[batch_signature(b)] = {b->k, b->cps};
+    }
+    if (mcs_per_pass) *mcs_per_pass = b->k;
+    if (ctas_per_sm) *ctas_per_sm = b->cps;
+    if (ms_per_mcs) *ms_per_mcs = best;
+    return KPZB_OK;
+}
+
+// the plan of a batch whose caller set none: a cached tuning of the same signature, else a
+// fresh tuning (KPZB_AUTOTUNE=0: the fixed default, 8 MCS per pass at one CTA per SM)
+static kpzb_status batch_resolve_plan(kpzb_batch* b)
+{
+    if (b->planned) return KPZB_OK;
+    {
+        std::lock_guard<std::mutex> lk(g_batch_mu);
+        auto it = g_batch_plans.find(batch_signature(b));
+        if (it != g_batch_plans.end()) {
+            b->k = it->second.first;
+            b->cps = it->second.second;
+            b->planned = true;
+        }
+    }
+    if (b->planned) return batch_layout(b);
+    const char* env = getenv("KPZB_AUTOTUNE");
+    if (env && env[0] == '0') {
+        b->planned = true;
+        return KPZB_OK;
+    }
+    return kpzb_batch_autotune(b, nullptr, nullptr, nullptr);
 }
 
 // n MCS for every replica: whole passes of k MCS (graph replays of `chunk` passes, then
@@ -293,6 +469,10 @@ extern "C" kpzb_status kpzb_batch_mcs(kpzb_batch* b, int n)
     BCHECK(b);
     if (n < 0) return fail(KPZB_EINVAL, "negative MCS count");
     if ((uint64_t)b->t + (uint64_t)n >= (1ull << 31)) return fail(KPZB_EINVAL, "MCS counter limit 2^31");
+    if (n > 0) {
+        const kpzb_status ps = batch_resolve_plan(b);
+        if (ps != KPZB_OK) return ps;
+    }
     cudaError_t e;
     int passes = n / b->k;
     const int rem = n % b->k;

@@ -371,6 +371,22 @@ class Batch:
         check(lib.kpzb_batch_set_fusion(self._h, mcs_per_pass, passes_per_graph),
               "kpzb_batch_set_fusion")
 
+    def setCtasPerSm(self, ctas_per_sm: int):
+        check(lib.kpzb_batch_set_ctas_per_sm(self._h, ctas_per_sm), "kpzb_batch_set_ctas_per_sm")
+
+    def plan(self):
+        """(MCS per pass, CTAs per SM) of the pass kernel (kpzb_batch_get_plan)."""
+        k, c = C.c_int(), C.c_int()
+        check(lib.kpzb_batch_get_plan(self._h, C.byref(k), C.byref(c)), "kpzb_batch_get_plan")
+        return int(k.value), int(c.value)
+
+    def autotune(self):
+        """Time every pass shape on the replicas, keep the fastest, restore the replicas
+        (kpzb_batch_autotune); returns (MCS per pass, CTAs per SM, ms per MCS)."""
+        k, c, ms = C.c_int(), C.c_int(), C.c_float()
+        check(lib.kpzb_batch_autotune(self._h, C.byref(k), C.byref(c), C.byref(ms)), "kpzb_batch_autotune")
+        return int(k.value), int(c.value), float(ms.value)
+
     def deviceMcs(self) -> int:
         v = C.c_uint64()
         check(lib.kpzb_batch_get_mcs(self._h, C.byref(v)), "kpzb_batch_get_mcs")

@@ -244,9 +244,20 @@ kpzb_status kpzb_batch_destroy(kpzb_batch* b);
 kpzb_status kpzb_batch_init_homogeneous(kpzb_batch* b);
 /* n MCS for every replica (synchronous).  Square lattices only, 8 <= lx <= 16. */
 kpzb_status kpzb_batch_mcs(kpzb_batch* b, int n);
-/* MCS per pass (1..32; default 8) and passes per captured CUDA graph (1..256; default 8).
- * Results are identical for every choice. */
+/* MCS per pass (1..32) and passes per captured CUDA graph (1..256; default 8).  Results are
+ * identical for every choice.  A batch whose caller sets neither this nor the CTAs per SM is
+ * tuned on its first kpzb_batch_mcs (kpzb_batch_autotune; KPZB_AUTOTUNE=0: 8 MCS per pass at
+ * one CTA per SM).  No counterpart in the reference (its frontend runs one lattice per
+ * scheduler; the launch shaping it replaces is kpz/kpzSCABit.cu:63-106). */
 kpzb_status kpzb_batch_set_fusion(kpzb_batch* b, int mcs_per_pass, int passes_per_graph);
+/* Persistent CTAs per SM of the pass kernel: 1 (512 threads, 226 KB of shared memory each), 2 or
+ * 3 (256 threads and a half or a third of the SM's shared memory each). */
+kpzb_status kpzb_batch_set_ctas_per_sm(kpzb_batch* b, int ctas_per_sm);
+kpzb_status kpzb_batch_get_plan(const kpzb_batch* b, int* mcs_per_pass, int* ctas_per_sm);
+/* Times every (MCS per pass in {2,4,6,8}, CTAs per SM in {1,2,3}) shape on the replicas as they
+ * are, keeps the fastest (cached per set of replica sizes and rate classes) and restores the
+ * replicas and the MCS count, so tuning changes no result.  Outputs may be NULL. */
+kpzb_status kpzb_batch_autotune(kpzb_batch* b, int* mcs_per_pass, int* ctas_per_sm, float* ms_per_mcs);
 kpzb_status kpzb_batch_get_mcs(const kpzb_batch* b, uint64_t* mcs);
 kpzb_status kpzb_batch_push(kpzb_batch* b, int i, const uint32_t* words);
 kpzb_status kpzb_batch_pop(kpzb_batch* b, int i, uint32_t* words);

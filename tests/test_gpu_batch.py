@@ -79,3 +79,44 @@ def test_batch_rejects_bad_sizes(kpzb):
         kpzb.Batch([17], [1.0], [0.0], [1])
     with pytest.raises(kpzb.KpzbError):
         kpzb.Batch([7], [1.0], [0.0], [1])
+
+
+@pytest.mark.parametrize("cps,k", [(2, 4), (3, 6), (2, 8)])
+def test_batch_ctas_per_sm_matches_single_runs(kpzb, cps, k):
+    """The 256-thread pass kernel at two or three persistent CTAs per SM (half or a third of the
+    SM's shared memory each, so more lattices are banded) gives the single runs' lattices."""
+    lxs = [8, 9, 10, 11, 12, 8, 10]
+    b, pq, seeds = make_batch(kpzb, lxs, seed0=300)
+    b.setFusion(k)
+    b.setCtasPerSm(cps)
+    assert b.plan() == (k, cps)
+    n = 2 * k + 3
+    b.mcs(n)
+    for i, lx in enumerate(lxs):
+        assert np.array_equal(b.pop(i), single(kpzb, lx, pq[i][0], pq[i][1], seeds[i], 0, n)), (i, lx)
+    b.close()
+
+
+def test_batch_autotune_restores_and_matches(kpzb, monkeypatch):
+    """Tuning times passes on the replicas and restores them and the MCS count; the tuned plan
+    then gives the single runs' lattices.  A batch without a plan is tuned on its first MCS."""
+    monkeypatch.delenv("KPZB_AUTOTUNE", raising=False)
+    lxs = [8, 10, 12, 9, 11]
+    b, pq, seeds = make_batch(kpzb, lxs, seed0=500)
+    b.mcs(3)
+    before = [b.pop(i) for i in range(len(lxs))]
+    k, cps, ms = b.autotune()
+    assert k in (2, 4, 6, 8) and cps in (1, 2, 3) and ms > 0
+    assert b.deviceMcs() == 3 and b.plan() == (k, cps)
+    for i in range(len(lxs)):
+        assert np.array_equal(b.pop(i), before[i])
+    b.mcs(2 * k + 1)
+    for i, lx in enumerate(lxs):
+        assert np.array_equal(b.pop(i), single(kpzb, lx, pq[i][0], pq[i][1], seeds[i], 0, 3 + 2 * k + 1)), (i, lx)
+    b.close()
+    c, pq2, seeds2 = make_batch(kpzb, [8, 9], seed0=900)  # untuned: tuned (or cached) on first use
+    c.mcs(5)
+    assert c.plan()[1] in (1, 2, 3)
+    for i, lx in enumerate([8, 9]):
+        assert np.array_equal(c.pop(i), single(kpzb, lx, pq2[i][0], pq2[i][1], seeds2[i], 0, 5))
+    c.close()

@@ -60,8 +60,9 @@ def parse():
                     help="run only lattice i of the headline pair (profiling a single rate)")
     ap.add_argument("--lx", type=int, default=0,
                     help="override the workload's log2 lattice side (small cases for ncu)")
-    ap.add_argument("--dt-inner", choices=["dt", "dbsh", "db", "dtdbsh", "dbshrep"], default="dt",
-                    help="--workload dt: the DT kernel's inner decomposition (dbsh = the reference's default)")
+    ap.add_argument("--dt-inner", choices=["dt", "dbsh", "db", "dtdbsh", "dbshrep"], default=None,
+                    help="--workload dt / c3curve: the DT kernel's inner decomposition (default dbsh, the "
+                         "reference's default)")
     ap.add_argument("--reference-gpu", action="store_true",
                     help="with --impl reference: time the reference's own CUDA scheduler on this GPU "
                          "(oracle/_ref/kpz_ref_gpu) instead of its CPU scheduler")
@@ -69,7 +70,10 @@ def parse():
                     help="launcher check: form the process group (gloo, CPU), barrier, max over ranks, print")
     ap.add_argument("--no-configs", action="store_true",
                     help="skip the configs / reference_gpu blocks measured after the headline")
-    ap.add_argument("--workload", choices=["scabit", "dt", "db4", "batch", "gram", "measure"], default="scabit",
+    ap.add_argument("--seeds", type=int, default=16, help="--workload c3curve: independent runs")
+    ap.add_argument("--t-end", type=int, default=2000, help="--workload c3curve: MCS per run")
+    ap.add_argument("--workload", choices=["scabit", "dt", "db4", "batch", "gram", "measure", "c3curve"],
+                    default="scabit",
                     help="scabit: the headline 16384^2 SCA runs; dt / batch / gram: the other configs; "
                          "db4: the C3 lattice under the DB4 scheduler")
     return ap.parse_args()
@@ -623,8 +627,9 @@ def run_reference_gpu(args, world, rank, local):
         m = args.steps * max(1, args.mcs_per_step // 100)
         jobs = [(args.workload, lx, 0.95, 0.05, max(1, args.warmup // 3), m)]
         if args.workload == "dt":
-            binary = REF_GPU_BIN.parent / REF_GPU_DT_BIN[args.dt_inner]
-            name = f"SchedulerDT<SLCG64, dis> ({args.dt_inner.upper()})"
+            inner = args.dt_inner or "dbsh"
+            binary = REF_GPU_BIN.parent / REF_GPU_DT_BIN[inner]
+            name = f"SchedulerDT<SLCG64, dis> ({inner.upper()})"
         else:
             name = "Scheduler<SLCG64, LocalLayoutDB4> (db4)"
         config = {"workload": f"reference {name}, {1 << lx}^2, p=0.95 q=0.05", "mcs_timed": m}
@@ -691,7 +696,7 @@ def run_dt(args, world, rank, local):
     db4 = args.workload == "db4"
     s = kpzb.Scheduler(lx, lx, scheduler="db4" if db4 else "dt", device=local)
     if not db4:
-        s.setDtInner(args.dt_inner)
+        s.setDtInner(args.dt_inner or "dbsh")
     s.setPQ(0.95, 0.05)
     s.supplySeed(1 + rank)
     s.setStream(st.cuda_stream)
@@ -719,6 +724,7 @@ def run_dt(args, world, rank, local):
     # 36.3 MB written for 2^28 attempts), scaled by the lattice's sites: every launch reads and
     # writes its domain set's blocks and halos once, so the traffic grows with N
     traffic = round(DT_NCU_BYTES_32768 * N / (1 << 30)) if (not db4 and args.dt_inner == "dt") else None
+    inner = args.dt_inner or "dbsh"
     s.setStream(0)
     ok, rep = s.consitencyCheck()
     s.close()
@@ -736,7 +742,7 @@ def run_dt(args, world, rank, local):
                                "5-site dead border") if db4 else
                               (f"DT random-sequential {1 << lx}^2 periodic ({N // 4 >> 20} MiB ENC_LOCAL), "
                                f"flat start, p=0.95 q=0.05, random origin + shuffled domain sets per MCS, "
-                               f"inner scheme {args.dt_inner.upper()}"),
+                               f"inner scheme {inner.upper()}"),
                   "mcs_per_step": m, "lattice": f"{1 << lx}x{1 << lx}", "parallelism": f"replicas x{world}"},
                  roofline={"bound": "int-alu", "kernel": "dt_kernel", "achieved": int_roofline["achieved"],
                            "peak": int_roofline["peak"], "unit": "Tops/s (algorithmic integer ops)",
@@ -855,6 +861,99 @@ def run_batch(args, world, rank, local):
                  timing="host wall clock around synchronous batch calls",
                  cpu_baseline=batch_cpu_sample(os.cpu_count() or 1) if (rank == 0 and world == 1 and not args.no_cpu)
                  else None)
+
+
+def c3_times(t_end):
+    ts = [2 ** k for k in range(20) if 2 ** k < t_end]
+    return ts + [t_end]
+
+
+def curve_stats(w2, ts):
+    """Seed-averaged W^2(t) with standard errors, and beta from a fit of log W^2 against log t
+    over t >= 32 with a jackknife error over the seeds."""
+    import numpy as np
+    w2 = np.asarray(w2, dtype=float)
+    n = len(w2)
+    t = np.asarray(ts, dtype=float)
+    sel = t >= 32
+
+    def beta(rows):
+        return float(np.polyfit(np.log(t[sel]), np.log(rows.mean(0)[sel]), 1)[0] / 2)
+    b = beta(w2)
+    jk = [beta(np.delete(w2, i, axis=0)) for i in range(n)] if n > 2 else [b]
+    bj = float(np.mean(jk))
+    err = float(np.sqrt((n - 1) / n * np.sum((np.array(jk) - bj) ** 2))) if n > 2 else None
+    return {"t": list(ts), "w2_mean": [round(float(v), 6) for v in w2.mean(0)],
+            "w2_stderr": [round(float(v), 6) for v in (w2.std(0, ddof=1) / np.sqrt(n) if n > 1 else 0 * w2[0])],
+            "beta": round(b, 5), "beta_jackknife_err": None if err is None else round(err, 5), "seeds": n}
+
+
+def run_c3curve(args, world, rank, local):
+    """Config C3 as a curve: DT random-sequential on the 65536^2 lattice (--lx), p=0.95 q=0.05,
+    flat start, --seeds independent runs to --t-end MCS (default 16 x 2000), inner scheme
+    --dt-inner (the reference's default DBSH unless given); W^2 at t = 2^k and t_end, the
+    interface velocity from the deposition/desorption counters, beta from W^2(t)."""
+    import numpy as np
+    import torch
+    torch.cuda.set_device(local)
+    import cudakpz_b200 as kpzb
+    lx = args.lx or 16
+    N = float(1 << (2 * lx))
+    ts = c3_times(args.t_end)
+    inner = args.dt_inner or "dbsh"
+    w2, vel = [], []
+    t0 = time.perf_counter()
+    for sd in range(1 + rank * args.seeds, 1 + (rank + 1) * args.seeds):
+        s = kpzb.Scheduler(lx, lx, scheduler="dt", device=local)
+        s.setDtInner(inner)
+        s.setPQ(0.95, 0.05)
+        s.supplySeed(sd)
+        s.enableCounters(True)
+        t, row = 0, []
+        for T in ts:
+            s.mcsPQSyncRng(T - t)
+            t = T
+            row.append(s.roughness().w2)
+        dep, des = s.counters()
+        vel.append(2.0 * (dep - des) / N / ts[-1])
+        w2.append(row)
+        s.close()
+    secs = time.perf_counter() - t0
+    st = curve_stats(w2, ts)
+    v = np.array(vel)
+    return _line(N * ts[-1] * len(w2) * world / (secs * 1e9), secs * 1e3, args, world,
+                 {"workload": f"DT {1 << lx}^2, p=0.95 q=0.05, flat start, inner scheme {inner.upper()}, "
+                              f"{len(w2)} seeds x {ts[-1]} MCS", "lattice": f"{1 << lx}x{1 << lx}"},
+                 curve=st, velocity={"mean": round(float(v.mean()), 6),
+                                     "stderr": round(float(v.std(ddof=1) / np.sqrt(len(v))), 6) if len(v) > 1 else None},
+                 timing="host wall clock around the whole curve (includes the roughness reductions)")
+
+
+def run_reference_c3curve(args, rank, local):
+    """The reference's own SchedulerDT<SLCG64, dis> build with the chosen inner scheme on the same
+    curve (kpz_ref_gpu dtcurve, supplySeed(1, seed)): W^2 at the same times, beta."""
+    if rank != 0:
+        return None
+    binary = REF_GPU_BIN.parent / REF_GPU_DT_BIN[args.dt_inner or "dbsh"]
+    if not binary.exists():
+        return {"impl": "reference", "unavailable": f"{binary.name} not built"}
+    lx = args.lx or 16
+    ts = c3_times(args.t_end)
+    w2 = []
+    t0 = time.perf_counter()
+    for sd in range(1, args.seeds + 1):
+        r = subprocess.run([str(binary), "dtcurve", str(lx), "0.95", "0.05", str(sd)] + [str(t) for t in ts],
+                           capture_output=True, text=True, timeout=7200)
+        if r.returncode != 0:
+            return {"impl": "reference", "unavailable": f"{binary.name} dtcurve exited {r.returncode}"}
+        rows = [ln.split() for ln in r.stdout.splitlines() if ln and not ln.startswith("#")]
+        w2.append([float(x[1]) for x in rows])
+    secs = time.perf_counter() - t0
+    N = float(1 << (2 * lx))
+    return {"metric": METRIC, "impl": "reference", "device": "gpu", "value": round(N * ts[-1] * len(w2) / (secs * 1e9), 3),
+            "unit": UNIT, "n_gpus": 1, "config": {"workload": f"reference SchedulerDT ({(args.dt_inner or 'dbsh').upper()}) "
+                                                              f"{1 << lx}^2, p=0.95 q=0.05, {len(w2)} seeds x {ts[-1]} MCS"},
+            "curve": curve_stats(w2, ts), "timing": "host wall clock around the whole curve"}
 
 
 def run_measure(args, world, rank, local):
@@ -1045,9 +1144,14 @@ def main():
             import torch.distributed as dist
             dist.destroy_process_group()
         return
+    if args.workload == "c3curve" and args.impl == "reference":
+        line = run_reference_c3curve(args, rank, local)
+        if line is not None:
+            print(json.dumps(line), flush=True)
+        return
     if args.workload != "scabit" and args.impl == "ours":
         fn = {"dt": run_dt, "db4": run_dt, "batch": run_batch, "gram": run_gram,
-              "measure": run_measure}[args.workload]
+              "measure": run_measure, "c3curve": run_c3curve}[args.workload]
         line = fn(args, world, rank, local)
         if rank == 0:
             print(json.dumps(line), flush=True)

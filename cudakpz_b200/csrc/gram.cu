@@ -1,22 +1,26 @@
-// gram.cu -- exact height autocorrelator over stored snapshots: snapshot -> int8 limbs,
+// gram.cu -- exact height autocorrelator over stored snapshots: snapshots kept as slope bits,
 // the int64 CUDA-core Gram, exact recombination and the C ABI (kpzb_gram_*).
 //
 // Reference behaviour: Correlator::correlateThreaded / correlateKernelCBBit accumulate
 // sum h_snap * h_sys for one (snapshot, system) pair per call (kpz/correlator.cpp:491-593,
-// kpz/correlatorCuda.cu:276-369); here the whole Gram G[s][t] = sum_sites h_s h_t over every
-// stored pair is produced at once.
+// kpz/correlatorCuda.cu:276-369), and Correlator keeps its snapshots as lattices
+// (kpz/correlator.cpp:37-106); here the whole Gram G[s][t] = sum_sites h_s h_t over every stored
+// pair is produced at once.
+//
+// Storage: a snapshot is its two X-slope quadrants (N/8 bytes) and two int32 per row
+// (gram_slope.cuh) -- 2 GiB for 64 snapshots of 16384^2, where stored int8 limbs would take
+// 48 GiB.  Heights are rebuilt on the fly by the Gram kernels.
 //
 // Exactness: snapshot s keeps its path-relative heights (kpz/correlator.cpp:47-96) shifted
 // by c_s = floor(<h_s>): v = h - c_s, split into three balanced base-128 digits
-// v = l0 + 128 l1 + 16384 l2 with l_a in [-64, 63] (|v| < 1,056,832).  Row a*64+s of the
-// limb matrix A (192 x N, int8) holds l_a of snapshot s, stored K-tile-major: the 192 rows x
-// 128 sites of K tile kt are one contiguous 24 KB block (element (r, k) at
-// (k / 128) * 24576 + r * 128 + k % 128), so the tensor-core kernel's TMA box of one tile is a
-// single contiguous read.  The limb Gram A A^T is
-// exact in int32 over windows of 2^18 sites (|l l'| <= 2^12) and summed in int64; then
+// v = l0 + 128 l1 + 16384 l2 with l_a in [-64, 63] (-1056832 <= v <= 1040447, checked when the
+// snapshot is added).  Row a*64+s of the limb matrix A (192 x N, int8, built tile by tile in
+// shared memory) holds l_a of snapshot s.  The limb Gram A A^T is exact in int32 over windows
+// of 2^18 sites (|l l'| <= 2^12) and summed in int64; then
 //   sum v_s v_t = sum_{a,b} 128^(a+b) Glimb[a*64+s][b*64+t],
 //   sum h_s h_t = sum v_s v_t + c_t S1v_s + c_s S1v_t + N c_s c_t,
-// all in int64.  FP64 appears only in the caller's normalisation.
+// all in int64, with S1v_s = S1(h_s) - N c_s exact from the height walk.  FP64 appears only in
+// the caller's normalisation.
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -25,100 +29,57 @@
 #include "kpzb_api_internal.h"
 #include "kpzb_common.cuh"
 #include "kpzb_gram.h"
+#include "gram_slope.cuh"
 #include "kpzb_internal.h"
 
 namespace kpzb {
 
-constexpr uint64_t LIMB_TILE = 128;                 // sites per K tile
-constexpr uint64_t LIMB_TILE_BYTES = 192 * LIMB_TILE;  // one tile of all 192 rows
-
-__host__ __device__ inline uint64_t limb_index(int row, uint64_t k)
+// per-row data of snapshot s: {b(y), z(y)} = {Hs(y) - c, h(0, y) - c} from the height walk's
+// row starts Hs and row sums (the analysis scratch of the snapshot just measured)
+__global__ void gram_rows_kernel(const int64_t* __restrict__ rowstart, const int32_t* __restrict__ rowinfo,
+                                 uint64_t rows, int64_t c, int2* __restrict__ out)
 {
-    return (k / LIMB_TILE) * LIMB_TILE_BYTES + (uint64_t)row * LIMB_TILE + (k % LIMB_TILE);
+    for (uint64_t y = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; y < rows; y += (uint64_t)gridDim.x * blockDim.x)
+        out[y] = make_int2((int32_t)(rowstart[y] - c), (int32_t)(rowstart[y] + rowinfo[2 * y + 1] - c));
 }
 
-// v = h - c split into balanced base-128 limbs (snapshot s: rows s, 64+s, 128+s); flags |v|
-// too large for three limbs.
-__global__ void limb_kernel(const int32_t* __restrict__ h, uint64_t n, int32_t c, int8_t* __restrict__ A, int s,
-                            unsigned long long* __restrict__ sums, unsigned int* __restrict__ err)
-{
-    long long s0 = 0, s1 = 0, s2 = 0;
-    const uint64_t n16 = n / 16;
-    for (uint64_t j = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; j < n16;
-         j += (uint64_t)gridDim.x * blockDim.x) {
-        uint32_t w[3][4];
-        for (int q = 0; q < 4; ++q) {
-            const int4 hv = reinterpret_cast<const int4*>(h)[4 * j + q];
-            const int vals[4] = {hv.x, hv.y, hv.z, hv.w};
-            uint32_t p0 = 0, p1 = 0, p2 = 0;
-            for (int e = 0; e < 4; ++e) {
-                const int v = vals[e] - c;
-                const int l0 = ((v + 64) & 127) - 64;
-                const int v1 = (v - l0) >> 7;
-                const int l1 = ((v1 + 64) & 127) - 64;
-                const int l2 = (v1 - l1) >> 7;
-                if (l2 < -64 || l2 > 63) atomicExch(err, 1u);
-                s0 += l0;
-                s1 += l1;
-                s2 += l2;
-                p0 |= (uint32_t)(uint8_t)(int8_t)l0 << (8 * e);
-                p1 |= (uint32_t)(uint8_t)(int8_t)l1 << (8 * e);
-                p2 |= (uint32_t)(uint8_t)(int8_t)l2 << (8 * e);
-            }
-            w[0][q] = p0;
-            w[1][q] = p1;
-            w[2][q] = p2;
-        }
-        for (int a = 0; a < 3; ++a)
-            *reinterpret_cast<uint4*>(A + limb_index(a * 64 + s, 16 * j)) =
-                make_uint4(w[a][0], w[a][1], w[a][2], w[a][3]);
-    }
-    for (int o = 16; o > 0; o >>= 1) {
-        s0 += __shfl_xor_sync(0xffffffffu, s0, o);
-        s1 += __shfl_xor_sync(0xffffffffu, s1, o);
-        s2 += __shfl_xor_sync(0xffffffffu, s2, o);
-    }
-    if ((threadIdx.x & 31) == 0) {
-        atomicAdd(&sums[0], (unsigned long long)s0);
-        atomicAdd(&sums[1], (unsigned long long)s1);
-        atomicAdd(&sums[2], (unsigned long long)s2);
-    }
-}
-
-// Plain int64 CUDA-core Gram of v = l0 + 128 l1 + 16384 l2 over all snapshot pairs:
-// a CTA stages 64 snapshots x 128 sites of v (int32) in shared memory, each of 256 threads
-// owns a 4x4 block of (s,t) pairs with int64 accumulators; CTA results go to G by atomics.
-constexpr int G64_KC = 128;
+// Plain int64 CUDA-core Gram of v = h - c over all snapshot pairs, from the same slope
+// snapshots: a CTA takes a contiguous range of 128-site tiles, its 256 threads rebuild the 64
+// snapshots x 128 sites of each tile into shared memory (gram_slope.cuh, a lane quad per
+// snapshot), then each thread owns a 4x4 block of (s,t) pairs with int64 accumulators; CTA
+// results go to G by atomics.
+constexpr int G64_KC = GS_TILE;
 __global__ void __launch_bounds__(256)
-gram_int64_kernel(const int8_t* __restrict__ A, uint64_t n, int ns, unsigned long long* __restrict__ G)
+gram_int64_kernel(const SlopeSnapGeom g, uint64_t nkt, unsigned long long* __restrict__ G)
 {
     __shared__ int32_t v[64][G64_KC + 1];
     const int ts = (threadIdx.x >> 4) * 4, tt = (threadIdx.x & 15) * 4;
+    const int ns = g.n;
     long long acc[4][4];
     for (int i = 0; i < 4; ++i)
         for (int j = 0; j < 4; ++j) acc[i][j] = 0;
     const bool active = ts < ns && tt < ns && tt + 3 >= ts;  // upper triangle (with diagonal blocks)
-    for (uint64_t k0 = (uint64_t)blockIdx.x * G64_KC; k0 < n; k0 += (uint64_t)gridDim.x * G64_KC) {
-        for (int e = threadIdx.x; e < 64 * G64_KC; e += 256) {
-            const int s = e / G64_KC, kk = e - s * G64_KC;
-            int32_t val = 0;
-            if (s < ns) {
-                const uint64_t idx = k0 + kk;
-                val = (int32_t)A[limb_index(s, idx)] + 128 * (int32_t)A[limb_index(64 + s, idx)] +
-                      16384 * (int32_t)A[limb_index(128 + s, idx)];
-            }
-            v[s][kk] = val;
-        }
+    const uint64_t per = nkt / gridDim.x, rem = nkt % gridDim.x;
+    const uint64_t kt0 = blockIdx.x * per + ((uint64_t)blockIdx.x < rem ? (uint64_t)blockIdx.x : rem);
+    const uint64_t nloc = per + (blockIdx.x < rem ? 1 : 0);
+    const int s = threadIdx.x >> 2, qt = threadIdx.x & 3;
+    SlopeCursor cur;
+    slope_cursor_init(cur, s, qt);
+    for (uint64_t i = 0; i < nloc; ++i) {
+        const uint64_t t = kt0 + i;
+        int32_t h[32], lo, hi;
+        slope_quarter_heights(g, cur, t, slope_quarter_load(g, cur, t), h, lo, hi);
+        for (int j = 0; j < 32; ++j) v[s][32 * qt + j] = h[j];
         __syncthreads();
         if (active) {
             for (int kk = 0; kk < G64_KC; ++kk) {
                 int32_t a[4], b[4];
-                for (int i = 0; i < 4; ++i) {
-                    a[i] = v[ts + i][kk];
-                    b[i] = v[tt + i][kk];
+                for (int ii = 0; ii < 4; ++ii) {
+                    a[ii] = v[ts + ii][kk];
+                    b[ii] = v[tt + ii][kk];
                 }
-                for (int i = 0; i < 4; ++i)
-                    for (int j = 0; j < 4; ++j) acc[i][j] += (long long)a[i] * b[j];
+                for (int ii = 0; ii < 4; ++ii)
+                    for (int jj = 0; jj < 4; ++jj) acc[ii][jj] += (long long)a[ii] * b[jj];
             }
         }
         __syncthreads();
@@ -136,16 +97,18 @@ using namespace kpzb;
 
 struct kpzb_gram {
     int lx = 0, ly = 0, device = 0, smax = 0, n = 0, sm_count = 148;
-    uint64_t N = 0;
+    uint64_t N = 0, Q = 0, rows = 0;
     cudaStream_t st = nullptr;
-    int8_t* d_limbs = nullptr;      // [192][N]
-    int32_t* d_heights = nullptr;   // scratch [N]
+    uint32_t* d_snap = nullptr;     // [smax][2][Q] X-slope quadrants
+    int2* d_rows = nullptr;         // [smax][rows] {b(y), z(y)}
     uint32_t* d_tmp = nullptr;      // scratch lattice for host snapshots
-    unsigned long long* d_sums = nullptr;  // [64][3] limb sums + error flag
-    unsigned long long* d_g = nullptr;     // 64 x 64 int64 (CUDA-core path)
+    unsigned long long* d_g = nullptr;  // 64 x 64 int64 (CUDA-core path)
     std::vector<int64_t> shift;     // c_s
+    std::vector<int64_t> s1v;       // sum (h_s - c_s)
     AnalysisScratch an{};
     GramTC tc{};
+
+    SlopeSnapGeom geom() const { return SlopeSnapGeom{d_snap, d_rows, Q, rows, lx, n}; }
 };
 
 #define GCHECK(g)                                                       \
@@ -185,15 +148,15 @@ extern "C" kpzb_status kpzb_gram_create(kpzb_gram** out, int lx, int ly, int max
     };
     if ((e = cudaStreamCreateWithFlags(&g->st, cudaStreamNonBlocking)) != cudaSuccess)
         return bail(cuda_fail(e, "cudaStreamCreate"));
-    // 192 limb rows always: rows of absent snapshots stay zero and add nothing
-    if ((e = cudaMalloc(&g->d_limbs, 192 * g->N)) != cudaSuccess) return bail(cuda_fail(e, "cudaMalloc(limbs)"));
-    if ((e = cudaMemset(g->d_limbs, 0, 192 * g->N)) != cudaSuccess) return bail(cuda_fail(e, "memset limbs"));
-    if ((e = cudaMalloc(&g->d_heights, g->N * 4)) != cudaSuccess) return bail(cuda_fail(e, "cudaMalloc(heights)"));
-    if ((e = cudaMalloc(&g->d_sums, (64 * 3 + 2) * 8)) != cudaSuccess) return bail(cuda_fail(e, "cudaMalloc(sums)"));
-    if ((e = cudaMemset(g->d_sums, 0, (64 * 3 + 2) * 8)) != cudaSuccess) return bail(cuda_fail(e, "memset sums"));
+    g->Q = g->N >> 6;
+    g->rows = 1ull << ly;
+    if ((e = cudaMalloc(&g->d_snap, (size_t)max_snapshots * 2 * g->Q * 4)) != cudaSuccess)
+        return bail(cuda_fail(e, "cudaMalloc(snapshots)"));
+    if ((e = cudaMalloc(&g->d_rows, (size_t)max_snapshots * g->rows * sizeof(int2))) != cudaSuccess)
+        return bail(cuda_fail(e, "cudaMalloc(snapshot rows)"));
     if ((e = cudaMalloc(&g->d_g, 64 * 64 * 8)) != cudaSuccess) return bail(cuda_fail(e, "cudaMalloc(G)"));
     if ((e = analysis_alloc(&g->an, ly)) != cudaSuccess) return bail(cuda_fail(e, "analysis_alloc"));
-    kpzb_status s = gram_tc_setup(&g->tc, g->d_limbs, g->N, g->sm_count);
+    kpzb_status s = gram_tc_setup(&g->tc, g->N, g->sm_count);
     if (s != KPZB_OK) return bail(s);
     *out = g;
     return KPZB_OK;
@@ -205,10 +168,9 @@ extern "C" kpzb_status kpzb_gram_destroy(kpzb_gram* g)
     cudaSetDevice(g->device);
     if (g->st) cudaStreamSynchronize(g->st);
     gram_tc_free(&g->tc);
-    cudaFree(g->d_limbs);
-    cudaFree(g->d_heights);
+    cudaFree(g->d_snap);
+    cudaFree(g->d_rows);
     cudaFree(g->d_tmp);
-    cudaFree(g->d_sums);
     cudaFree(g->d_g);
     if (g->an.rowinfo) analysis_free(&g->an);
     if (g->st) cudaStreamDestroy(g->st);
@@ -224,22 +186,24 @@ extern "C" kpzb_status kpzb_gram_add_device(kpzb_gram* g, const uint32_t* d_cbbi
     if (!d_cbbit) return fail(KPZB_EINVAL, "null lattice");
     if (g->n >= g->smax) return fail(KPZB_ESTATE, "snapshot capacity reached");
     const int s = g->n;
-    // the snapshot's mean fixes its integer shift c_s = floor(<h>)
+    // the snapshot's mean fixes its integer shift c_s = floor(<h>); the walk that measures it
+    // leaves the row starts and row sums in the analysis scratch
     MomentsOut m;
     GCU(analysis_moments(d_cbbit, nullptr, g->lx, g->ly, &g->an, &m, g->st), "snapshot moments");
     const long double mean = (long double)m.s1 / (long double)g->N;
     const int64_t c = (int64_t)std::floor((double)mean);
-    if (m.hmax - c > 1000000 || c - m.hmin > 1000000) return fail(KPZB_EINVAL, "heights exceed three int8 limbs");
-    GCU(analysis_heights(d_cbbit, g->lx, g->ly, &g->an, g->d_heights, g->st), "snapshot heights");
-    const int grid = (int)std::min<uint64_t>(g->N / 16 / 256 + 1, (uint64_t)g->sm_count * 8);
-    limb_kernel<<<grid, 256, 0, g->st>>>(g->d_heights, g->N, (int32_t)c, g->d_limbs, s, g->d_sums + 3 * s,
-                                         reinterpret_cast<unsigned int*>(g->d_sums + 192));
-    GCU(cudaGetLastError(), "limb_kernel");
-    unsigned long long flag = 0;
-    GCU(cudaMemcpyAsync(&flag, g->d_sums + 192, 8, cudaMemcpyDeviceToHost, g->st), "limb flag");
-    GCU(cudaStreamSynchronize(g->st), "limb sync");
-    if (flag) return fail(KPZB_EINVAL, "heights exceed three int8 limbs");
+    if (m.hmin - c < -1056832 || m.hmax - c > 1040447) return fail(KPZB_EINVAL, "heights exceed three int8 limbs");
+    // the two X-slope quadrants (sublattice 0 at word 0, sublattice 1 at 2Q)
+    uint32_t* dst = g->d_snap + (uint64_t)s * 2 * g->Q;
+    GCU(cudaMemcpyAsync(dst, d_cbbit, g->Q * 4, cudaMemcpyDeviceToDevice, g->st), "snapshot copy");
+    GCU(cudaMemcpyAsync(dst + g->Q, d_cbbit + 2 * g->Q, g->Q * 4, cudaMemcpyDeviceToDevice, g->st), "snapshot copy");
+    const int grid = (int)std::min<uint64_t>(g->rows / 256 + 1, (uint64_t)g->sm_count * 4);
+    gram_rows_kernel<<<grid, 256, 0, g->st>>>(g->an.rowstart, g->an.rowinfo, g->rows, c,
+                                             g->d_rows + (uint64_t)s * g->rows);
+    GCU(cudaGetLastError(), "gram_rows_kernel");
+    GCU(cudaStreamSynchronize(g->st), "snapshot sync");
     g->shift.push_back(c);
+    g->s1v.push_back(m.s1 - (int64_t)g->N * c);
     g->n++;
     return KPZB_OK;
 }
@@ -277,19 +241,18 @@ extern "C" kpzb_status kpzb_gram_compute(kpzb_gram* g, int method, int64_t* G, i
     if (method != 0 && method != 1) return fail(KPZB_EINVAL, "method 0 (tensor) or 1 (int64)");
     const int n = g->n;
     if (n == 0) return KPZB_OK;
-    std::vector<unsigned long long> sums(64 * 3);
-    GCU(cudaMemcpyAsync(sums.data(), g->d_sums, 64 * 3 * 8, cudaMemcpyDeviceToHost, g->st), "limb sums");
-    std::vector<int64_t> gv(64 * 64, 0), s1v(64, 0);
+    std::vector<int64_t> gv(64 * 64, 0), s1v(g->s1v);
+    const SlopeSnapGeom geo = g->geom();
     if (method == 1) {
         GCU(cudaMemsetAsync(g->d_g, 0, 64 * 64 * 8, g->st), "memset G");
         const int grid = (int)std::min<uint64_t>(g->N / G64_KC, (uint64_t)g->sm_count * 4);
-        gram_int64_kernel<<<grid, 256, 0, g->st>>>(g->d_limbs, g->N, n, g->d_g);
+        gram_int64_kernel<<<grid, 256, 0, g->st>>>(geo, g->N / G64_KC, g->d_g);
         GCU(cudaGetLastError(), "gram_int64_kernel");
         GCU(cudaMemcpyAsync(gv.data(), g->d_g, 64 * 64 * 8, cudaMemcpyDeviceToHost, g->st), "G copy");
         GCU(cudaStreamSynchronize(g->st), "gram sync");
     } else {
         std::vector<int64_t> gl(192 * 192);
-        kpzb_status st = gram_tc_run(&g->tc, g->N, gl.data(), g->st);
+        kpzb_status st = gram_tc_run(&g->tc, geo, g->N, gl.data(), g->st);
         if (st != KPZB_OK) return st;
         // sum v_s v_t = sum_{a,b} 128^(a+b) Glimb[a*64+s][b*64+t]; the tensor kernel fills
         // the upper triangle of the limb Gram (row <= col), the rest by symmetry
@@ -302,8 +265,6 @@ extern "C" kpzb_status kpzb_gram_compute(kpzb_gram* g, int method, int64_t* G, i
                 gv[s * 64 + t] = acc;
             }
     }
-    for (int s = 0; s < n; ++s)
-        s1v[s] = (int64_t)sums[3 * s] + 128 * (int64_t)sums[3 * s + 1] + 16384 * (int64_t)sums[3 * s + 2];
     finish(g, gv, s1v, G, S1);
     return KPZB_OK;
 }

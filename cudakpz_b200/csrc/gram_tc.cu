@@ -1,22 +1,25 @@
-// gram_tc.cu -- exact int8 limb Gram A A^T (A: 192 x N, K-tile-major) on tcgen05 tensor cores.
+// gram_tc.cu -- exact limb Gram of the stored snapshots on tcgen05 tensor cores (sm_100a).
 //
-// One persistent CTA per SM takes a contiguous K range.  Warp 0 streams 192-row x 128-byte
-// K tiles of A -- each a contiguous 24 KB block of the tile-major limb matrix -- into a ring
-// of shared-memory stages with 2D TMA (SWIZZLE_128B, local HBM only, no multicast); warp 1 allocates 256 TMEM columns and issues, per 32-byte K step,
+// One persistent CTA per SM takes a contiguous range of 128-site K tiles.  Eight producer warps
+// rebuild each tile's heights from the snapshots' slope bits (gram_slope.cuh: 64 snapshots x 4
+// lanes, 32 sites a lane), shift them by the snapshot's integer mean and split them into three
+// signed int8 limbs, written straight into a shared-memory stage in the K-major SWIZZLE_128B
+// layout the MMA descriptors expect (limb row a * 64 + s, 128 bytes a row, 16-byte chunk c of
+// row r at chunk position c ^ (r mod 8)); a fence.proxy.async hands the stage to the tensor
+// core.  Warp 0 owns 256 TMEM columns and issues, per 32-byte K step,
 //   D1[0:128, 0:192]   += A[0:128]   . A[0:192]^T   (M=128, N=192)
 //   D2[0:128, 0:64]    += A[64:192]  . A[128:192]^T (M=128, N=64)
 // (kind::i8, signed, int32 accumulators in TMEM); together they cover every (row <= col)
 // entry of the symmetric 192 x 192 limb Gram.  Every 2^18 K elements (|l l'| <= 2^12, so
-// the int32 sums stay below 2^30) warps 2-5 read the accumulators with tcgen05.ld and add
+// the int32 sums stay below 2^30) warps 1-4 read the accumulators with tcgen05.ld and add
 // them to the CTA's int64 partial in global memory; a final kernel sums the partials.
-// Every mbarrier wait is bounded: on expiry the kernel raises a flag, stops issuing work,
-// drains what it issued, frees its TMEM and returns.
-#include <cuda.h>
-#include <cudaTypedefs.h>
-
+// Only the slope bits cross HBM: 16 bytes per snapshot per tile instead of 384 bytes of
+// stored limbs.  Every mbarrier wait is bounded: on expiry the kernel raises a flag, stops
+// issuing work, drains what it issued, frees its TMEM and returns.
 #include <algorithm>
 #include <cstring>
 
+#include "gram_slope.cuh"
 #include "kpzb_api_internal.h"
 #include "kpzb_gram.h"
 #include "scabit_band.cuh"
@@ -24,11 +27,13 @@
 namespace kpzb {
 
 constexpr int TC_ROWS = 192;
-constexpr int TC_KT = 128;                        // K bytes per tile (one 128B swizzle row)
+constexpr int TC_KT = GS_TILE;                    // K bytes per tile (one 128B swizzle row)
 constexpr int TC_STAGE = TC_ROWS * TC_KT;         // 24 KB
 constexpr int TC_STAGES = 6;
 constexpr int TC_WINDOW = (1 << 18) / TC_KT;      // K tiles per int32 accumulation window
-constexpr int TC_THREADS = 192;
+constexpr int TC_PRODUCERS = 256;                 // 64 snapshots x 4 quarter tiles
+constexpr int TC_PROD_WARP0 = 5;                  // warps 5..12 produce, 1..4 flush, 0 issues
+constexpr int TC_THREADS = TC_PROD_WARP0 * 32 + TC_PRODUCERS;
 constexpr int TC_COLS = 256;                      // TMEM columns: D1 0..191, D2 192..255
 constexpr uint32_t TC_SPIN = 1u << 26;
 
@@ -55,13 +60,17 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity
     return true;
 }
 
-__device__ __forceinline__ void tma_load_2d(void* dst, const void* tmap, int x, int y, uint64_t* bar)
+// four values' low bytes, first in the lowest byte
+__device__ __forceinline__ uint32_t pack4(int32_t a, int32_t b, int32_t c, int32_t d)
 {
-    asm volatile(
-        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(
-            smem_u32(dst)),
-        "l"(tmap), "r"(x), "r"(y), "r"(smem_u32(bar))
-        : "memory");
+    return __byte_perm(__byte_perm((uint32_t)a, (uint32_t)b, 0x0040), __byte_perm((uint32_t)c, (uint32_t)d, 0x0040),
+                       0x5410);
+}
+
+// the 16-byte chunk `chunk` (sites 16 chunk .. +15) of limb row r in a SWIZZLE_128B stage
+__device__ __forceinline__ void put_chunk(uint8_t* stage, int r, int chunk, uint4 v)
+{
+    *reinterpret_cast<uint4*>(stage + r * TC_KT + ((chunk ^ (r & 7)) << 4)) = v;
 }
 
 __device__ __forceinline__ void umma_i8(uint32_t dtmem, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
@@ -82,8 +91,7 @@ __device__ __forceinline__ void umma_commit(uint64_t* bar)
 }
 
 __global__ void __launch_bounds__(TC_THREADS, 1)
-gram_tc_kernel(const __grid_constant__ CUtensorMap tmap, uint64_t nkt, long long* __restrict__ part,
-               unsigned int* __restrict__ err)
+gram_tc_kernel(const SlopeSnapGeom g, uint64_t nkt, long long* __restrict__ part, unsigned int* __restrict__ err)
 {
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     __shared__ __align__(8) uint64_t full[TC_STAGES], empty[TC_STAGES], accf, acce;
@@ -101,14 +109,14 @@ gram_tc_kernel(const __grid_constant__ CUtensorMap tmap, uint64_t nkt, long long
     if (threadIdx.x == 0) {
         abort_flag = 0;
         for (int s = 0; s < TC_STAGES; ++s) {
-            mbar_init(&full[s], 1);
+            mbar_init(&full[s], TC_PRODUCERS);
             mbar_init(&empty[s], 1);
         }
         mbar_init(&accf, 1);
         mbar_init(&acce, 128);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
-    if (warp == 1) {
+    if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_base)),
                      "r"(TC_COLS));
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
@@ -118,25 +126,78 @@ gram_tc_kernel(const __grid_constant__ CUtensorMap tmap, uint64_t nkt, long long
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const uint32_t tbase = tmem_base;
 
-    if (warp == 0) {
-        if (lane == 0) {
-            uint64_t issued = 0;
-            for (uint64_t i = 0; i < nloc; ++i) {
-                const int s = (int)(i % TC_STAGES);
-                const uint32_t ph = (uint32_t)((i / TC_STAGES) & 1);
-                if (abort_flag || !mbar_wait_bounded(&empty[s], ph ^ 1u)) {
-                    abort_flag = 1;
-                    break;
-                }
-                mbar_expect_tx(&full[s], TC_STAGE);
-                tma_load_2d(smem + s * TC_STAGE, &tmap, 0, (int)((kt0 + i) * TC_ROWS), &full[s]);
-                issued = i + 1;
+    if (warp >= TC_PROD_WARP0) {
+        // producers: lane quad of snapshot s, lane qt of the quad takes a quarter of each tile
+        const int p = threadIdx.x - TC_PROD_WARP0 * 32;
+        const int s = p >> 2, qt = p & 3;
+        SlopeCursor cur;
+        slope_cursor_init(cur, s, qt);
+        SlopeQuarter next = nloc ? slope_quarter_load(g, cur, kt0) : SlopeQuarter{};
+        for (uint64_t i = 0; i < nloc; ++i) {
+            const uint64_t t = kt0 + i;
+            const SlopeQuarter q = next;
+            if (i + 1 < nloc) next = slope_quarter_load(g, cur, t + 1);  // one tile ahead
+            int32_t v[32], lo, hi;
+            slope_quarter_heights(g, cur, t, q, v, lo, hi);
+            const int st = (int)(i % TC_STAGES);
+            const uint32_t ph = (uint32_t)((i / TC_STAGES) & 1);
+            // every lane of the warp waits, and the warp leaves together
+            const bool ok = !abort_flag && mbar_wait_bounded(&empty[st], ph ^ 1u);
+            if (!__all_sync(0xFFFFFFFFu, ok)) {
+                abort_flag = 1;
+                break;
             }
-            // copies still in flight land before the CTA retires (bounded)
-            for (uint64_t j = issued > TC_STAGES ? issued - TC_STAGES : 0; j < issued; ++j)
-                mbar_wait_bounded(&full[j % TC_STAGES], (uint32_t)((j / TC_STAGES) & 1));
+            uint8_t* stage = smem + st * TC_STAGE;
+            if (__all_sync(0xFFFFFFFFu, lo >= -64 && hi <= 63)) {
+                // every value is its own low limb; the two upper limbs are zero
+#pragma unroll
+                for (int c = 0; c < 2; ++c) {
+                    const int b = 16 * c;
+                    put_chunk(stage, s, 2 * qt + c,
+                              make_uint4(pack4(v[b], v[b + 1], v[b + 2], v[b + 3]),
+                                         pack4(v[b + 4], v[b + 5], v[b + 6], v[b + 7]),
+                                         pack4(v[b + 8], v[b + 9], v[b + 10], v[b + 11]),
+                                         pack4(v[b + 12], v[b + 13], v[b + 14], v[b + 15])));
+                    put_chunk(stage, 64 + s, 2 * qt + c, make_uint4(0u, 0u, 0u, 0u));
+                    put_chunk(stage, 128 + s, 2 * qt + c, make_uint4(0u, 0u, 0u, 0u));
+                }
+            } else {
+                // balanced base-128 digits v = l0 + 128 l1 + 16384 l2, l_a in [-64, 63]
+                int32_t l1v[32], l2v[32];
+#pragma unroll
+                for (int j = 0; j < 32; ++j) {
+                    const int32_t l0 = ((v[j] + 64) & 127) - 64;
+                    const int32_t w1 = (v[j] - l0) >> 7;
+                    const int32_t l1 = ((w1 + 64) & 127) - 64;
+                    v[j] = l0;
+                    l1v[j] = l1;
+                    l2v[j] = (w1 - l1) >> 7;
+                }
+#pragma unroll
+                for (int c = 0; c < 2; ++c) {
+                    const int b = 16 * c;
+                    put_chunk(stage, s, 2 * qt + c,
+                              make_uint4(pack4(v[b], v[b + 1], v[b + 2], v[b + 3]),
+                                         pack4(v[b + 4], v[b + 5], v[b + 6], v[b + 7]),
+                                         pack4(v[b + 8], v[b + 9], v[b + 10], v[b + 11]),
+                                         pack4(v[b + 12], v[b + 13], v[b + 14], v[b + 15])));
+                    put_chunk(stage, 64 + s, 2 * qt + c,
+                              make_uint4(pack4(l1v[b], l1v[b + 1], l1v[b + 2], l1v[b + 3]),
+                                         pack4(l1v[b + 4], l1v[b + 5], l1v[b + 6], l1v[b + 7]),
+                                         pack4(l1v[b + 8], l1v[b + 9], l1v[b + 10], l1v[b + 11]),
+                                         pack4(l1v[b + 12], l1v[b + 13], l1v[b + 14], l1v[b + 15])));
+                    put_chunk(stage, 128 + s, 2 * qt + c,
+                              make_uint4(pack4(l2v[b], l2v[b + 1], l2v[b + 2], l2v[b + 3]),
+                                         pack4(l2v[b + 4], l2v[b + 5], l2v[b + 6], l2v[b + 7]),
+                                         pack4(l2v[b + 8], l2v[b + 9], l2v[b + 10], l2v[b + 11]),
+                                         pack4(l2v[b + 12], l2v[b + 13], l2v[b + 14], l2v[b + 15])));
+                }
+            }
+            // the generic-proxy writes become visible to the tensor core, then the stage is full
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(&full[st])) : "memory");
         }
-    } else if (warp == 1) {
+    } else if (warp == 0) {
         if (lane == 0) {
             const uint32_t id1 = idesc_i8(128, 192), id2 = idesc_i8(128, 64);
             for (uint64_t i = 0; i < nloc && !abort_flag; ++i) {
@@ -165,7 +226,7 @@ gram_tc_kernel(const __grid_constant__ CUtensorMap tmap, uint64_t nkt, long long
             }
         }
     } else {
-        // epilogue: warps 2..5 own TMEM lane quarters (warp % 4)
+        // epilogue: warps 1..4 own TMEM lane quarters (warp % 4)
         const int q = warp & 3;
         const int r = 32 * q + lane;  // accumulator row (TMEM lane)
         long long* prow1 = part + (uint64_t)blockIdx.x * TC_ROWS * TC_ROWS + (uint64_t)r * TC_ROWS;
@@ -205,7 +266,7 @@ gram_tc_kernel(const __grid_constant__ CUtensorMap tmap, uint64_t nkt, long long
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     if (abort_flag && threadIdx.x == 0) atomicExch(err, 1u);
-    if (warp == 1) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tbase), "r"(TC_COLS));
+    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tbase), "r"(TC_COLS));
 }
 
 __global__ void gram_reduce_kernel(const long long* __restrict__ part, int grid, long long* __restrict__ out)
@@ -217,26 +278,11 @@ __global__ void gram_reduce_kernel(const long long* __restrict__ part, int grid,
     }
 }
 
-kpzb_status gram_tc_setup(GramTC* tc, const int8_t* d_limbs, uint64_t N, int sm_count)
+kpzb_status gram_tc_setup(GramTC* tc, uint64_t N, int sm_count)
 {
     if (N % TC_KT || N > (1ull << 30)) return fail(KPZB_EINVAL, "gram: N must be a multiple of 128, <= 2^30");
-    PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
-    cudaDriverEntryPointQueryResult q;
-    cudaError_t e = cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", reinterpret_cast<void**>(&encode),
-                                            cudaEnableDefault, &q);
-    if (e != cudaSuccess || !encode || q != cudaDriverEntryPointSuccess)
-        return fail(KPZB_ECUDA, "cuTensorMapEncodeTiled unavailable");
-    // the tile-major matrix as 2D: 128-byte rows, 192 rows per K tile, N / 128 tiles
-    const cuuint64_t dims[2] = {(cuuint64_t)TC_KT, (cuuint64_t)TC_ROWS * (N / TC_KT)};
-    const cuuint64_t strides[1] = {(cuuint64_t)TC_KT};  // bytes between rows
-    const cuuint32_t box[2] = {(cuuint32_t)TC_KT, (cuuint32_t)TC_ROWS};
-    const cuuint32_t estr[2] = {1, 1};
-    CUtensorMap* map = reinterpret_cast<CUtensorMap*>(tc->tmap);
-    const CUresult r = encode(map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, const_cast<int8_t*>(d_limbs), dims, strides,
-                              box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
-                              CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-    if (r != CUDA_SUCCESS) return fail(KPZB_ECUDA, "cuTensorMapEncodeTiled failed");
     tc->grid = sm_count;
+    cudaError_t e;
     if ((e = cudaMalloc(&tc->d_part, (size_t)tc->grid * TC_ROWS * TC_ROWS * 8)) != cudaSuccess)
         return cuda_fail(e, "cudaMalloc(gram partials)");
     if ((e = cudaMalloc(&tc->d_out, TC_ROWS * TC_ROWS * 8 + 64)) != cudaSuccess) return cuda_fail(e, "cudaMalloc(gram)");
@@ -257,16 +303,15 @@ void gram_tc_free(GramTC* tc)
     tc->ready = false;
 }
 
-kpzb_status gram_tc_run(GramTC* tc, uint64_t N, int64_t* out, cudaStream_t st)
+kpzb_status gram_tc_run(GramTC* tc, const SlopeSnapGeom& g, uint64_t N, int64_t* out, cudaStream_t st)
 {
     if (!tc->ready) return fail(KPZB_ESTATE, "gram tensor path not set up");
     cudaError_t e;
     if ((e = cudaMemsetAsync(tc->d_part, 0, (size_t)tc->grid * TC_ROWS * TC_ROWS * 8, st)) != cudaSuccess)
         return cuda_fail(e, "memset partials");
     if ((e = cudaMemsetAsync(tc->d_err, 0, 4, st)) != cudaSuccess) return cuda_fail(e, "memset flag");
-    const CUtensorMap* map = reinterpret_cast<const CUtensorMap*>(tc->tmap);
     gram_tc_kernel<<<tc->grid, TC_THREADS, TC_STAGES * TC_STAGE + 1024, st>>>(
-        *map, N / TC_KT, reinterpret_cast<long long*>(tc->d_part), tc->d_err);
+        g, N / TC_KT, reinterpret_cast<long long*>(tc->d_part), tc->d_err);
     if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, "gram_tc_kernel");
     gram_reduce_kernel<<<64, 256, 0, st>>>(reinterpret_cast<const long long*>(tc->d_part), tc->grid,
                                           reinterpret_cast<long long*>(tc->d_out));

@@ -115,3 +115,39 @@ def test_gram_capacity(kpzb):
         g.add_host(w)
     assert e.value.status == 5
     g.close()
+
+
+@pytest.mark.parametrize("method", [0, 1])
+@pytest.mark.parametrize("lx,ly,n", [(8, 6, 3), (12, 4, 64), (9, 11, 17)])
+def test_gram_tile_rows_and_partial_counts(kpzb, oracle, method, lx, ly, n):
+    """Row lengths of two to 32 tiles, flat lattices and tall ones, and snapshot counts that
+    leave most of the 64 lane quads without a snapshot: the slope walk across tiles, the
+    per-CTA tile ranges that start inside a row, and the zero rows of absent snapshots."""
+    snaps = snapshots(kpzb, lx, ly, n, p=0.55, q=0.45, step=2, seed=13)
+    g = kpzb.Gram(lx, ly, max_snapshots=64)
+    for w in snaps:
+        g.add_host(w)
+    G, S1 = g.compute(method)
+    Gr, S1r = oracle_gram(oracle, snaps, lx, ly)
+    assert np.array_equal(S1, S1r)
+    assert np.array_equal(G, Gr), np.argwhere(G != Gr)[:5]
+    g.close()
+
+
+def test_gram_mixed_limb_paths(kpzb, oracle):
+    """Snapshots of small heights (one limb) beside steep ones (all three): a tile's warps take
+    the one-limb path only when every value of the warp fits, both paths in one Gram."""
+    lx, ly = 10, 8
+    snaps = snapshots(kpzb, lx, ly, 4, step=3)
+    rng = np.random.default_rng(5)
+    for i in range(4):
+        bits = rng.random((oracle.size_words(lx, ly), 32)) < (0.8 if i % 2 else 0.25)
+        snaps.append(np.packbits(bits, axis=1, bitorder="little").view(np.uint32).ravel().copy())
+    g = kpzb.Gram(lx, ly, max_snapshots=8)
+    for w in snaps:
+        g.add_host(w)
+    Gr, S1r = oracle_gram(oracle, snaps, lx, ly)
+    for method in (0, 1):
+        G, S1 = g.compute(method)
+        assert np.array_equal(G, Gr) and np.array_equal(S1, S1r), method
+    g.close()

@@ -44,20 +44,23 @@ __device__ __forceinline__ void slope_cursor_init(SlopeCursor& c, int s, int qt)
     c.pre = 0;
 }
 
-// The raw quarter words of tile t (loads only; issued ahead of slope_quarter_heights).
+// The raw quarter words of tile t.
 struct SlopeQuarter {
-    uint32_t e, o;  // X bits of even x (sublattice y & 1) and of odd x, this lane's 16 bits at bit 0
+    uint32_t e, o;  // the X words holding this lane's 16 even-x bits (sublattice y & 1) and odd-x bits
     int2 bz;        // {b(y), z(y)}
 };
 
-__device__ __forceinline__ SlopeQuarter slope_quarter_load(const SlopeSnapGeom& g, const SlopeCursor& c, uint64_t t)
+// where the quarter's words lie (for loads issued ahead, e.g. by cp.async); lanes of absent
+// snapshots get null pointers
+struct SlopeQuarterAddr {
+    const uint32_t* e;
+    const uint32_t* o;
+    const int2* bz;
+};
+
+__device__ __forceinline__ SlopeQuarterAddr slope_quarter_addr(const SlopeSnapGeom& g, const SlopeCursor& c, uint64_t t)
 {
-    SlopeQuarter q;
-    if (c.s >= g.n) {
-        q.e = q.o = 0u;
-        q.bz = make_int2(0, 0);
-        return q;
-    }
+    if (c.s >= g.n) return SlopeQuarterAddr{nullptr, nullptr, nullptr};
     const int tpr_lg = g.lx - 7;  // log2 tiles per row
     const uint64_t y = t >> tpr_lg;
     const uint32_t x0 = (uint32_t)(t & ((1ull << tpr_lg) - 1)) << 7;
@@ -65,11 +68,15 @@ __device__ __forceinline__ SlopeQuarter slope_quarter_load(const SlopeSnapGeom& 
     const uint64_t w = y * Wr + (x0 >> 6) + (uint64_t)(c.qt >> 1);
     const uint32_t* base = g.snap + (uint64_t)c.s * 2 * g.Q;
     const int se = (int)(y & 1);
-    const int sh = 16 * (c.qt & 1);
-    q.e = (__ldg(base + (uint64_t)se * g.Q + w) >> sh) & 0xFFFFu;
-    q.o = (__ldg(base + (uint64_t)(se ^ 1) * g.Q + w) >> sh) & 0xFFFFu;
-    q.bz = __ldg(g.rows + (uint64_t)c.s * g.nrows + y);
-    return q;
+    return SlopeQuarterAddr{base + (uint64_t)se * g.Q + w, base + (uint64_t)(se ^ 1) * g.Q + w,
+                            g.rows + (uint64_t)c.s * g.nrows + y};
+}
+
+__device__ __forceinline__ SlopeQuarter slope_quarter_load(const SlopeSnapGeom& g, const SlopeCursor& c, uint64_t t)
+{
+    const SlopeQuarterAddr a = slope_quarter_addr(g, c, t);
+    if (!a.e) return SlopeQuarter{0u, 0u, make_int2(0, 0)};
+    return SlopeQuarter{__ldg(a.e), __ldg(a.o), __ldg(a.bz)};
 }
 
 // Count of X-slope bits of row y in [1, x0) for the cursor's snapshot, from the row's words
@@ -107,6 +114,9 @@ __device__ __forceinline__ void slope_quarter_heights(const SlopeSnapGeom& g, Sl
     } else if (c.last_tile == ~0ull || t != c.last_tile + 1) {
         c.pre = slope_row_prefix(g, c, t);
     }
+    const int sh = 16 * (c.qt & 1);
+    q.e = (q.e >> sh) & 0xFFFFu;
+    q.o = (q.o >> sh) & 0xFFFFu;
     const bool first = x0 == 0 && c.qt == 0;
     if (first) q.e &= ~1u;  // x = 0 closes the row in the walk; its bit is not counted here
     const int32_t cnt = __popc(q.e) + __popc(q.o);
@@ -120,15 +130,24 @@ __device__ __forceinline__ void slope_quarter_heights(const SlopeSnapGeom& g, Sl
     const int32_t total = __shfl_sync(0xFFFFFFFFu, incl, (lane & ~3) | 3);
     const int32_t excl = incl - cnt;
     const int32_t xs = (int32_t)x0 + 32 * c.qt;
-    int32_t acc = q.bz.x + 2 * (c.pre + excl) - xs + 1;
+    const int32_t acc0 = q.bz.x + 2 * (c.pre + excl) - xs + 1;
+    // four independent chains of 8 sites, each started from the count of the bits before it
+    // (sites 8j .. 8j+7 hold even-x bits 4j .. 4j+3 and odd-x bits 4j .. 4j+3)
 #pragma unroll
-    for (int i = 0; i < 32; ++i) {
-        const uint32_t word = (i & 1) ? q.o : q.e;
-        const int32_t bit = (int32_t)((word >> (i >> 1)) & 1u);
-        acc += 2 * bit - 1;
-        v[i] = acc;
+    for (int j = 0; j < 4; ++j) {
+        const uint32_t below = (1u << (4 * j)) - 1u;
+        int32_t acc = acc0 + 2 * (__popc(q.e & below) + __popc(q.o & below)) - 8 * j;
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            const int i = 8 * j + k;
+            const uint32_t word = (i & 1) ? q.o : q.e;
+            const int32_t bit = (int32_t)((word >> (i >> 1)) & 1u);
+            acc += 2 * bit - 1;
+            v[i] = acc;
+        }
     }
-    lo = q.bz.x + 2 * (c.pre + excl) - xs + 1 - 32;  // every step is +-1
+    const int32_t acc = acc0;
+    lo = acc - 32;  // every step is +-1
     hi = lo + 64;
     if (first) {
         v[0] = q.bz.y;

@@ -35,6 +35,8 @@ constexpr int TC_PRODUCERS = 256;                 // 64 snapshots x 4 quarter ti
 constexpr int TC_PROD_WARP0 = 5;                  // warps 5..12 produce, 1..4 flush, 0 issues
 constexpr int TC_THREADS = TC_PROD_WARP0 * 32 + TC_PRODUCERS;
 constexpr int TC_COLS = 256;                      // TMEM columns: D1 0..191, D2 192..255
+constexpr int TC_PREFETCH = 8;                    // tiles of slope words in flight per producer
+constexpr int TC_SMEM = TC_STAGES * TC_STAGE + TC_PREFETCH * TC_PRODUCERS * 16 + 1024;
 constexpr uint32_t TC_SPIN = 1u << 26;
 
 // UMMA instruction descriptor, kind::i8: S32 accumulate (bits 4-5 = 2), signed A and B
@@ -97,7 +99,12 @@ gram_tc_kernel(const SlopeSnapGeom g, uint64_t nkt, long long* __restrict__ part
     __shared__ __align__(8) uint64_t full[TC_STAGES], empty[TC_STAGES], accf, acce;
     __shared__ uint32_t tmem_base;
     __shared__ volatile int abort_flag;
+    // per stage and producer warp: 1 when the warp wrote non-zero upper limbs (rows 64..191);
+    // every warp writes its byte for every tile, before its arrival on the stage
+    __shared__ __align__(8) uint8_t upper[TC_STAGES][8];
     uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    // per producer lane, TC_PREFETCH slots of {e word, o word, b, z} filled by cp.async
+    uint4* ring = reinterpret_cast<uint4*>(smem + TC_STAGES * TC_STAGE);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 
     // contiguous K-tile range of this CTA
@@ -109,7 +116,7 @@ gram_tc_kernel(const SlopeSnapGeom g, uint64_t nkt, long long* __restrict__ part
     if (threadIdx.x == 0) {
         abort_flag = 0;
         for (int s = 0; s < TC_STAGES; ++s) {
-            mbar_init(&full[s], TC_PRODUCERS);
+            mbar_init(&full[s], TC_PRODUCERS / 32);  // one arrival per producer warp
             mbar_init(&empty[s], 1);
         }
         mbar_init(&accf, 1);
@@ -132,23 +139,46 @@ gram_tc_kernel(const SlopeSnapGeom g, uint64_t nkt, long long* __restrict__ part
         const int s = p >> 2, qt = p & 3;
         SlopeCursor cur;
         slope_cursor_init(cur, s, qt);
-        SlopeQuarter next = nloc ? slope_quarter_load(g, cur, kt0) : SlopeQuarter{};
+        // tile t's words into slot t mod TC_PREFETCH, one copy group per tile (empty groups
+        // past the range and for absent snapshots keep the group count uniform)
+        auto issue = [&](uint64_t i) {
+            if (i < nloc) {
+                const SlopeQuarterAddr a = slope_quarter_addr(g, cur, kt0 + i);
+                if (a.e) {
+                    uint4* slot = ring + (i % TC_PREFETCH) * TC_PRODUCERS + p;
+                    const uint32_t d = smem_u32(slot);
+                    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(d), "l"(a.e) : "memory");
+                    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(d + 4), "l"(a.o) : "memory");
+                    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(d + 8), "l"(a.bz) : "memory");
+                }
+            }
+            asm volatile("cp.async.commit_group;" ::: "memory");
+        };
+        for (int d = 0; d < TC_PREFETCH; ++d) issue((uint64_t)d);
         for (uint64_t i = 0; i < nloc; ++i) {
             const uint64_t t = kt0 + i;
-            const SlopeQuarter q = next;
-            if (i + 1 < nloc) next = slope_quarter_load(g, cur, t + 1);  // one tile ahead
+            asm volatile("cp.async.wait_group %0;" ::"n"(TC_PREFETCH - 1) : "memory");
+            SlopeQuarter q{0u, 0u, make_int2(0, 0)};
+            if (s < g.n) {
+                const uint4 r = ring[(i % TC_PREFETCH) * TC_PRODUCERS + p];
+                q = SlopeQuarter{r.x, r.y, make_int2((int32_t)r.z, (int32_t)r.w)};
+            }
             int32_t v[32], lo, hi;
             slope_quarter_heights(g, cur, t, q, v, lo, hi);
+            issue(i + TC_PREFETCH);  // into the slot just read (its value is in registers)
             const int st = (int)(i % TC_STAGES);
             const uint32_t ph = (uint32_t)((i / TC_STAGES) & 1);
-            // every lane of the warp waits, and the warp leaves together
-            const bool ok = !abort_flag && mbar_wait_bounded(&empty[st], ph ^ 1u);
-            if (!__all_sync(0xFFFFFFFFu, ok)) {
+            // lane 0 waits for the stage to be free; the warp follows it, or leaves with it
+            bool ok = true;
+            if (lane == 0) ok = !abort_flag && mbar_wait_bounded(&empty[st], ph ^ 1u);
+            if (!__shfl_sync(0xFFFFFFFFu, ok, 0)) {
                 abort_flag = 1;
                 break;
             }
             uint8_t* stage = smem + st * TC_STAGE;
-            if (__all_sync(0xFFFFFFFFu, lo >= -64 && hi <= 63)) {
+            const bool one_limb = __all_sync(0xFFFFFFFFu, lo >= -64 && hi <= 63);
+            if (lane == 0) upper[st][warp - TC_PROD_WARP0] = one_limb ? 0 : 1;
+            if (one_limb) {
                 // every value is its own low limb; the two upper limbs are zero
 #pragma unroll
                 for (int c = 0; c < 2; ++c) {
@@ -193,13 +223,16 @@ gram_tc_kernel(const SlopeSnapGeom g, uint64_t nkt, long long* __restrict__ part
                                          pack4(l2v[b + 12], l2v[b + 13], l2v[b + 14], l2v[b + 15])));
                 }
             }
-            // the generic-proxy writes become visible to the tensor core, then the stage is full
+            // every writer makes its generic-proxy writes visible to the tensor core; the warp
+            // then reports its part of the stage with one arrival
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-            asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(&full[st])) : "memory");
+            __syncwarp();
+            if (lane == 0) asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(&full[st])) : "memory");
         }
+        asm volatile("cp.async.wait_all;" ::: "memory");  // no copy lands after the CTA retires
     } else if (warp == 0) {
         if (lane == 0) {
-            const uint32_t id1 = idesc_i8(128, 192), id2 = idesc_i8(128, 64);
+            const uint32_t id1 = idesc_i8(128, 192), id2 = idesc_i8(128, 64), id0 = idesc_i8(128, 64);
             for (uint64_t i = 0; i < nloc && !abort_flag; ++i) {
                 const int s = (int)(i % TC_STAGES);
                 const uint32_t ph = (uint32_t)((i / TC_STAGES) & 1);
@@ -215,11 +248,19 @@ gram_tc_kernel(const SlopeSnapGeom g, uint64_t nkt, long long* __restrict__ part
                 }
                 asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
                 const uint32_t sa = smem_u32(smem + s * TC_STAGE);
+                // a tile whose values all fit the low limb has zero rows 64..191: only the low
+                // limbs' 64 x 64 block is non-zero, and D1[0:128, 0:64] += A[0:128] . A[0:64]^T
+                // (rows 64..127 of A zero) adds exactly what the full products would
+                const bool full_tile = *reinterpret_cast<const volatile uint64_t*>(&upper[s][0]) != 0ull;
                 for (int kk = 0; kk < TC_KT / 32; ++kk) {
                     const uint32_t acc = (first && kk == 0) ? 0u : 1u;
-                    umma_i8(tbase, sdesc_sw128(sa + 32 * kk), sdesc_sw128(sa + 32 * kk), id1, acc);
-                    umma_i8(tbase + 192, sdesc_sw128(sa + 64 * TC_KT + 32 * kk),
-                            sdesc_sw128(sa + 128 * TC_KT + 32 * kk), id2, acc);
+                    if (full_tile || acc == 0u) {
+                        umma_i8(tbase, sdesc_sw128(sa + 32 * kk), sdesc_sw128(sa + 32 * kk), id1, acc);
+                        umma_i8(tbase + 192, sdesc_sw128(sa + 64 * TC_KT + 32 * kk),
+                                sdesc_sw128(sa + 128 * TC_KT + 32 * kk), id2, acc);
+                    } else {
+                        umma_i8(tbase, sdesc_sw128(sa + 32 * kk), sdesc_sw128(sa + 32 * kk), id0, acc);
+                    }
                 }
                 umma_commit(&empty[s]);
                 if ((i % TC_WINDOW) == TC_WINDOW - 1 || i + 1 == nloc) umma_commit(&accf);
@@ -288,7 +329,7 @@ kpzb_status gram_tc_setup(GramTC* tc, uint64_t N, int sm_count)
     if ((e = cudaMalloc(&tc->d_out, TC_ROWS * TC_ROWS * 8 + 64)) != cudaSuccess) return cuda_fail(e, "cudaMalloc(gram)");
     tc->d_err = reinterpret_cast<unsigned int*>(tc->d_out + TC_ROWS * TC_ROWS);
     if ((e = cudaFuncSetAttribute(gram_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  TC_STAGES * TC_STAGE + 1024)) != cudaSuccess)
+                                  TC_SMEM)) != cudaSuccess)
         return cuda_fail(e, "gram smem attribute");
     tc->ready = true;
     return KPZB_OK;
@@ -310,7 +351,7 @@ kpzb_status gram_tc_run(GramTC* tc, const SlopeSnapGeom& g, uint64_t N, int64_t*
     if ((e = cudaMemsetAsync(tc->d_part, 0, (size_t)tc->grid * TC_ROWS * TC_ROWS * 8, st)) != cudaSuccess)
         return cuda_fail(e, "memset partials");
     if ((e = cudaMemsetAsync(tc->d_err, 0, 4, st)) != cudaSuccess) return cuda_fail(e, "memset flag");
-    gram_tc_kernel<<<tc->grid, TC_THREADS, TC_STAGES * TC_STAGE + 1024, st>>>(
+    gram_tc_kernel<<<tc->grid, TC_THREADS, TC_SMEM, st>>>(
         g, N / TC_KT, reinterpret_cast<long long*>(tc->d_part), tc->d_err);
     if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, "gram_tc_kernel");
     gram_reduce_kernel<<<64, 256, 0, st>>>(reinterpret_cast<const long long*>(tc->d_part), tc->grid,

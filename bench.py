@@ -68,6 +68,10 @@ def parse():
                          "(oracle/_ref/kpz_ref_gpu) instead of its CPU scheduler")
     ap.add_argument("--dry-run", action="store_true",
                     help="launcher check: form the process group (gloo, CPU), barrier, max over ranks, print")
+    ap.add_argument("--lattice-streams", type=int, default=2,
+                    help="1: the lattices of a step run one after the other on one stream; 2: each "
+                         "lattice on its own stream, concurrently (per-lattice figures then come from "
+                         "a short sequential run after the timed one)")
     ap.add_argument("--no-configs", action="store_true",
                     help="skip the configs / reference_gpu blocks measured after the headline")
     ap.add_argument("--seeds", type=int, default=16, help="--workload c3curve: independent runs")
@@ -284,9 +288,42 @@ def run_ours(args, world, rank, local):
     torch.cuda.synchronize()
     barrier(world)
     wall = time.perf_counter() - t_wall0
-    clk = clocks.stop()
     per_lat = [sum(ev[i][j].elapsed_time(ev[i][j + 1]) for i in range(args.steps)) for j in range(len(scheds))]
-    ms = max_over_ranks(sum(per_lat), world)
+    step_ms = sum(per_lat)
+    conc = args.lattice_streams > 1 and len(scheds) > 1
+    if conc:
+        # the same steps with each lattice on its own stream: both start after the L2 flush and
+        # the step ends when both are done (their launches fill each other's idle SM slots)
+        lat_st = [torch.cuda.Stream() for _ in scheds]
+        for s, st in zip(scheds, lat_st):
+            s.setStream(st.cuda_stream)
+        ev0 = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+        ev1 = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+        torch.cuda.synchronize()
+        barrier(world)
+        t_wall0 = time.perf_counter()
+        for i in range(args.steps):
+            with torch.cuda.stream(dev_stream):
+                flush_l2(torch, flush)
+            ev0[i].record(dev_stream)
+            done = []
+            for s, st in zip(scheds, lat_st):
+                st.wait_event(ev0[i])
+                s.mcsPQSyncRngAsync(M)
+                e = torch.cuda.Event()
+                e.record(st)
+                done.append(e)
+            for e in done:
+                dev_stream.wait_event(e)
+            ev1[i].record(dev_stream)
+        torch.cuda.synchronize()
+        barrier(world)
+        wall = time.perf_counter() - t_wall0
+        step_ms = sum(ev0[i].elapsed_time(ev1[i]) for i in range(args.steps))
+        for s in scheds:
+            s.setStream(dev_stream.cuda_stream)
+    clk = clocks.stop()
+    ms = max_over_ranks(step_ms, world)
     updates = float(N) * M * len(scheds) * args.steps * world
     value = updates / (ms * 1e6)
 
@@ -331,7 +368,7 @@ def run_ours(args, world, rank, local):
                 "hbm": hbm, "fusion_gain": hbm["frac"]}
     if None not in opw:
         ops_step = sum(float(N) * M * o / 32.0 for o in opw)
-        int_ach = ops_step * args.steps / (sum(per_lat) * 1e-3)
+        int_ach = ops_step * args.steps / (step_ms * 1e-3)
         upd_per_op = float(N) * M * len(scheds) / ops_step  # attempts per algorithmic ALU op
         int_roof_upd = lop3 * upd_per_op / 1e9
         hbm_roof_upd = peak  # 1 B per attempt: GB/s == attempts/ns
@@ -1198,6 +1235,10 @@ def main():
                            "lattice": "16384x16384", "mcs_per_step": args.mcs_per_step,
                            "lattices_per_gpu": len(PQS), "mcs_per_pass": ks,
                            "l2": "flushed between steps (256 MiB write, untimed)",
+                           "lattice_streams": ("concurrent: each lattice on its own stream, the step timed "
+                                               "from the flush to both lattices done; per_lattice from a "
+                                               "sequential run of the same steps")
+                           if args.lattice_streams > 1 else "sequential on one stream",
                            "parallelism": f"replicas x{world}"},
                 "per_lattice": per_lattice, "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
                 "clocks": clk,

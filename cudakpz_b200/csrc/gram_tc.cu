@@ -41,7 +41,7 @@ constexpr int TC_THREADS = (TC_PROD_WARP0 + TC_PROD_WARPS) * 32;
 constexpr int TC_COLS = 256;                      // TMEM columns: D1 0..191, D2 192..255
 constexpr int TC_LUT = 256;                       // 8-site slope patterns
 constexpr int TC_SMEM = TC_STAGES * TC_STAGE + TC_LUT * 8 + 1024;
-constexpr uint32_t TC_SPIN = 1u << 26;
+constexpr uint64_t TC_WAIT_NS = 4000000000ull;    // bound of every mbarrier wait (4 s)
 
 // UMMA instruction descriptor, kind::i8: S32 accumulate (bits 4-5 = 2), signed A and B
 // (bits 7-9, 10-12 = 1), both K-major, N>>3 at bit 17, M>>4 at bit 24.
@@ -58,12 +58,23 @@ __device__ __forceinline__ uint64_t sdesc_sw128(uint32_t saddr)
            (2ull << 61);
 }
 
+__device__ __forceinline__ uint64_t global_ns()
+{
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// waits for the phase with the given parity; false after TC_WAIT_NS of global time
 __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity)
 {
-    uint32_t spins = 0;
-    while (!mbar_try_wait(bar, parity))
-        if (++spins > TC_SPIN) return false;
-    return true;
+    if (mbar_try_wait(bar, parity)) return true;
+    const uint64_t t0 = global_ns();
+    for (;;) {
+        for (int k = 0; k < 64; ++k)
+            if (mbar_try_wait(bar, parity)) return true;
+        if (global_ns() - t0 > TC_WAIT_NS) return false;
+    }
 }
 
 // four values' low bytes, first in the lowest byte
